@@ -1,0 +1,249 @@
+/*
+ * mf.h -- C ABI of the B200-native tiled CG / BiCGSTAB solver (libmf.so).
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and
+ * returns an int status (MF_OK = 0, negative = error, see mf_status_str).
+ * Host pointers are named *_host, device pointers *_dev.
+ *
+ * Reference interfaces replaced (paths are inside the Mille-feuille tree):
+ *   cg_solve_inc(...)        Performance-Comparison/Mille-feuille_CG_NVIDIA.cu:3979
+ *   bicgstab(...)            Performance-Comparison/Mille-feuille_BiCGSTAB_NVIDIA.cu:1476
+ *   Tile_create(...)         Performance-Comparison/csr2block.h:267
+ *   blockspmv_cpu(...)       Performance-Comparison/blockspmv_cpu.h:2   (SpMV part)
+ *   read_Dmatrix_32(...)     Performance-Comparison/biio2.0/src/biio.h:153
+ *   binary_read_csr / binary_write_csr   biio2.0/src/biio.h:22 / :74
+ *   row compression          Mille-feuille_CG_NVIDIA.cu:4154-4213
+ *   two-pointer balance      Mille-feuille_CG_NVIDIA.cu:4216-4484
+ */
+#ifndef MF_H_
+#define MF_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+enum {
+    MF_OK = 0,
+    MF_ERR_ARG = -1,           /* invalid argument / precondition           */
+    MF_ERR_CUDA = -2,          /* a CUDA runtime call failed                */
+    MF_ERR_TIMEOUT = -3,       /* a bounded device wait ran out             */
+    MF_ERR_NOT_CONVERGED = -4, /* maxiter reached above tolerance           */
+    MF_ERR_BREAKDOWN = -5,     /* zero/NaN denominator in the recurrence    */
+    MF_ERR_IO = -6,            /* file could not be read / parsed           */
+    MF_ERR_NOMEM = -7,         /* host or device allocation failed          */
+    MF_ERR_RESIDENCY = -8,     /* persistent grid cannot be co-resident     */
+    MF_ERR_UNSUPPORTED = -9    /* feature not available for this input      */
+};
+const char *mf_status_str(int status);
+/* Text of the last error recorded by the library (thread-unsafe, for logs). */
+const char *mf_last_error(void);
+
+/* ---- precision ------------------------------------------------------- */
+enum { MF_PREC_FP64 = 0, MF_PREC_FP32 = 1, MF_PREC_FP16 = 2, MF_PREC_FP8 = 3 };
+enum {
+    MF_MODE_FP64 = 0,        /* every tile FP64, exact blockspmv order          */
+    MF_MODE_MIXED_RULE = 1,  /* per-tile precision from the magnitude rule      */
+    MF_MODE_MIXED_MLP = 2,   /* per-tile precision from the learned selector    */
+    MF_MODE_FIXED = 3        /* every tile at options.fixed_precision           */
+};
+
+/* ---- host CSR matrix (0-based, int32) -------------------------------- */
+typedef struct {
+    int n;              /* rows                                  */
+    int ncols;          /* columns                               */
+    int nnz;            /* row_ptr[n]                            */
+    const int *row_ptr; /* n+1, row_ptr[0] == 0                  */
+    const int *col_idx; /* nnz                                   */
+    const double *val;  /* nnz                                   */
+} mf_csr;
+
+/* ---- options ---------------------------------------------------------- */
+typedef struct {
+    int precision_mode;      /* MF_MODE_*                                      */
+    int fixed_precision;     /* MF_PREC_* used by MF_MODE_FIXED                */
+    int replace_every;       /* true-residual replacement period of the mixed
+                                precision modes (FP64 mode never replaces)    */
+    int ctas_per_sm;         /* persistent CTAs per SM, 0 = autotune           */
+    int rb_per_slab;         /* row blocks per slab, 0 = default (32)          */
+    int slab_bytes;          /* max bytes of one streamed slab, 0 = default    */
+    double timeout_s;        /* limit of every device spin-wait, 0 = 2 s       */
+    int check_true_residual; /* confirm convergence with b - A x (default 1)   */
+    int fixed_iterations;    /* >0: run exactly this many iterations           */
+    double mixed_tau;        /* magnitude-rule tolerance scale, 0 = default    */
+    int device;              /* CUDA device ordinal                            */
+    int reserved[7];         /* reserved[0] == 0x5741: test hook, the CG kernel
+                                first waits on a flag nothing sets, so the
+                                bounded wait must end it with MF_ERR_TIMEOUT */
+} mf_options;
+void mf_options_default(mf_options *opt);
+
+/* ---- solve result ----------------------------------------------------- */
+typedef struct {
+    int status;              /* MF_OK or MF_ERR_*                              */
+    int iterations;          /* iterations executed                            */
+    int replacements;        /* true-residual replacements performed           */
+    int level_switches;      /* precision tightenings performed                */
+    double rel_residual_true;/* ||b - A x|| / ||b|| recomputed in FP64         */
+    double rel_residual_rec; /* recursive residual ||r_k|| / ||b||             */
+    double time_ms;          /* device time of the solve launch                */
+    double spmv_bytes;       /* algorithmic bytes of one SpMV (current layout) */
+    double spmv_bytes_fp64;  /* algorithmic bytes of one FP64 SpMV             */
+    double tile_frac[4];     /* fraction of tiles per MF_PREC_* at the end     */
+    int error_site;          /* device error site code (0 = none)              */
+    int reserved[7];
+} mf_result;
+
+/* ---- opaque handles --------------------------------------------------- */
+typedef struct mf_matrix mf_matrix; /* host CSR (+ optional vectors)          */
+typedef struct mf_tiles mf_tiles;   /* device tile matrix + solver layout     */
+
+/* ---- host matrices: generators, readers, writers ---------------------- */
+/* 2D 5-point Laplacian on an N x N grid, b = A * ones.                       */
+int mf_gen_poisson2d(int N, mf_matrix **out);
+/* 3D 7-point upwind convection-diffusion, D = 1, h = 1, v = (vx,vy,vz),
+ * b ~ U[-1,1] drawn from seed.                                               */
+int mf_gen_convdiff3d(int N, double vx, double vy, double vz, uint64_t seed,
+                      mf_matrix **out);
+/* 3D 7-point variable-coefficient Poisson, face coefficients log-uniform in
+ * [klo, khi], x* ~ U[0,1] (same stream), b = A x*.                           */
+int mf_gen_varpoisson3d(int N, double klo, double khi, uint64_t seed,
+                        mf_matrix **out);
+/* Random sparse SPD system (4..12 off-diagonals per row, U[-1,0], symmetrised,
+ * diagonal = row sum of |off| + 0.01), b ~ U[-1,1].                          */
+int mf_gen_spd_random(int n, uint64_t seed, mf_matrix **out);
+/* Sizes of a batch: count values log-uniform in [lo, hi].                    */
+int mf_gen_batch_sizes(int count, int lo, int hi, uint64_t seed, int *sizes_host);
+/* Matrix Market reader with read_Dmatrix_32 semantics (0-based, symmetric
+ * and hermitian expanded, file order kept within rows).                      */
+int mf_read_mtx(const char *path, mf_matrix **out);
+/* .cbd binary CSR (int rows, int cols, int64 nnz, int64 row_ptr[rows+1],
+ * int col_idx[nnz], double val[nnz]).                                        */
+int mf_read_cbd(const char *path, mf_matrix **out);
+int mf_write_cbd(const mf_matrix *m, const char *path);
+int mf_matrix_from_csr(int n, int ncols, int nnz, const int *row_ptr,
+                       const int *col_idx, const double *val, mf_matrix **out);
+int mf_matrix_info(const mf_matrix *m, int *n, int *ncols, int *nnz,
+                   int *has_b, int *has_xstar);
+int mf_matrix_csr(const mf_matrix *m, mf_csr *csr);      /* borrowed views */
+const double *mf_matrix_b(const mf_matrix *m);            /* NULL if none   */
+const double *mf_matrix_xstar(const mf_matrix *m);        /* NULL if none   */
+int mf_matrix_set_b(mf_matrix *m, const double *b_host);
+void mf_matrix_free(mf_matrix *m);
+
+/* ---- tile encoder (GPU csr2block) ------------------------------------- */
+/* Upload a host CSR and encode it on the GPU into 16x16 tiles (the
+ * Tile_create layout) plus the solver's slab layout.                         */
+int mf_encode(const mf_csr *A, const mf_options *opt, mf_tiles **out);
+/* Same, from CSR arrays already on the device (no host copies).              */
+int mf_encode_dev(int n, int ncols, int nnz, const int *row_ptr_dev,
+                  const int *col_idx_dev, const double *val_dev,
+                  const mf_options *opt, mf_tiles **out);
+void mf_free(mf_tiles *t);
+
+typedef struct {
+    int rowA, colA, tilem, tilen, tilenum, csrsize, csrptrlen;
+    int cnt_non_new;       /* nonzero_row_new[tilenum] (row compression)     */
+    int nslabs, nctas;     /* solver layout                                  */
+    long long layout_bytes;/* bytes of the slab layout (current level)       */
+    double encode_ms;      /* device time of the encoder                     */
+    double layout_ms;      /* host + device time of the slab layout build    */
+} mf_tile_info;
+int mf_tiles_info(const mf_tiles *t, mf_tile_info *info);
+
+/* Host copies of the Tile_create arrays (caller allocates, NULL = skip).
+ * Sizes: tile_ptr tilem+1; tile_columnidx tilenum; tile_nnz, blknnz,
+ * csr_offset, csrptr_offset tilenum+1; Format tilenum; blknnznnz tilenum+1;
+ * Blockcsr_Val, Blockcsr_Val_Low, Tile_csr_Col csrsize; Blockcsr_Ptr
+ * csrptrlen; csr_compressedIdx ceil(csrsize/2) (always zero, as in the
+ * reference). Derived arrays: ptroffset1, ptroffset2, tile_rowidx tilenum;
+ * nonzero_row_new tilenum+1; blockrowid_new, blockcsr_ptr_new
+ * cnt_non_new+1; block_signal tilem+1.                                       */
+typedef struct {
+    int *tile_ptr, *tile_columnidx, *tile_nnz, *blknnz, *csr_offset,
+        *csrptr_offset;
+    char *Format;
+    unsigned char *blknnznnz;
+    double *Blockcsr_Val;
+    float *Blockcsr_Val_Low;
+    unsigned char *Tile_csr_Col, *Blockcsr_Ptr, *csr_compressedIdx;
+    int *ptroffset1, *ptroffset2, *tile_rowidx, *nonzero_row_new, *block_signal;
+    unsigned char *blockrowid_new, *blockcsr_ptr_new;
+} mf_tile_arrays;
+int mf_tiles_export(const mf_tiles *t, mf_tile_arrays *host);
+
+/* Per-tile precision codes (MF_PREC_*) and scales of the current layout.    */
+int mf_tiles_precisions(const mf_tiles *t, unsigned char *prec_host,
+                        float *scale_host);
+/* Re-encode the solver layout with explicit per-tile precisions.            */
+int mf_tiles_set_precisions(mf_tiles *t, const unsigned char *prec_host);
+
+/* Two-pointer warp work split of the reference driver (compatibility
+ * export; the solver itself uses an nnz-balanced contiguous partition).
+ * Returns the number of warp units in *index; arrays sized tilenum+1 and
+ * index+1 (call once with NULL arrays to get *index).                       */
+int mf_balance_twopointer(const mf_tiles *t, int block_nnz, int block_per_warp,
+                          int *index, int *balance_tile_ptr_new,
+                          int *index_each_block_new, int *row_each_block_new,
+                          int *non_each_block_new);
+
+/* ---- SpMV ------------------------------------------------------------- */
+/* y = A x with the tiled kernel. x_dev has ncols entries, y_dev rowA.
+ * FP64 layout: bit-identical to blockspmv_cpu's summation order.
+ * stream: a cudaStream_t (NULL = default stream).                           */
+int mf_spmv(const mf_tiles *t, const double *x_dev, double *y_dev, void *stream);
+/* Same with host buffers (copies included).                                 */
+int mf_spmv_host(const mf_tiles *t, const double *x_host, double *y_host);
+/* Device time (ms) of `reps` back-to-back tiled SpMVs on the given vectors. */
+int mf_spmv_bench(const mf_tiles *t, const double *x_dev, double *y_dev,
+                  int reps, double *ms_per_spmv, double *alg_bytes);
+/* Same two calls on mixed-precision layout `level` (-1 = FP64 layout).      */
+int mf_spmv_level(const mf_tiles *t, int level, const double *x_dev, double *y_dev);
+int mf_spmv_bench_level(const mf_tiles *t, int level, const double *x_dev,
+                        double *y_dev, int reps, double *ms_per_spmv,
+                        double *alg_bytes);
+
+/* ---- solvers ---------------------------------------------------------- */
+/* Single persistent-kernel CG. b and x (x0 in, solution out) on the host.  */
+int mf_solve_cg(mf_tiles *t, const double *b_host, double *x_host, double tol,
+                int maxiter, const mf_options *opt, mf_result *res);
+/* Same with device vectors (n entries each).                                */
+int mf_solve_cg_dev(mf_tiles *t, const double *b_dev, double *x_dev, double tol,
+                    int maxiter, const mf_options *opt, mf_result *res);
+/* Single persistent-kernel BiCGSTAB.                                         */
+int mf_solve_bicgstab(mf_tiles *t, const double *b_host, double *x_host,
+                      double tol, int maxiter, const mf_options *opt,
+                      mf_result *res);
+int mf_solve_bicgstab_dev(mf_tiles *t, const double *b_dev, double *x_dev,
+                          double tol, int maxiter, const mf_options *opt,
+                          mf_result *res);
+/* ||b - A x|| / ||b|| with the FP64 tiled SpMV (device vectors).             */
+int mf_true_residual(mf_tiles *t, const double *b_dev, const double *x_dev,
+                     double *rel);
+
+/* ---- drop-in replacements of the reference entry points --------------- */
+/* Same signature as the reference. n is truncated to a multiple of 16 as
+ * the reference's callers do; columns beyond the truncated n are dropped.
+ * x is zeroed and overwritten with the solution; *iter receives the
+ * iteration count (the reference leaves it untouched). maxiter and
+ * threshold (relative residual) are honoured; filename, ori and block_nnz
+ * are accepted for signature compatibility.                                 */
+void cg_solve_inc(int *RowPtr, int *ColIdx, double *Val, float *Val_Low,
+                  double *x, double *b, int n, int *iter, int maxiter,
+                  double threshold, char *filename, int nnzR, int ori,
+                  int block_nnz);
+/* Returns 0 on convergence, 1 otherwise (reference: 1 when itr >= maxits).
+ * rhs is overwritten with A * ones and solved from x = 0, as the reference
+ * does; tolerance 1e-10 relative, at most 10000 iterations.                 */
+int bicgstab(int *RowPtr, int *ColIdx, double *Val, double *rhs, double *x,
+             int nnzR, char *filename, int n, int block_nnz);
+
+/* ---- version ------------------------------------------------------------ */
+const char *mf_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MF_H_ */

@@ -1,0 +1,495 @@
+// C ABI of libmf (declared in include/mf.h): handles, encoder entry points,
+// exports of the Tile_create arrays, SpMV and the persistent solvers.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "solver.h"
+#include "tiles.h"
+
+using namespace mf;
+
+namespace mf {
+int build_mixed_levels(mf_tiles *t, cudaStream_t s);  // precision.cpp
+}
+
+template <class T>
+static int d2h(T *dst, const T *src, size_t count) {
+    if (!dst || count == 0) return MF_OK;
+    MF_CUDA_TRY(cudaMemcpy(dst, src, count * sizeof(T), cudaMemcpyDeviceToHost));
+    return MF_OK;
+}
+
+extern "C" {
+
+const char *mf_status_str(int s) {
+    switch (s) {
+        case MF_OK: return "ok";
+        case MF_ERR_ARG: return "invalid argument";
+        case MF_ERR_CUDA: return "CUDA error";
+        case MF_ERR_TIMEOUT: return "device wait timed out";
+        case MF_ERR_NOT_CONVERGED: return "not converged";
+        case MF_ERR_BREAKDOWN: return "breakdown";
+        case MF_ERR_IO: return "I/O error";
+        case MF_ERR_NOMEM: return "out of memory";
+        case MF_ERR_RESIDENCY: return "persistent grid cannot be co-resident";
+        case MF_ERR_UNSUPPORTED: return "unsupported input";
+        default: return "unknown status";
+    }
+}
+
+const char *mf_version(void) { return "mf-b200 0.1 (sm_100a)"; }
+
+const char *mf_last_error(void) { return mf::last_error().c_str(); }
+
+void mf_options_default(mf_options *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof *o);
+    o->precision_mode = MF_MODE_FP64;
+    o->fixed_precision = MF_PREC_FP64;
+    o->replace_every = 50;
+    o->ctas_per_sm = 0;
+    o->rb_per_slab = 0;
+    o->slab_bytes = 0;
+    o->timeout_s = 2.0;
+    o->check_true_residual = 1;
+    o->fixed_iterations = 0;
+    o->mixed_tau = 0.0;
+    o->device = 0;
+}
+
+static int fetch_host_tiles(mf_tiles *t) {
+    t->h_tile_ptr.resize(t->tilem + 1);
+    t->h_tile_col.resize(t->tilenum);
+    std::vector<int> off(t->tilenum + 1);
+    MF_CUDA_TRY(cudaMemcpy(t->h_tile_ptr.data(), t->tile_ptr.p, sizeof(int) * (t->tilem + 1), cudaMemcpyDeviceToHost));
+    if (t->tilenum > 0)
+        MF_CUDA_TRY(cudaMemcpy(t->h_tile_col.data(), t->tile_col.p, sizeof(int) * t->tilenum, cudaMemcpyDeviceToHost));
+    MF_CUDA_TRY(cudaMemcpy(off.data(), t->tile_off.p, sizeof(int) * (t->tilenum + 1), cudaMemcpyDeviceToHost));
+    t->h_tile_nnz.resize(t->tilenum);
+    for (int k = 0; k < t->tilenum; ++k) t->h_tile_nnz[k] = off[k + 1] - off[k];
+    return MF_OK;
+}
+
+int mf_encode_dev(int n, int ncols, int nnz, const int *rp, const int *ci, const double *val,
+                  const mf_options *opt, mf_tiles **out) {
+    if (!out || n <= 0 || ncols <= 0 || nnz < 0 || !rp || (nnz > 0 && (!ci || !val))) return MF_ERR_ARG;
+    auto *t = new mf_tiles;
+    if (opt) t->opt = *opt;
+    else mf_options_default(&t->opt);
+    int rc;
+    MF_CUDA_TRY(cudaSetDevice(t->opt.device));
+    t->device = t->opt.device;
+    cudaDeviceProp prop;
+    MF_CUDA_TRY(cudaGetDeviceProperties(&prop, t->device));
+    t->nsm = prop.multiProcessorCount;
+    if ((rc = kernel_config(t, &t->G)) != MF_OK) { delete t; return rc; }
+    cudaStream_t s = 0;
+    if ((rc = encode_device(t, n, ncols, nnz, rp, ci, val, s)) != MF_OK) { delete t; return rc; }
+    if ((rc = fetch_host_tiles(t)) != MF_OK) { delete t; return rc; }
+    std::vector<uint8_t> prec(t->tilenum, MF_PREC_FP64);
+    if ((rc = build_layout(t, t->L64, prec, s)) != MF_OK) { delete t; return rc; }
+    if (t->opt.precision_mode != MF_MODE_FP64) {
+        if ((rc = build_mixed_levels(t, s)) != MF_OK) { delete t; return rc; }
+    }
+    *out = t;
+    return MF_OK;
+}
+
+int mf_encode(const mf_csr *A, const mf_options *opt, mf_tiles **out) {
+    if (!A || !out || A->n <= 0 || A->ncols <= 0 || A->nnz < 0 || !A->row_ptr) return MF_ERR_ARG;
+    if (A->row_ptr[0] != 0 || A->row_ptr[A->n] != A->nnz) return MF_ERR_ARG;
+    for (int i = 0; i < A->nnz; ++i)
+        if (A->col_idx[i] < 0 || A->col_idx[i] >= A->ncols) return MF_ERR_ARG;
+    const int dev = opt ? opt->device : 0;
+    MF_CUDA_TRY(cudaSetDevice(dev));
+    DevArray<int> rp, ci;
+    DevArray<double> v;
+    if (rp.alloc(A->n + 1) || ci.alloc(A->nnz) || v.alloc(A->nnz)) return MF_ERR_NOMEM;
+    MF_CUDA_TRY(cudaMemcpy(rp.p, A->row_ptr, sizeof(int) * (A->n + 1), cudaMemcpyHostToDevice));
+    if (A->nnz > 0) {
+        MF_CUDA_TRY(cudaMemcpy(ci.p, A->col_idx, sizeof(int) * A->nnz, cudaMemcpyHostToDevice));
+        MF_CUDA_TRY(cudaMemcpy(v.p, A->val, sizeof(double) * A->nnz, cudaMemcpyHostToDevice));
+    }
+    return mf_encode_dev(A->n, A->ncols, A->nnz, rp.p, ci.p, v.p, opt, out);
+}
+
+void mf_free(mf_tiles *t) { delete t; }
+
+int mf_tiles_info(const mf_tiles *t, mf_tile_info *info) {
+    if (!t || !info) return MF_ERR_ARG;
+    info->rowA = t->rowA;
+    info->colA = t->colA;
+    info->tilem = t->tilem;
+    info->tilen = t->tilen;
+    info->tilenum = t->tilenum;
+    info->csrsize = t->csrsize;
+    info->csrptrlen = t->csrptrlen;
+    info->cnt_non_new = t->cnt_non_new;
+    info->nslabs = t->L64.nslabs;
+    info->nctas = t->G;
+    info->layout_bytes = (long long)t->L64.bytes;
+    info->encode_ms = t->encode_ms;
+    info->layout_ms = t->layout_ms;
+    return MF_OK;
+}
+
+int mf_tiles_export(const mf_tiles *t, mf_tile_arrays *h) {
+    if (!t || !h) return MF_ERR_ARG;
+    const size_t tn = (size_t)t->tilenum;
+    int rc = MF_OK;
+    rc |= d2h(h->tile_ptr, t->tile_ptr.p, (size_t)t->tilem + 1);
+    rc |= d2h(h->tile_columnidx, t->tile_col.p, tn);
+    rc |= d2h(h->tile_nnz, t->tile_off.p, tn + 1);
+    rc |= d2h(h->blknnz, t->tile_off.p, tn + 1);
+    rc |= d2h(h->csr_offset, t->tile_off.p, tn + 1);
+    rc |= d2h(h->csrptr_offset, t->csrptr_off.p, tn + 1);
+    rc |= d2h(h->blknnznnz, t->blknnznnz.p, tn + 1);
+    rc |= d2h(h->Blockcsr_Val, t->val.p, (size_t)t->csrsize);
+    rc |= d2h(h->Blockcsr_Val_Low, t->val_low.p, (size_t)t->csrsize);
+    rc |= d2h(h->Tile_csr_Col, t->col.p, (size_t)t->csrsize);
+    rc |= d2h(h->Blockcsr_Ptr, t->ptr.p, (size_t)t->csrptrlen);
+    rc |= d2h(h->ptroffset1, t->tile_off.p, tn);
+    rc |= d2h(h->ptroffset2, t->csrptr_off.p, tn);
+    rc |= d2h(h->tile_rowidx, t->tile_rowidx.p, tn);
+    rc |= d2h(h->nonzero_row_new, t->nonzero_row_new.p, tn + 1);
+    rc |= d2h(h->block_signal, t->block_signal.p, (size_t)t->tilem + 1);
+    rc |= d2h(h->blockrowid_new, t->blockrowid_new.p, (size_t)t->cnt_non_new + 1);
+    rc |= d2h(h->blockcsr_ptr_new, t->blockcsr_ptr_new.p, (size_t)t->cnt_non_new + 1);
+    if (rc != MF_OK) return MF_ERR_CUDA;
+    if (h->Format) std::memset(h->Format, 0, tn);
+    if (h->csr_compressedIdx) std::memset(h->csr_compressedIdx, 0, ((size_t)t->csrsize + 1) / 2);
+    // A 1-row tail block: Tile_create's exclusive_scan_char leaves the row
+    // count in the pointer and step 4 then copies no values for it
+    // (csr2block.h:237-251, utils.h:52-53). The device keeps correct tiles;
+    // the export reproduces the reference arrays.
+    const int rl_last = t->rowA - (t->tilem - 1) * 16;
+    if (rl_last == 1) {
+        std::vector<int> tp(2), off(2);
+        cudaMemcpy(tp.data(), t->tile_ptr.p + t->tilem - 1, 2 * sizeof(int), cudaMemcpyDeviceToHost);
+        for (int k = tp[0]; k < tp[1]; ++k) {
+            int o[2];
+            cudaMemcpy(o, t->tile_off.p + k, 2 * sizeof(int), cudaMemcpyDeviceToHost);
+            int cc = 0;
+            cudaMemcpy(&cc, t->csrptr_off.p + k, sizeof(int), cudaMemcpyDeviceToHost);
+            if (h->Blockcsr_Ptr) h->Blockcsr_Ptr[cc] = (unsigned char)(o[1] - o[0]);
+            for (int q = o[0]; q < o[1]; ++q) {
+                if (h->Blockcsr_Val) h->Blockcsr_Val[q] = 0.0;
+                if (h->Blockcsr_Val_Low) h->Blockcsr_Val_Low[q] = 0.0f;
+                if (h->Tile_csr_Col) h->Tile_csr_Col[q] = 0;
+            }
+        }
+    }
+    return MF_OK;
+}
+
+int mf_tiles_precisions(const mf_tiles *t, unsigned char *prec, float *scale) {
+    if (!t) return MF_ERR_ARG;
+    const Layout *L = &t->L64;
+    for (int l = MF_NLEVELS - 1; l >= 0; --l)
+        if (t->mixed_ready && t->Lmix[l].built) {
+            L = &t->Lmix[0];
+            break;
+        }
+    if (prec) std::memcpy(prec, L->prec.data(), L->prec.size());
+    if (scale && t->tilenum > 0)
+        MF_CUDA_TRY(cudaMemcpy(scale, L->scale_dev.p, sizeof(float) * t->tilenum, cudaMemcpyDeviceToHost));
+    return MF_OK;
+}
+
+int mf_tiles_set_precisions(mf_tiles *t, const unsigned char *prec) {
+    if (!t || !prec) return MF_ERR_ARG;
+    std::vector<uint8_t> p(prec, prec + t->tilenum);
+    for (auto &v : p)
+        if (v > MF_PREC_FP8) return MF_ERR_ARG;
+    int rc = build_layout(t, t->Lmix[0], p, 0);
+    if (rc) return rc;
+    for (int l = 1; l < MF_NLEVELS; ++l) t->Lmix[l].built = false;
+    t->mixed_ready = true;
+    return MF_OK;
+}
+
+// ------------------------------------------------------------------ SpMV
+static int prepare_x(mf_tiles *t, const double *x, const double **xs) {
+    // the x stage reads whole 16-entry segments: use x directly when it is
+    // 16-byte aligned and covers every segment, else a padded copy
+    const size_t need = (size_t)t->tilen * 16;
+    if (((uintptr_t)x & 15u) == 0 && (size_t)t->colA == need) {
+        *xs = x;
+        return MF_OK;
+    }
+    if (t->xpad.n < need && t->xpad.alloc(need)) return MF_ERR_NOMEM;
+    MF_CUDA_TRY(cudaMemsetAsync(t->xpad.p, 0, need * sizeof(double)));
+    MF_CUDA_TRY(cudaMemcpyAsync(t->xpad.p, x, (size_t)t->colA * sizeof(double), cudaMemcpyDeviceToDevice));
+    *xs = t->xpad.p;
+    return MF_OK;
+}
+
+int mf_spmv(const mf_tiles *tc, const double *x, double *y, void *stream) {
+    mf_tiles *t = const_cast<mf_tiles *>(tc);
+    if (!t || !x || !y) return MF_ERR_ARG;
+    const double *xs;
+    int rc = prepare_x(t, x, &xs);
+    if (rc) return rc;
+    rc = launch_spmv(t, -1, xs, y, 1, (cudaStream_t)stream);
+    if (rc) return rc;
+    MF_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    return MF_OK;
+}
+
+int mf_spmv_level(const mf_tiles *tc, int level, const double *x, double *y) {
+    mf_tiles *t = const_cast<mf_tiles *>(tc);
+    if (!t || !x || !y) return MF_ERR_ARG;
+    const double *xs;
+    int rc = prepare_x(t, x, &xs);
+    if (rc) return rc;
+    rc = launch_spmv(t, level, xs, y, 1, 0);
+    if (rc) return rc;
+    MF_CUDA_TRY(cudaDeviceSynchronize());
+    return MF_OK;
+}
+
+int mf_spmv_host(const mf_tiles *t, const double *x, double *y) {
+    if (!t || !x || !y) return MF_ERR_ARG;
+    DevArray<double> dx, dy;
+    if (dx.alloc((size_t)t->tilen * 16) || dy.alloc((size_t)t->tilem * 16)) return MF_ERR_NOMEM;
+    MF_CUDA_TRY(cudaMemset(dx.p, 0, sizeof(double) * t->tilen * 16));
+    MF_CUDA_TRY(cudaMemcpy(dx.p, x, sizeof(double) * t->colA, cudaMemcpyHostToDevice));
+    int rc = mf_spmv(t, dx.p, dy.p, nullptr);
+    if (rc) return rc;
+    MF_CUDA_TRY(cudaMemcpy(y, dy.p, sizeof(double) * t->rowA, cudaMemcpyDeviceToHost));
+    return MF_OK;
+}
+
+int mf_spmv_bench_level(const mf_tiles *tc, int level, const double *x, double *y, int reps, double *ms,
+                        double *alg_bytes) {
+    mf_tiles *t = const_cast<mf_tiles *>(tc);
+    if (!t || !x || !y || reps <= 0) return MF_ERR_ARG;
+    const double *xs;
+    int rc = prepare_x(t, x, &xs);
+    if (rc) return rc;
+    // warm-up
+    if ((rc = launch_spmv(t, level, xs, y, 1, 0))) return rc;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, 0);
+    for (int i = 0; i < reps; ++i)
+        if ((rc = launch_spmv(t, level, xs, y, 1, 0))) return rc;
+    cudaEventRecord(e1, 0);
+    MF_CUDA_TRY(cudaEventSynchronize(e1));
+    float f = 0;
+    cudaEventElapsedTime(&f, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (ms) *ms = f / reps;
+    if (alg_bytes) *alg_bytes = level >= 0 ? t->Lmix[level].alg_bytes : t->L64.alg_bytes;
+    return MF_OK;
+}
+
+int mf_spmv_bench(const mf_tiles *t, const double *x, double *y, int reps, double *ms, double *alg_bytes) {
+    return mf_spmv_bench_level(t, -1, x, y, reps, ms, alg_bytes);
+}
+
+// --------------------------------------------------------------- solvers
+static int ensure_workspace(mf_tiles *t) {
+    const size_t n16 = (size_t)t->tilem * 16;
+    const size_t need = 8 * n16 + 2 * 4 * (size_t)t->G + 64;
+    if (t->ws.n < need) {
+        if (t->ws.alloc(need)) return MF_ERR_NOMEM;
+    }
+    const size_t sw = sync_words(t->G) + sizeof(DevResult) / 4 + 8;
+    if (t->sync.n < sw) {
+        if (t->sync.alloc(sw)) return MF_ERR_NOMEM;
+    }
+    return MF_OK;
+}
+
+struct WsView {
+    double *b, *x, *r, *d, *q, *s, *t, *rh, *partial;
+    DevResult *res;
+};
+
+static WsView ws_view(mf_tiles *t) {
+    const size_t n16 = (size_t)t->tilem * 16;
+    WsView v;
+    double *w = t->ws.p;
+    v.b = w;
+    v.x = w + n16;
+    v.r = w + 2 * n16;
+    v.d = w + 3 * n16;
+    v.q = w + 4 * n16;
+    v.s = w + 5 * n16;
+    v.t = w + 6 * n16;
+    v.rh = w + 7 * n16;
+    v.partial = w + 8 * n16;
+    v.res = reinterpret_cast<DevResult *>(t->sync.p + sync_words(t->G));
+    return v;
+}
+
+static int true_residual_ws(mf_tiles *t, const double *b, const double *x, double *rel) {
+    // ax into the q slot of the workspace, norms into the partial area tail
+    WsView v = ws_view(t);
+    int rc = launch_spmv(t, -1, x, v.q, 1, 0);
+    if (rc) return rc;
+    double *out = v.partial + 2 * 4 * t->G;
+    if ((rc = launch_residual_norms(t->rowA, b, v.q, out, 0))) return rc;
+    double h[2];
+    MF_CUDA_TRY(cudaMemcpy(h, out, sizeof h, cudaMemcpyDeviceToHost));
+    *rel = h[1] > 0 ? std::sqrt(h[0]) / std::sqrt(h[1]) : std::sqrt(h[0]);
+    return MF_OK;
+}
+
+// kind 0 = CG, 1 = BiCGSTAB. b_dev / x_dev: n entries (device). x in: x0.
+static int solve_dev(mf_tiles *t, int kind, const double *b_dev, double *x_dev, double tol, int maxiter,
+                     const mf_options *opt_in, mf_result *res) {
+    if (!t || !b_dev || !x_dev) return MF_ERR_ARG;
+    if (t->rowA != t->colA) {
+        set_last_error("the solvers need a square matrix");
+        return MF_ERR_UNSUPPORTED;
+    }
+    mf_options opt = opt_in ? *opt_in : t->opt;
+    int rc = ensure_workspace(t);
+    if (rc) return rc;
+    WsView v = ws_view(t);
+    const size_t n16 = (size_t)t->tilem * 16;
+    const int n = t->rowA;
+    MF_CUDA_TRY(cudaMemsetAsync(t->ws.p, 0, sizeof(double) * 8 * n16));
+    MF_CUDA_TRY(cudaMemcpyAsync(v.b, b_dev, sizeof(double) * n, cudaMemcpyDeviceToDevice));
+    MF_CUDA_TRY(cudaMemcpyAsync(v.x, x_dev, sizeof(double) * n, cudaMemcpyDeviceToDevice));
+    MF_CUDA_TRY(cudaMemsetAsync(t->sync.p, 0, sizeof(uint32_t) * t->sync.n));
+    KParams P;
+    base_params(t, P);
+    if (opt.timeout_s > 0) P.limit_ns = (uint64_t)(opt.timeout_s * 1e9);
+    P.sync = t->sync.p;
+    P.partial = v.partial;
+    P.b = v.b;
+    P.x = v.x;
+    P.r = v.r;
+    P.d = v.d;
+    P.q = v.q;
+    P.s = v.s;
+    P.t = v.t;
+    P.rh = v.rh;
+    P.tol = tol;
+    P.maxiter = maxiter;
+    P.fixed_iterations = opt.fixed_iterations;
+    P.replace_every = opt.replace_every;
+    P.res = v.res;
+    P.inject_wait = opt.reserved[0] == 0x5741 ? 1 : 0;
+    const bool mixed = kind == 0 && opt.precision_mode != MF_MODE_FP64 && t->mixed_ready;
+    if (mixed) {
+        int nl = 1;
+        static const double level_rel[MF_NLEVELS] = {1e-4, 1e-7, 0.0};
+        for (int l = 0; l < MF_NLEVELS; ++l) {
+            if (!t->Lmix[l].built) break;
+            LayoutArgs &a = P.lay[nl];
+            a.slabs = t->Lmix[l].slabs.p;
+            a.head = t->Lmix[l].head.p;
+            a.cta_slab = t->Lmix[l].cta_slab.p;
+            a.cta_rb = t->Lmix[l].cta_rb.p;
+            a.cta_dep = t->Lmix[l].cta_dep.p;
+            P.level_rel[nl] = level_rel[l];
+            ++nl;
+        }
+        P.nlay = nl;
+        P.start_layout = 1;
+        if (P.replace_every <= 0) P.replace_every = 50;
+    } else {
+        P.replace_every = 0;  // the FP64 recurrence of the reference never replaces
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, 0);
+    rc = launch_solver(t, kind, P, 0);
+    cudaEventRecord(e1, 0);
+    cudaError_t ce = cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    if (ce != cudaSuccess) {
+        set_last_error(cudaGetErrorString(ce));
+        return MF_ERR_CUDA;
+    }
+    DevResult dr;
+    uint32_t err[2];
+    MF_CUDA_TRY(cudaMemcpy(&dr, v.res, sizeof dr, cudaMemcpyDeviceToHost));
+    MF_CUDA_TRY(cudaMemcpy(err, t->sync.p + SYNC_ERROR, sizeof err, cudaMemcpyDeviceToHost));
+    MF_CUDA_TRY(cudaMemcpy(x_dev, v.x, sizeof(double) * n, cudaMemcpyDeviceToDevice));
+    int status = err[0] ? (int)err[0] : dr.status;
+    mf_result R;
+    std::memset(&R, 0, sizeof R);
+    R.status = status;
+    R.iterations = err[0] ? -1 : dr.iterations;
+    R.replacements = dr.replacements;
+    R.level_switches = dr.level_switches;
+    R.error_site = (int)err[1];
+    R.rel_residual_rec = dr.bb > 0 ? std::sqrt(dr.rr) / std::sqrt(dr.bb) : std::sqrt(dr.rr);
+    R.time_ms = ms;
+    R.spmv_bytes_fp64 = t->L64.alg_bytes;
+    const Layout *Lf = &t->L64;
+    if (mixed && dr.final_layout >= 1 && t->Lmix[dr.final_layout - 1].built) Lf = &t->Lmix[dr.final_layout - 1];
+    R.spmv_bytes = Lf->alg_bytes;
+    for (int p = 0; p < 4; ++p) R.tile_frac[p] = Lf->tile_frac[p];
+    R.rel_residual_true = NAN;
+    if (!err[0] && opt.check_true_residual) {
+        double rel = 0;
+        int rc2 = true_residual_ws(t, v.b, v.x, &rel);
+        if (rc2) return rc2;
+        R.rel_residual_true = rel;
+    }
+    if (res) *res = R;
+    return status;
+}
+
+int mf_solve_cg_dev(mf_tiles *t, const double *b, double *x, double tol, int maxiter, const mf_options *opt,
+                    mf_result *res) {
+    return solve_dev(t, 0, b, x, tol, maxiter, opt, res);
+}
+int mf_solve_bicgstab_dev(mf_tiles *t, const double *b, double *x, double tol, int maxiter,
+                          const mf_options *opt, mf_result *res) {
+    return solve_dev(t, 1, b, x, tol, maxiter, opt, res);
+}
+
+static int solve_host(mf_tiles *t, int kind, const double *b, double *x, double tol, int maxiter,
+                      const mf_options *opt, mf_result *res) {
+    if (!t || !b || !x) return MF_ERR_ARG;
+    DevArray<double> db, dx;
+    if (db.alloc(t->rowA) || dx.alloc(t->rowA)) return MF_ERR_NOMEM;
+    MF_CUDA_TRY(cudaMemcpy(db.p, b, sizeof(double) * t->rowA, cudaMemcpyHostToDevice));
+    MF_CUDA_TRY(cudaMemcpy(dx.p, x, sizeof(double) * t->rowA, cudaMemcpyHostToDevice));
+    int rc = solve_dev(t, kind, db.p, dx.p, tol, maxiter, opt, res);
+    if (rc == MF_OK || rc == MF_ERR_NOT_CONVERGED || rc == MF_ERR_BREAKDOWN)
+        MF_CUDA_TRY(cudaMemcpy(x, dx.p, sizeof(double) * t->rowA, cudaMemcpyDeviceToHost));
+    return rc;
+}
+
+int mf_solve_cg(mf_tiles *t, const double *b, double *x, double tol, int maxiter, const mf_options *opt,
+                mf_result *res) {
+    return solve_host(t, 0, b, x, tol, maxiter, opt, res);
+}
+int mf_solve_bicgstab(mf_tiles *t, const double *b, double *x, double tol, int maxiter, const mf_options *opt,
+                      mf_result *res) {
+    return solve_host(t, 1, b, x, tol, maxiter, opt, res);
+}
+
+int mf_true_residual(mf_tiles *t, const double *b, const double *x, double *rel) {
+    if (!t || !b || !x || !rel) return MF_ERR_ARG;
+    int rc = ensure_workspace(t);
+    if (rc) return rc;
+    WsView v = ws_view(t);
+    const size_t n16 = (size_t)t->tilem * 16;
+    MF_CUDA_TRY(cudaMemset(v.x, 0, sizeof(double) * n16));
+    MF_CUDA_TRY(cudaMemcpy(v.x, x, sizeof(double) * t->rowA, cudaMemcpyDeviceToDevice));
+    return true_residual_ws(t, b, v.x, rel);
+}
+
+}  // extern "C"

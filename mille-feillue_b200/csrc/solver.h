@@ -1,0 +1,60 @@
+// Kernel parameter block and host launch entry points of the persistent
+// solver kernels (solver.cu). Host-includable (no device code).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "tiles.h"
+
+namespace mf {
+
+constexpr int NWARPS = 16;                 // compute warps per CTA (2 row blocks each)
+constexpr int NTHREADS = NWARPS * 32;
+constexpr int KMAX_LAYOUTS = 1 + MF_NLEVELS;
+constexpr int FLAG_STRIDE = 8;             // one 32-byte sector per CTA flag
+enum { SYNC_ARRIVE = 0, SYNC_ERROR = 32, SYNC_SITE = 33, SYNC_FLAGS = 64 };
+inline size_t sync_words(int G) { return (size_t)SYNC_FLAGS + (size_t)G * FLAG_STRIDE + 32; }
+
+inline int slab_area_of(int slab_max) { return (slab_max + 127) & ~127; }
+inline int stage_stride_of(int slab_max) { return slab_area_of(slab_max) + XSEG_MAX * 128; }
+
+struct LayoutArgs {
+    const uint8_t *slabs;
+    const uint8_t *head;
+    const int *cta_slab, *cta_rb, *cta_dep;
+};
+
+struct DevResult {
+    int iterations, status, replacements, level_switches, final_layout, pad;
+    double rr, bb;
+};
+
+struct KParams {
+    LayoutArgs lay[KMAX_LAYOUTS];
+    int nlay, start_layout;
+    int stage_stride, slab_area;
+    int rowA, tilem;
+    const int *tile_ptr, *tile_col, *tile_off, *csrptr_off;
+    const uint8_t *ptr;
+    const double *val;
+    const uint8_t *col;
+    uint64_t limit_ns;
+    uint32_t *sync;
+    double *partial;
+    double *x, *r, *d, *q, *s, *t, *rh;
+    const double *b;
+    double tol;
+    int maxiter, fixed_iterations, replace_every;
+    int inject_wait;  // test hook: wait once on a flag that nothing sets
+    double level_rel[KMAX_LAYOUTS];
+    DevResult *res;
+};
+
+int kernel_config(mf_tiles *t, int *G_out);
+void base_params(mf_tiles *t, KParams &P);
+int launch_spmv(mf_tiles *t, int level, const double *x, double *y, int reps, cudaStream_t s);
+int launch_solver(mf_tiles *t, int kind, KParams &P, cudaStream_t s);
+int launch_residual_norms(int n, const double *b, const double *ax, double *out, cudaStream_t s);
+
+}  // namespace mf

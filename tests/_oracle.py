@@ -1,0 +1,272 @@
+"""ctypes bindings of the CPU oracle (oracle/liboracle.so) and of the
+reference's own CPU code compiled unmodified (oracle/_ref/libmfref.so).
+
+Test infrastructure only: the product (libmf.so) never loads these.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libmfref.so")
+
+_i = C.c_int
+_p = C.c_void_p
+
+
+class MfoTiles(C.Structure):
+    _fields_ = [(n, _i) for n in ("rowA", "colA", "tilem", "tilen", "tilenum", "csrsize", "csrptrlen")] + [
+        (n, C.POINTER(C.c_int)) for n in ("tile_ptr", "tile_columnidx", "tile_nnz", "blknnz", "csr_offset", "csrptr_offset")
+    ] + [
+        ("Format", C.POINTER(C.c_char)),
+        ("blknnznnz", C.POINTER(C.c_ubyte)),
+        ("Blockcsr_Val", C.POINTER(C.c_double)),
+        ("Blockcsr_Val_Low", C.POINTER(C.c_float)),
+        ("Tile_csr_Col", C.POINTER(C.c_ubyte)),
+        ("Blockcsr_Ptr", C.POINTER(C.c_ubyte)),
+        ("csr_compressedIdx", C.POINTER(C.c_ubyte)),
+    ]
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(ORACLE_SO)
+        L = _lib
+        L.mfo_tile_create.argtypes = [_i, _i, _p, _p, _p, C.POINTER(MfoTiles)]
+        L.mfo_tiles_free.argtypes = [C.POINTER(MfoTiles)]
+        L.mfo_blockspmv.argtypes = [C.POINTER(MfoTiles), _p, _p, _p, _p, _p]
+        L.mfo_row_compress.argtypes = [C.POINTER(MfoTiles), _p, _p, _p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
+        L.mfo_row_compress.restype = _i
+        L.mfo_balance_twopointer.argtypes = [C.POINTER(MfoTiles), _i, _i, _p, _p, _p, _p]
+        L.mfo_balance_twopointer.restype = _i
+        L.mfo_csr_spmv.argtypes = [_i, _p, _p, _p, _p, _p]
+        L.mfo_dot.argtypes = [_i, _p, _p]
+        L.mfo_dot.restype = C.c_double
+        L.mfo_cg.argtypes = [C.POINTER(MfoTiles), _p, _p, C.c_double, _i, C.POINTER(C.c_double)]
+        L.mfo_cg.restype = _i
+        L.mfo_bicgstab.argtypes = [C.POINTER(MfoTiles), _p, _p, C.c_double, _i, C.POINTER(C.c_double)]
+        L.mfo_bicgstab.restype = _i
+        L.mfo_fp8_e4m3_encode.argtypes = [C.c_double]
+        L.mfo_fp8_e4m3_encode.restype = C.c_uint8
+        L.mfo_fp8_e4m3_decode.argtypes = [C.c_uint8]
+        L.mfo_fp8_e4m3_decode.restype = C.c_double
+        L.mfo_fp16_encode.argtypes = [C.c_double]
+        L.mfo_fp16_encode.restype = C.c_uint16
+        L.mfo_fp16_decode.argtypes = [C.c_uint16]
+        L.mfo_fp16_decode.restype = C.c_double
+        L.mfo_tile_scale.argtypes = [_i, C.c_double]
+        L.mfo_tile_scale.restype = C.c_double
+        L.mfo_mixed_spmv.argtypes = [C.POINTER(MfoTiles), _p, _p, _p]
+        L.mfo_mlp_forward.argtypes = [_p] * 7 + [_i, _p]
+        L.mfo_mlp_forward.restype = C.c_float
+        L.mfo_mlp_grad.argtypes = [_p] * 8 + [_i] + [_p] * 6
+        L.mfo_mlp_grad.restype = C.c_float
+    return _lib
+
+
+def ref_available():
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        _ref = C.CDLL(REF_SO)
+        R = _ref
+        R.ref_tile_create.argtypes = [_i, _i, _i, _p, _p, _p]
+        R.ref_tile_create.restype = _p
+        R.ref_tile_sizes.argtypes = [_p, _p]
+        R.ref_tile_array.argtypes = [_p, C.c_char_p, _p]
+        R.ref_tile_array.restype = _i
+        R.ref_blockspmv.argtypes = [_p, _p, _p, _p, _p, _p, _i]
+        R.ref_tile_free.argtypes = [_p]
+        R.ref_read_mtx.argtypes = [C.c_char_p, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i),
+                                   C.POINTER(C.POINTER(_i)), C.POINTER(C.POINTER(_i)), C.POINTER(C.POINTER(C.c_double))]
+        R.ref_read_mtx.restype = _i
+        R.ref_free.argtypes = [_p]
+    return _ref
+
+
+ARRAY_SPECS = {
+    # name: (dtype, length key)
+    "tile_ptr": (np.int32, "tilem+1"),
+    "tile_columnidx": (np.int32, "tilenum"),
+    "tile_nnz": (np.int32, "tilenum+1"),
+    "blknnz": (np.int32, "tilenum+1"),
+    "csr_offset": (np.int32, "tilenum+1"),
+    "csrptr_offset": (np.int32, "tilenum+1"),
+    "Format": (np.int8, "tilenum"),
+    "blknnznnz": (np.uint8, "tilenum+1"),
+    "Blockcsr_Val": (np.float64, "csrsize"),
+    "Blockcsr_Val_Low": (np.float32, "csrsize"),
+    "Tile_csr_Col": (np.uint8, "csrsize"),
+    "Blockcsr_Ptr": (np.uint8, "csrptrlen"),
+    "csr_compressedIdx": (np.uint8, "csrhalf"),
+}
+
+
+def _length(key, s):
+    return {
+        "tilem+1": s["tilem"] + 1,
+        "tilenum": s["tilenum"],
+        "tilenum+1": s["tilenum"] + 1,
+        "csrsize": s["csrsize"],
+        "csrptrlen": s["csrptrlen"],
+        "csrhalf": (s["csrsize"] + 1) // 2,
+    }[key]
+
+
+class OracleTiles:
+    """Tile_create restated by the oracle (mfo_tile_create)."""
+
+    def __init__(self, rowA, colA, rp, ci, val):
+        self.rp = np.ascontiguousarray(rp, np.int32)
+        self.ci = np.ascontiguousarray(ci, np.int32)
+        self.val = np.ascontiguousarray(val, np.float64)
+        self.t = MfoTiles()
+        rc = lib().mfo_tile_create(rowA, colA, _ptr(self.rp), _ptr(self.ci), _ptr(self.val), C.byref(self.t))
+        assert rc == 0
+        self.sizes = {k: getattr(self.t, k) for k in ("rowA", "colA", "tilem", "tilen", "tilenum", "csrsize", "csrptrlen")}
+
+    def array(self, name):
+        dt, key = ARRAY_SPECS[name]
+        n = _length(key, self.sizes)
+        p = getattr(self.t, name)
+        raw = C.cast(p, C.POINTER(C.c_ubyte))
+        buf = C.string_at(raw, n * np.dtype(dt).itemsize) if n > 0 else b""
+        return np.frombuffer(buf, dtype=dt).copy()
+
+    def arrays(self):
+        return {k: self.array(k) for k in ARRAY_SPECS}
+
+    def spmv(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros(self.sizes["rowA"], np.float64)
+        lib().mfo_blockspmv(C.byref(self.t), _ptr(x), _ptr(y), None, None, None)
+        return y
+
+    def offsets(self):
+        n = self.sizes["tilenum"]
+        p1 = np.zeros(max(n, 1), np.int32)
+        p2 = np.zeros(max(n, 1), np.int32)
+        rbb = np.zeros(1, np.int32)
+        lib().mfo_blockspmv(C.byref(self.t), None, None, _ptr(p1), _ptr(p2), _ptr(rbb))
+        return p1[:n], p2[:n], int(rbb[0])
+
+    def mixed_spmv(self, prec, x):
+        x = np.ascontiguousarray(x, np.float64)
+        prec = np.ascontiguousarray(prec, np.uint8)
+        y = np.zeros(self.sizes["rowA"], np.float64)
+        lib().mfo_mixed_spmv(C.byref(self.t), _ptr(prec), _ptr(x), _ptr(y))
+        return y
+
+    def row_compress(self):
+        s = self.sizes
+        nz = np.zeros(s["tilenum"] + 1, np.int32)
+        tr = np.zeros(max(s["tilenum"], 1), np.int32)
+        bs = np.zeros(s["tilem"] + 1, np.int32)
+        a = C.c_void_p()
+        b = C.c_void_p()
+        cnt = lib().mfo_row_compress(C.byref(self.t), _ptr(nz), _ptr(tr), _ptr(bs), C.byref(a), C.byref(b))
+        rid = np.frombuffer(C.string_at(a, cnt + 1), np.uint8).copy()
+        rpn = np.frombuffer(C.string_at(b, cnt + 1), np.uint8).copy()
+        C.CDLL(None).free.argtypes = [_p]
+        C.CDLL(None).free(a)
+        C.CDLL(None).free(b)
+        return dict(nonzero_row_new=nz, tile_rowidx=tr[: s["tilenum"]], block_signal=bs,
+                    blockrowid_new=rid, blockcsr_ptr_new=rpn)
+
+    def balance(self, block_nnz, block_per_warp=180):
+        n = self.sizes["tilenum"]
+        idx = lib().mfo_balance_twopointer(C.byref(self.t), block_nnz, block_per_warp, None, None, None, None)
+        bp = np.zeros(idx + 1, np.int32)
+        a = np.zeros(n + 1, np.int32)
+        b = np.zeros(n + 1, np.int32)
+        c = np.zeros(n + 1, np.int32)
+        idx2 = lib().mfo_balance_twopointer(C.byref(self.t), block_nnz, block_per_warp, _ptr(bp), _ptr(a), _ptr(b), _ptr(c))
+        assert idx2 == idx
+        return idx, bp, a, b, c
+
+    def cg(self, b, tol, maxiter, x0=None):
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(self.sizes["rowA"]) if x0 is None else np.array(x0, np.float64)
+        rel = C.c_double()
+        it = lib().mfo_cg(C.byref(self.t), _ptr(b), _ptr(x), tol, maxiter, C.byref(rel))
+        return it, x, rel.value
+
+    def bicgstab(self, b, tol, maxiter, x0=None):
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(self.sizes["rowA"]) if x0 is None else np.array(x0, np.float64)
+        rel = C.c_double()
+        it = lib().mfo_bicgstab(C.byref(self.t), _ptr(b), _ptr(x), tol, maxiter, C.byref(rel))
+        return it, x, rel.value
+
+    def __del__(self):
+        try:
+            lib().mfo_tiles_free(C.byref(self.t))
+        except Exception:
+            pass
+
+
+class RefTiles:
+    """Tile_create of the reference itself (oracle/_ref/libmfref.so)."""
+
+    def __init__(self, rowA, colA, rp, ci, val):
+        self.rp = np.ascontiguousarray(rp, np.int32)
+        self.ci = np.ascontiguousarray(ci, np.int32)
+        self.val = np.ascontiguousarray(val, np.float64)
+        self.h = ref().ref_tile_create(rowA, colA, int(self.rp[rowA]), _ptr(self.rp), _ptr(self.ci), _ptr(self.val))
+        s = np.zeros(7, np.int32)
+        ref().ref_tile_sizes(self.h, _ptr(s))
+        self.sizes = dict(zip(("tilem", "tilen", "tilenum", "csrsize", "csrptrlen", "rowA", "colA"), map(int, s)))
+
+    def array(self, name):
+        dt, key = ARRAY_SPECS[name]
+        n = _length(key, self.sizes)
+        a = np.zeros(max(n, 1), dt)
+        assert ref().ref_tile_array(self.h, name.encode(), _ptr(a)) == 0
+        return a[:n]
+
+    def arrays(self):
+        return {k: self.array(k) for k in ARRAY_SPECS}
+
+    def spmv(self, x, fill_compressed=True):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros(self.sizes["tilem"] * 16, np.float64)
+        n = self.sizes["tilenum"]
+        p1 = np.zeros(max(n, 1), np.int32)
+        p2 = np.zeros(max(n, 1), np.int32)
+        rbb = np.zeros(1, np.int32)
+        ref().ref_blockspmv(self.h, _ptr(x), _ptr(y), _ptr(p1), _ptr(p2), _ptr(rbb), 1 if fill_compressed else 0)
+        return y[: self.sizes["rowA"]], p1[:n], p2[:n], int(rbb[0])
+
+    def __del__(self):
+        try:
+            ref().ref_tile_free(self.h)
+        except Exception:
+            pass
+
+
+def ref_read_mtx(path):
+    m, n, nnz = _i(), _i(), _i()
+    rp = C.POINTER(_i)()
+    ci = C.POINTER(_i)()
+    va = C.POINTER(C.c_double)()
+    ref().ref_read_mtx(path.encode(), C.byref(m), C.byref(n), C.byref(nnz), C.byref(rp), C.byref(ci), C.byref(va))
+    R = np.ctypeslib.as_array(rp, shape=(m.value + 1,)).copy()
+    CI = np.ctypeslib.as_array(ci, shape=(nnz.value,)).copy()
+    V = np.ctypeslib.as_array(va, shape=(nnz.value,)).copy()
+    for p in (rp, ci, va):
+        ref().ref_free(C.cast(p, _p))
+    return m.value, n.value, R, CI, V

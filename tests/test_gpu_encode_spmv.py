@@ -1,0 +1,143 @@
+"""GPU encoder and tiled SpMV parity against the oracle and the golden
+fixtures made from the reference's own code. Integer/byte arrays and the
+FP64 SpMV must be bit-exact."""
+import numpy as np
+import pytest
+
+from _oracle import ARRAY_SPECS
+
+pytestmark = pytest.mark.gpu
+
+DERIVED = ("nonzero_row_new", "tile_rowidx", "block_signal", "blockrowid_new", "blockcsr_ptr_new")
+
+
+def _random(n, per_row, seed, unsorted=True, dense_rows=()):
+    rng = np.random.default_rng(seed)
+    rp, ci, va = [0], [], []
+    for r in range(n):
+        cols = set(rng.integers(0, n, size=int(rng.integers(0, per_row + 1))).tolist())
+        cols.add(r)
+        if r in dense_rows:
+            cols |= set(range(n))
+        cols = sorted(cols)
+        if unsorted:
+            rng.shuffle(cols)
+        ci += cols
+        va += rng.standard_normal(len(cols)).tolist()
+        rp.append(len(ci))
+    return np.array(rp, np.int32), np.array(ci, np.int32), np.array(va)
+
+
+def _with_empty_rows(n, seed):
+    rp, ci, va = _random(n, 5, seed)
+    keep = np.ones(n, bool)
+    keep[::7] = False  # empty rows
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    m = keep[rows]
+    counts = np.bincount(rows[m], minlength=n)
+    return np.concatenate([[0], np.cumsum(counts)]).astype(np.int32), ci[m], va[m]
+
+
+def _cases(mf):
+    A = mf.Matrix.poisson2d(256)
+    B = mf.Matrix.convdiff3d(64)
+    C = mf.Matrix.varpoisson3d(32)
+    D = mf.Matrix.spd_random(20000, 5)
+    out = {"poisson2d_256": (A.n, *A.csr()), "convdiff3d_64": (B.n, *B.csr()),
+           "varpoisson3d_32": (C.n, *C.csr()), "spd_random_20000": (D.n, *D.csr())}
+    out["random_5000_unsorted"] = (5000, *_random(5000, 20, 1))
+    out["dense_rows_4000"] = (4000, *_random(4000, 3, 2, dense_rows=(5, 6, 7, 3000)))  # >2048 per row block
+    out["empty_rows_1001"] = (1001, *_with_empty_rows(1001, 3))
+    return out
+
+
+@pytest.fixture(scope="module")
+def cases(mf):
+    return _cases(mf)
+
+
+def test_encoder_matches_golden(mf, golden):
+    for case, g in golden.items():
+        rowA, n = map(int, g["rowA"])
+        rp = g["row_ptr"][: rowA + 1]
+        nnz = int(rp[rowA])
+        t = mf.Tiles(csr=(rowA, n, rp, g["col_idx"][:nnz], g["val"][:nnz]))
+        ex = t.export()
+        for name in ARRAY_SPECS:
+            assert np.array_equal(ex[name], g[name]), (case, name)
+        assert np.array_equal(ex["ptroffset1"], g["ptroffset1"]) and np.array_equal(ex["ptroffset2"], g["ptroffset2"])
+        if rowA == n:
+            assert np.array_equal(t.spmv(g["x"]), g["y"]), case
+
+
+def test_encoder_matches_oracle(mf, O, cases):
+    for name, (n, rp, ci, v) in cases.items():
+        t = mf.Tiles(csr=(n, n, rp, ci, v))
+        o = O.OracleTiles(n, n, rp, ci, v)
+        ex = t.export()
+        for k in ARRAY_SPECS:
+            assert np.array_equal(ex[k], o.array(k)), (name, k)
+        rc = o.row_compress()
+        for k in DERIVED:
+            assert np.array_equal(ex[k], rc[k]), (name, k)
+        p1, p2, _ = o.offsets()
+        assert np.array_equal(ex["ptroffset1"], p1) and np.array_equal(ex["ptroffset2"], p2), name
+
+
+def test_spmv_bitexact_vs_oracle(mf, O, cases):
+    rng = np.random.default_rng(0)
+    for name, (n, rp, ci, v) in cases.items():
+        t = mf.Tiles(csr=(n, n, rp, ci, v))
+        o = O.OracleTiles(n, n, rp, ci, v)
+        for _ in range(2):
+            x = rng.standard_normal(n) * 10.0 ** rng.uniform(-3, 3, n)
+            y = t.spmv(x)
+            assert np.array_equal(y, o.spmv(x)), name
+
+
+@pytest.mark.parametrize("slab_bytes,rb_per_slab", [(2048, 1), (4096, 3), (16384, 8), (0, 0)])
+def test_spmv_small_slabs_and_fallback_modes(mf, O, cases, slab_bytes, rb_per_slab):
+    """Tiny stages force many slabs per CTA, the gather mode and the
+    oversize (global-memory) path; results stay bit-exact."""
+    rng = np.random.default_rng(1)
+    for name in ("poisson2d_256", "spd_random_20000", "dense_rows_4000", "empty_rows_1001"):
+        n, rp, ci, v = cases[name]
+        opts = mf.options(slab_bytes=slab_bytes, rb_per_slab=rb_per_slab)
+        t = mf.Tiles(csr=(n, n, rp, ci, v), opts=opts)
+        o = O.OracleTiles(n, n, rp, ci, v)
+        x = rng.standard_normal(n)
+        assert np.array_equal(t.spmv(x), o.spmv(x)), (name, slab_bytes)
+
+
+@pytest.mark.parametrize("prec", [1, 2, 3])
+def test_low_precision_spmv_bitexact_vs_oracle(mf, O, cases, prec):
+    rng = np.random.default_rng(2)
+    for name in ("poisson2d_256", "varpoisson3d_32", "spd_random_20000", "dense_rows_4000"):
+        n, rp, ci, v = cases[name]
+        t = mf.Tiles(csr=(n, n, rp, ci, v), opts=mf.options(precision_mode=mf.MODE_FIXED, fixed_precision=prec))
+        o = O.OracleTiles(n, n, rp, ci, v)
+        x = rng.standard_normal(n)
+        import torch
+
+        xd = torch.tensor(x, device="cuda")
+        yd = torch.zeros(n, dtype=torch.float64, device="cuda")
+        t.spmv_level_dev(0, xd.data_ptr(), yd.data_ptr())
+        y = yd.cpu().numpy()
+        p, _ = t.precisions()
+        yo = o.mixed_spmv(p, x)
+        assert np.array_equal(y, yo), (name, prec, np.max(np.abs(y - yo)))
+
+
+def test_spmv_full_size_varpoisson_128(mf, O):
+    A = mf.Matrix.varpoisson3d(128)
+    n = A.n
+    rp, ci, v = A.csr()
+    t = mf.Tiles(A)
+    inf = t.info()
+    assert (inf["tilem"], inf["tilenum"]) == (131072, 880640)
+    x = A.xstar()
+    y = t.spmv(x)
+    # b = A x* in CSR order differs from the tiled order only by rounding
+    assert np.allclose(y, A.b(), rtol=1e-12, atol=1e-9)
+    o = O.OracleTiles(n, n, rp, ci, v)
+    assert np.array_equal(y, o.spmv(x))

@@ -1,0 +1,126 @@
+"""Persistent-kernel CG / BiCGSTAB against the CPU oracle's restatement of
+the reference recurrences (iteration counts within +-2 %) and against the
+1e-10 true relative residual."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _csr_mat(rp, ci, v, n):
+    import scipy.sparse as sp
+
+    return sp.csr_matrix((v, ci, rp), shape=(n, n))
+
+
+@pytest.mark.parametrize("maker", ["poisson2d_128", "varpoisson3d_16", "varpoisson3d_24", "spd_random_30000"])
+def test_cg_iterations_match_oracle(mf, O, maker):
+    kind, size = maker.rsplit("_", 1)
+    size = int(size)
+    A = {"poisson2d": lambda: mf.Matrix.poisson2d(size), "varpoisson3d": lambda: mf.Matrix.varpoisson3d(size),
+         "spd_random": lambda: mf.Matrix.spd_random(size, 9)}[kind]()
+    n = A.n
+    rp, ci, v = A.csr()
+    b = A.b()
+    t = mf.Tiles(A)
+    x, res = t.solve_cg(b, tol=1e-10, maxiter=20000)
+    o = O.OracleTiles(n, n, rp, ci, v)
+    it_o, x_o, rel_o = o.cg(b, 1e-10, 20000)
+    assert res["status"] == 0, res
+    assert abs(res["iterations"] - it_o) <= max(2, 0.02 * it_o), (res["iterations"], it_o)
+    M = _csr_mat(rp, ci, v, n)
+    true_rel = np.linalg.norm(b - M @ x) / np.linalg.norm(b)
+    assert true_rel <= 1.5e-10 and abs(true_rel - res["rel_residual_true"]) <= 1e-3 * true_rel + 1e-16
+    assert np.linalg.norm(x - x_o) / np.linalg.norm(x_o) < 1e-6
+
+
+@pytest.mark.parametrize("N", [12, 24])
+def test_bicgstab_iterations_match_oracle(mf, O, N):
+    A = mf.Matrix.convdiff3d(N)
+    n = A.n
+    rp, ci, v = A.csr()
+    b = A.b()
+    t = mf.Tiles(A)
+    x, res = t.solve_bicgstab(b, tol=1e-10, maxiter=5000)
+    o = O.OracleTiles(n, n, rp, ci, v)
+    it_o, x_o, rel_o = o.bicgstab(b, 1e-10, 5000)
+    assert res["status"] == 0, res
+    assert abs(res["iterations"] - it_o) <= max(2, 0.02 * it_o), (res["iterations"], it_o)
+    M = _csr_mat(rp, ci, v, n)
+    assert np.linalg.norm(b - M @ x) / np.linalg.norm(b) <= 1.5e-10
+
+
+def test_cg_full_size_varpoisson_128(mf):
+    """Config of the headline metric: 128^3 variable-coefficient Poisson,
+    x0 = 0, FP64, to a 1e-10 true relative residual."""
+    A = mf.Matrix.varpoisson3d(128)
+    b = A.b()
+    t = mf.Tiles(A)
+    x, res = t.solve_cg(b, tol=1e-10, maxiter=40000)
+    assert res["status"] == 0, res
+    assert res["rel_residual_true"] <= 1.2e-10, res
+    xs = A.xstar()
+    assert np.linalg.norm(x - xs) / np.linalg.norm(xs) < 1e-4
+
+
+def test_bicgstab_full_size_convdiff_64(mf):
+    A = mf.Matrix.convdiff3d(64)
+    t = mf.Tiles(A)
+    x, res = t.solve_bicgstab(A.b(), tol=1e-10, maxiter=5000)
+    assert res["status"] == 0 and res["rel_residual_true"] <= 1.5e-10, res
+
+
+def test_fixed_iteration_count_mode(mf):
+    A = mf.Matrix.poisson2d(64)
+    t = mf.Tiles(A)
+    x, res = t.solve_cg(A.b(), tol=1e-10, maxiter=10000, opts=mf.options(fixed_iterations=100))
+    assert res["iterations"] == 100
+
+
+def test_nonzero_initial_guess(mf):
+    A = mf.Matrix.poisson2d(100)
+    b = A.b()
+    t = mf.Tiles(A)
+    x0 = np.full(A.n, 0.5)
+    x, res = t.solve_cg(b, x0=x0, tol=1e-10)
+    assert res["status"] == 0 and res["rel_residual_true"] <= 1.5e-10
+    assert np.allclose(x, 1.0, atol=1e-6)
+
+
+def test_dropin_cg_solve_inc(mf):
+    A = mf.Matrix.poisson2d(90)  # 8100 rows: truncated to 8096 as the reference does
+    rp, ci, v = A.csr()
+    n = A.n
+    nt = (n // 16) * 16
+    xt = np.ones(nt)
+    import scipy.sparse as sp
+
+    M = sp.csr_matrix((v, ci, rp), shape=(n, n))[:nt, :nt]
+    b = M @ xt
+    x = np.zeros(n)
+    it = mf.cg_solve_inc(rp, ci, v, x, np.concatenate([b, np.zeros(n - nt)]), nt, maxiter=10000, threshold=1e-10)
+    assert it > 0
+    assert np.linalg.norm(b - M @ x[:nt]) / np.linalg.norm(b) <= 1.5e-10
+
+
+def test_dropin_bicgstab(mf):
+    A = mf.Matrix.convdiff3d(10)
+    rp, ci, v = A.csr()
+    n = A.n
+    rhs = np.ones(n)
+    x = np.zeros(n)
+    assert mf.bicgstab(rp, ci, v, rhs, x, n) == 0
+    assert np.allclose(rhs[: (n // 16) * 16], np.add.reduceat(v, rp[:-1])[: (n // 16) * 16])
+
+
+def test_bounded_wait_times_out_and_context_survives(mf):
+    A = mf.Matrix.poisson2d(64)
+    t = mf.Tiles(A)
+    o = mf.options(timeout_s=0.05)
+    o.reserved[0] = 0x5741
+    with pytest.raises(mf.MfError) as e:
+        t.solve_cg(A.b(), opts=o)
+    assert e.value.status == mf.MF_ERR_TIMEOUT
+    # the context is still usable
+    x, res = t.solve_cg(A.b(), tol=1e-10)
+    assert res["status"] == 0

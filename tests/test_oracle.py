@@ -1,0 +1,141 @@
+"""The CPU oracle is pinned against the reference's own code: the golden
+fixtures (made by tests/golden/make_golden.py from Tile_create and
+blockspmv_cpu compiled unmodified) and, where the reference tree exists,
+a live run of that code."""
+import numpy as np
+import pytest
+
+from _oracle import ARRAY_SPECS
+
+
+def test_oracle_matches_golden_tile_arrays(O, golden):
+    for case, g in golden.items():
+        rowA, n = map(int, g["rowA"])
+        o = O.OracleTiles(rowA, n, g["row_ptr"], g["col_idx"], g["val"])
+        for name in ARRAY_SPECS:
+            assert np.array_equal(o.array(name), g[name]), (case, name)
+        y = o.spmv(g["x"])
+        assert np.array_equal(y, g["y"]), case  # bit-exact summation order
+        p1, p2, rbb = o.offsets()
+        assert np.array_equal(p1, g["ptroffset1"]) and np.array_equal(p2, g["ptroffset2"]), case
+        assert rbb == int(g["rowblkblock"][0]), case
+
+
+def _sym_random(n, seed):
+    rng = np.random.default_rng(seed)
+    import scipy.sparse as sp
+
+    A = sp.random(n, n, density=min(1.0, 8.0 / n), random_state=seed, format="csr")
+    A = (A + A.T + sp.identity(n) * 20).tocsr()
+    A.sort_indices()
+    return A
+
+
+@pytest.mark.parametrize("n,seed", [(512, 0), (1000, 1), (4096, 2)])
+def test_oracle_matches_reference_live(O, n, seed):
+    if not O.ref_available():
+        pytest.skip("reference harness not built (reference tree absent)")
+    A = _sym_random(n, seed)
+    o = O.OracleTiles(n, n, A.indptr, A.indices, A.data)
+    r = O.RefTiles(n, n, A.indptr, A.indices, A.data)
+    for name in ARRAY_SPECS:
+        assert np.array_equal(o.array(name), r.array(name)), name
+    x = np.random.default_rng(seed).standard_normal(n)
+    assert np.array_equal(o.spmv(x), r.spmv(x)[0])
+
+
+def test_reference_blockspmv_needs_nibble_columns(O, golden):
+    """As shipped, blockspmv_cpu reads csr_compressedIdx, which Tile_create
+    never fills; it is then exact only for x constant on each 16-segment.
+    The oracle uses Tile_csr_Col (what the reference GPU kernels read)."""
+    if not O.ref_available():
+        pytest.skip("reference harness not built")
+    g = golden["poisson2d_32"]
+    rowA, n = map(int, g["rowA"])
+    r = O.RefTiles(rowA, n, g["row_ptr"], g["col_idx"], g["val"])
+    ones = np.ones(n)
+    y0, *_ = r.spmv(ones, fill_compressed=False)
+    o = O.OracleTiles(rowA, n, g["row_ptr"], g["col_idx"], g["val"])
+    assert np.array_equal(y0, o.spmv(ones))
+
+
+def test_oracle_cg_converges_and_matches_scipy(O):
+    import scipy.sparse as sp
+
+    A = _sym_random(2000, 3)
+    b = np.random.default_rng(3).standard_normal(2000)
+    o = O.OracleTiles(2000, 2000, A.indptr, A.indices, A.data)
+    it, x, rel = O.OracleTiles.cg(o, b, 1e-10, 5000)
+    assert rel <= 1e-10
+    assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) < 1e-9
+    assert it > 5
+
+
+def test_oracle_bicgstab_nonsymmetric(O):
+    import scipy.sparse as sp
+
+    rng = np.random.default_rng(4)
+    A = sp.random(1500, 1500, density=0.004, random_state=4, format="csr") + sp.identity(1500) * 4
+    A = A.tocsr()
+    A.sort_indices()
+    b = rng.uniform(-1, 1, 1500)
+    o = O.OracleTiles(1500, 1500, A.indptr, A.indices, A.data)
+    it, x, rel = o.bicgstab(b, 1e-10, 5000)
+    assert rel <= 1e-10
+    assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) < 1e-9
+
+
+def test_fp8_e4m3_encoding_spec(O):
+    L = O.lib()
+    # every code decodes and re-encodes to itself (except NaN)
+    for code in range(256):
+        v = L.mfo_fp8_e4m3_decode(code)
+        if np.isnan(v):
+            assert (code & 0x7F) == 0x7F
+            continue
+        enc = L.mfo_fp8_e4m3_encode(v)
+        if v == 0.0:
+            assert enc in (0x00, 0x80)
+        else:
+            assert enc == code, (code, v, enc)
+    assert L.mfo_fp8_e4m3_decode(0x7E) == 448.0
+    assert L.mfo_fp8_e4m3_encode(1e9) == 0x7E  # saturating
+    assert L.mfo_fp8_e4m3_decode(0x01) == 2.0 ** -9
+    # ties to even: 1 + 1/16 lies halfway between 1 and 1.125
+    assert L.mfo_fp8_e4m3_decode(L.mfo_fp8_e4m3_encode(1.0625)) == 1.0
+    assert L.mfo_fp8_e4m3_decode(L.mfo_fp8_e4m3_encode(1.1875)) == 1.25
+
+
+def test_fp16_encoding_matches_numpy(O):
+    L = O.lib()
+    rng = np.random.default_rng(0)
+    vals = np.concatenate([rng.standard_normal(2000) * 10.0 ** rng.integers(-8, 5, 2000), [65504.0, 6e-8, 1e-9]])
+    for v in vals:
+        h = L.mfo_fp16_encode(float(v))
+        assert h == int(np.float16(v).view(np.uint16)), v
+
+
+def test_two_pointer_balance_small_case(O):
+    # 6 tiles with nnz [4, 1, 1, 1, 1, 4]: block_nnz 6, block_per_warp 180.
+    # i=0 (4) joins; j=5: 4+4>=6 closes unit 1 with tiles {0,5};
+    # i=1 (1) joins; j=4 (1) joins; i=2, j=3 (1,1) join -> last unit {1,4,2,3}.
+    n = 96
+    rp = [0]
+    ci, va = [], []
+    pattern = {0: [0, 1, 2, 3], 1: [4], 2: [5], 3: [5], 4: [5], 5: [5]}
+    # one row block; tile k has the listed nnz in distinct column blocks
+    entries = [(0, 0), (1, 0), (2, 0), (3, 0), (0, 16), (0, 32), (0, 48), (0, 64), (0, 80), (1, 80), (2, 80), (3, 80)]
+    rows = {}
+    for r, c in entries:
+        rows.setdefault(r, []).append(c)
+    for r in range(n):
+        for c in sorted(rows.get(r, [])):
+            ci.append(c)
+            va.append(1.0)
+        rp.append(len(ci))
+    o = O.OracleTiles(16, n, np.array(rp[:17]), np.array(ci), np.array(va))
+    idx, bp, a, b, c = o.balance(6, 180)
+    assert list(o.array("blknnz")) == [0, 4, 5, 6, 7, 8, 12]
+    assert idx == 2
+    assert list(bp) == [0, 2, 6]
+    assert list(a[:6]) == [0, 5, 1, 4, 2, 3]
