@@ -67,7 +67,7 @@ typedef struct {
     int replace_every;       /* true-residual replacement period of the mixed
                                 precision modes (FP64 mode never replaces)    */
     int ctas_per_sm;         /* persistent CTAs per SM, 0 = autotune           */
-    int rb_per_slab;         /* row blocks per slab, 0 = default (32)          */
+    int rb_per_slab;         /* row blocks per slab, 0 = default (30)          */
     int slab_bytes;          /* max bytes of one streamed slab, 0 = default    */
     double timeout_s;        /* limit of every device spin-wait, 0 = 2 s       */
     int check_true_residual; /* confirm convergence with b - A x (default 1)   */

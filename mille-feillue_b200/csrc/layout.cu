@@ -1,12 +1,13 @@
-// Slab layout of the persistent solver.
+// Slab layout of the persistent solver (row-sliced planes, see tiles.h).
 //
 // The row blocks are split into G contiguous CTA ranges of equal cost (slab
 // bytes + per-row vector work), and each range into slabs: consecutive row
 // blocks whose encoded bytes fit one shared-memory stage and whose distinct
 // x segments (16-entry pieces of the input vector) fit the x stage as at
-// most MAXRUNS contiguous runs. The planner runs on the host over the tile
-// column indices; the slab bytes themselves are written on the GPU from the
-// encoder's tile arrays.
+// most MAXRUNS contiguous runs. Row-block sizes and plane precisions are
+// computed on the GPU from the encoder's tile arrays; the host plans the
+// slabs over those sizes and the tile columns; the slab bytes are written on
+// the GPU.
 #include <cuda_fp16.h>
 #include <cuda_fp8.h>
 #include <cuda_runtime.h>
@@ -24,29 +25,197 @@ namespace mf {
 namespace {
 
 struct SlabPlan {
-    int rb0, nrb, ntiles, t0, nnz, mode;
-    uint32_t valbytes, bytes, off16;
+    int rb0, nrb, ntiles, mode;
+    uint32_t bytes, off16;
     int seg_off, nseg;  // unique sorted x segments (staged mode)
     int run_off, nruns;
 };
 
+struct TileArgs {
+    const int *tile_ptr, *tile_col, *tile_off, *csrptr_off;
+    const unsigned char *bptr;
+    const double *val;
+    const unsigned char *col;
+    const unsigned char *prec;
+    const float *scale;
+    int tilem, rowA;
+};
+
+// Walks the entries of row r of row block rb in the reference's order
+// (tiles ascending, CSR order inside the tile).
+struct RowCursor {
+    int t, t1;   // current tile, end tile
+    int q, qe;   // current entry index, end (absolute in val/col)
+    int r, rl;
+};
+
+__device__ __forceinline__ void row_range(const TileArgs &A, int t, int r, int rl, int &s, int &e) {
+    const int base = A.tile_off[t];
+    const int nk = A.tile_off[t + 1] - base;
+    const int cc = A.csrptr_off[t];
+    s = base + A.bptr[cc + r];
+    e = base + (r + 1 < rl ? (int)A.bptr[cc + r + 1] : nk);
+}
+
+__device__ __forceinline__ void cursor_skip_empty(const TileArgs &A, RowCursor &c) {
+    while (c.q >= c.qe && c.t < c.t1) {
+        ++c.t;
+        if (c.t < c.t1) row_range(A, c.t, c.r, c.rl, c.q, c.qe);
+    }
+}
+
+__device__ __forceinline__ void cursor_init(const TileArgs &A, RowCursor &c, int rb, int r) {
+    c.r = r;
+    c.rl = rb == A.tilem - 1 ? A.rowA - (A.tilem - 1) * 16 : 16;
+    c.t = A.tile_ptr[rb];
+    c.t1 = A.tile_ptr[rb + 1];
+    c.q = c.qe = 0;
+    if (r < c.rl && c.t < c.t1) {
+        row_range(A, c.t, r, c.rl, c.q, c.qe);
+        cursor_skip_empty(A, c);
+    } else {
+        c.t = c.t1;
+    }
+}
+
+__device__ __forceinline__ bool cursor_valid(const RowCursor &c) { return c.t < c.t1 && c.q < c.qe; }
+
+__device__ __forceinline__ void cursor_next(const TileArgs &A, RowCursor &c) {
+    ++c.q;
+    cursor_skip_empty(A, c);
+}
+
+__device__ __forceinline__ int scale_exp(float s) {
+    int e;
+    frexpf(s, &e);
+    return e - 1;  // s = 2^(e-1) for a power of two
+}
+
+// Storage precision and scale of one plane from its entries' tile
+// precisions / scales (warp-wide; lanes without an entry pass prec = -1).
+// Every stored value keeps the exact dequantized value of its tile.
+__device__ void plane_format(int prec, float scale, int &pprec, float &pscale) {
+    const unsigned full = 0xffffffffu;
+    const bool has = prec >= 0;
+    const bool any64 = __any_sync(full, has && prec == MF_PREC_FP64);
+    const bool any32 = __any_sync(full, has && prec == MF_PREC_FP32);
+    const bool any16 = __any_sync(full, has && prec == MF_PREC_FP16);
+    const bool anyl = __any_sync(full, has);
+    pscale = 1.0f;
+    if (!anyl || any64) {
+        pprec = MF_PREC_FP64;
+        return;
+    }
+    if (any32) {
+        pprec = MF_PREC_FP32;
+        return;
+    }
+    const int e = has ? scale_exp(scale) + 1024 : 1 << 20;
+    const int emin = (int)__reduce_min_sync(full, (unsigned)e);
+    const int emax = (int)__reduce_max_sync(full, has ? (unsigned)e : 0u);
+    if (emin == emax) {
+        pprec = any16 ? MF_PREC_FP16 : MF_PREC_FP8;
+        pscale = ldexpf(1.0f, emin - 1024);
+    } else if (!any16 && emax - emin <= 7) {
+        pprec = MF_PREC_FP16;
+        pscale = ldexpf(1.0f, emin - 1024);
+    } else {
+        pprec = MF_PREC_FP32;
+    }
+}
+
+// Dequantized value of entry q of tile t (FP64 tiles: the value itself).
+__device__ __forceinline__ double dequant(const TileArgs &A, int t, int q) {
+    const int p = A.prec[t];
+    const double v = A.val[q];
+    if (p == MF_PREC_FP64) return v;
+    if (p == MF_PREC_FP32) return (double)__double2float_rn(v);
+    const double s = (double)A.scale[t];
+    const double inv = 1.0 / s;
+    if (p == MF_PREC_FP16) return (double)__half2float(__double2half(v * inv)) * s;
+    const __nv_fp8_storage_t b = __nv_cvt_double_to_fp8(v * inv, __NV_SATFINITE, __NV_E4M3);
+    return (double)__half2float(__half(__nv_cvt_fp8_to_halfraw(b, __NV_E4M3))) * s;
+}
+
+// Power-of-two scale of every FP16 / FP8 tile (1 for the others).
+__global__ void k_tile_scales(int tilenum, const int *tile_off, const double *val, const unsigned char *prec,
+                              float *scale) {
+    const int lane = threadIdx.x & 31;
+    const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (t >= tilenum) return;
+    const int vo = tile_off[t], nk = tile_off[t + 1] - vo;
+    double mx = 0.0;
+    for (int k = lane; k < nk; k += 32) mx = fmax(mx, fabs(val[vo + k]));
+    for (int d = 16; d > 0; d >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, d));
+    if (lane) return;
+    const int p = prec[t];
+    double s = 1.0;
+    if (p >= MF_PREC_FP16 && mx > 0.0) {
+        int e;
+        frexp(mx, &e);
+        if (p == MF_PREC_FP16) {
+            s = ldexp(1.0, e - 15);
+        } else {
+            const double ratio = mx / 448.0;
+            int k2;
+            frexp(ratio, &k2);
+            if (ldexp(1.0, k2 - 1) == ratio) k2 -= 1;
+            s = ldexp(1.0, k2);
+        }
+    }
+    scale[t] = (float)s;
+}
+
+// Per row block: plane count W and value bytes of the row-sliced block.
+__global__ void k_rb_info(TileArgs A, bool mixed, int *rbW, unsigned *rbvb) {
+    const int lane = threadIdx.x & 31;
+    const int rb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (rb >= A.tilem) return;
+    RowCursor c;
+    cursor_init(A, c, rb, lane < 16 ? lane : 99);
+    int len = 0;
+    {
+        RowCursor d = c;
+        while (lane < 16 && cursor_valid(d)) {
+            ++len;
+            cursor_next(A, d);
+        }
+    }
+    const int W = (int)__reduce_max_sync(0xffffffffu, (unsigned)len);
+    unsigned vb = 0;
+    if (!mixed) {
+        vb = 128u * W;
+    } else {
+        for (int k = 0; k < W; ++k) {
+            const bool has = lane < 16 && cursor_valid(c);
+            int pp;
+            float ps;
+            plane_format(has ? (int)A.prec[c.t] : -1, has ? A.scale[c.t] : 1.0f, pp, ps);
+            vb += 16u * prec_width(pp);
+            if (has) cursor_next(A, c);
+        }
+    }
+    if (lane == 0) {
+        rbW[rb] = W;
+        rbvb[rb] = vb;
+    }
+}
+
 constexpr int FILL_THREADS = 256;
 
-// Device: one CTA writes one slab.
-__global__ void __launch_bounds__(FILL_THREADS) fill_slabs(
-    const SlabPlan *__restrict__ plans, const int *__restrict__ slab_cta, const int *__restrict__ cta_slab,
-    const int *__restrict__ segs, const XRun *__restrict__ runs, const int *__restrict__ tile_ptr,
-    const int *__restrict__ tile_col, const int *__restrict__ tile_off, const int *__restrict__ csrptr_off,
-    const unsigned char *__restrict__ bptr, const double *__restrict__ val, const unsigned char *__restrict__ col,
-    const unsigned char *__restrict__ prec, float *__restrict__ scale_out, int tilem, int rowA, uint8_t *slabs) {
-    __shared__ uint32_t s_voff[MAXT + 1];
-    __shared__ uint32_t s_coff[MAXT + 1];
-    __shared__ int sh[FILL_THREADS / 32];
+__global__ void __launch_bounds__(FILL_THREADS) k_fill_slabs(const SlabPlan *__restrict__ plans,
+                                                             const int *__restrict__ slab_cta,
+                                                             const int *__restrict__ cta_slab,
+                                                             const int *__restrict__ segs,
+                                                             const XRun *__restrict__ runs, TileArgs A,
+                                                             const int *__restrict__ rbW,
+                                                             const unsigned *__restrict__ rbvb, bool mixed,
+                                                             uint8_t *slabs) {
+    __shared__ uint32_t s_off[RB_PER_SLAB_MAX + 1];
     const int s = blockIdx.x;
     const SlabPlan P = plans[s];
     uint8_t *base = slabs + (size_t)P.off16 * 16;
-    const SlabOffsets o = slab_offsets(P.nrb, P.ntiles, P.valbytes, P.nnz);
-    // zero the slab (padding bytes deterministic)
+    const bool gather = P.mode == SLAB_GATHER;
     for (uint32_t i = threadIdx.x * 16; i < P.bytes; i += FILL_THREADS * 16)
         *reinterpret_cast<uint4 *>(base + i) = make_uint4(0, 0, 0, 0);
     __syncthreads();
@@ -55,11 +224,11 @@ __global__ void __launch_bounds__(FILL_THREADS) fill_slabs(
         memset(&h, 0, sizeof h);
         h.rb0 = P.rb0;
         h.nrb = (uint16_t)P.nrb;
-        h.ntiles = (uint16_t)P.ntiles;
+        h.ntiles = (uint16_t)min(P.ntiles, 65535);
         h.nxseg = (uint16_t)P.nseg;
         h.mode = (uint16_t)P.mode;
+        h.mixed = mixed ? 1 : 0;
         h.bytes = P.bytes;
-        h.cols16 = (uint16_t)(o.cols / 16);
         const int g = slab_cta[s];
         const int nx = s + STAGES;
         if (nx < cta_slab[g + 1]) {
@@ -68,140 +237,100 @@ __global__ void __launch_bounds__(FILL_THREADS) fill_slabs(
             h.next_bytes = Q.bytes;
             h.next_xbytes = Q.mode == SLAB_STAGED ? (uint32_t)Q.nseg * 128u : 0u;
             h.next_nruns = Q.mode == SLAB_STAGED ? (uint16_t)Q.nruns : 0;
-            XRun *dst = reinterpret_cast<XRun *>(base + o.runs);
+            XRun *dst = reinterpret_cast<XRun *>(base + 32);
             for (int k = 0; k < h.next_nruns; ++k) dst[k] = runs[Q.run_off + k];
         }
         *reinterpret_cast<SlabHeader *>(base) = h;
+        uint32_t off = slab_blocks_off(P.mode == SLAB_OVERSIZE ? 0 : P.nrb);
+        RbDir *dir = reinterpret_cast<RbDir *>(base + slab_rbdir_off());
+        if (P.mode != SLAB_OVERSIZE) {
+            for (int j = 0; j < P.nrb; ++j) {
+                s_off[j] = off;
+                const int W = rbW[P.rb0 + j];
+                dir[j].off = off;
+                dir[j].W = (uint32_t)W;
+                off += rb_block_bytes(W, mixed, gather, rbvb[P.rb0 + j]);
+            }
+            dir[P.nrb].off = off;
+            dir[P.nrb].W = 0;
+        }
     }
+    __syncthreads();
     if (P.mode == SLAB_OVERSIZE) return;
-    // per-tile value / column offsets (block scan over the slab's tiles)
-    const int nt = P.ntiles;
-    const int per = (nt + FILL_THREADS - 1) / FILL_THREADS;
-    uint32_t vsum = 0, csum = 0;
-    for (int k = 0; k < per; ++k) {
-        const int j = threadIdx.x * per + k;
-        if (j < nt) {
-            const int t = P.t0 + j;
-            const int nk = tile_off[t + 1] - tile_off[t];
-            vsum += tile_val_bytes(prec[t], nk);
-            csum += (uint32_t)nk;
-        }
-    }
-    // exclusive block scan of (vsum, csum): both fit 32 bits; do two scans
-    for (int pass = 0; pass < 2; ++pass) {
-        uint32_t v = pass == 0 ? vsum : csum;
-        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-        uint32_t x = v;
-        for (int d = 1; d < 32; d <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
-            if (lane >= d) x += y;
-        }
-        if (lane == 31) sh[w] = (int)x;
-        __syncthreads();
-        uint32_t wb = 0;
-        for (int q = 0; q < w; ++q) wb += (uint32_t)sh[q];
-        uint32_t ex = wb + x - v;
-        __syncthreads();
-        uint32_t *dst = pass == 0 ? s_voff : s_coff;
-        for (int k = 0; k < per; ++k) {
-            const int j = threadIdx.x * per + k;
-            if (j < nt) {
-                dst[j] = ex;
-                const int t = P.t0 + j;
-                const int nk = tile_off[t + 1] - tile_off[t];
-                ex += pass == 0 ? tile_val_bytes(prec[t], nk) : (uint32_t)nk;
-            }
-        }
-        if (threadIdx.x == FILL_THREADS - 1) dst[nt] = ex;
-        __syncthreads();
-    }
-    // row-block directory
-    RbDir *rbd = reinterpret_cast<RbDir *>(base + o.rbdir);
-    for (int j = threadIdx.x; j <= P.nrb; j += FILL_THREADS) {
-        const int tj = (j < P.nrb ? tile_ptr[P.rb0 + j] : tile_ptr[P.rb0 + P.nrb]) - P.t0;
-        RbDir d;
-        d.tile0 = (uint16_t)tj;
-        d.val_off = s_voff[tj];
-        d.col0 = (uint16_t)s_coff[tj];
-        rbd[j] = d;
-    }
-    uint32_t *slot = reinterpret_cast<uint32_t *>(base + o.slot);
-    uint8_t *rowend = base + o.rowend;
-    uint8_t *vals = base + o.vals;
-    uint8_t *cols = base + o.cols;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // one warp per tile
-    for (int j = warp; j < nt; j += FILL_THREADS / 32) {
-        const int t = P.t0 + j;
-        const int p = prec[t];
-        const int vo = tile_off[t];
-        const int nk = tile_off[t + 1] - vo;
-        // row block of tile t and its row length
-        int lo = P.rb0, hi = P.rb0 + P.nrb - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (tile_ptr[mid] <= t) lo = mid; else hi = mid - 1;
+    for (int j = warp; j < P.nrb; j += FILL_THREADS / 32) {
+        const int rb = P.rb0 + j;
+        const int W = rbW[rb];
+        uint8_t *blk = base + s_off[j];
+        RowCursor c;
+        cursor_init(A, c, rb, lane < 16 ? lane : 99);
+        // row lengths
+        int len = 0;
+        {
+            RowCursor d = c;
+            while (lane < 16 && cursor_valid(d)) {
+                ++len;
+                cursor_next(A, d);
+            }
         }
-        const int rl = lo == tilem - 1 ? rowA - (tilem - 1) * 16 : 16;
-        if (lane == 0) {
-            uint32_t sv;
-            if (P.mode == SLAB_STAGED) {
-                // slot = position of the tile column in the sorted unique list
-                const int c = tile_col[t];
-                int a = 0, b = P.nseg - 1;
-                while (a < b) {
-                    const int mid = (a + b) >> 1;
-                    if (segs[P.seg_off + mid] < c) a = mid + 1; else b = mid;
+        if (lane < 16) blk[lane] = (uint8_t)len;
+        PlaneDesc *pd = reinterpret_cast<PlaneDesc *>(blk + rb_pdesc_off());
+        uint8_t *idxb = blk + rb_idx_off(W, mixed);
+        uint8_t *vals = blk + rb_vals_off(W, mixed, gather);
+        uint32_t voff = 0;
+        int prev_t = -1;
+        for (int k = 0; k < W; ++k) {
+            const bool has = lane < 16 && cursor_valid(c);
+            int pp = MF_PREC_FP64;
+            float ps = 1.0f;
+            if (mixed) plane_format(has ? (int)A.prec[c.t] : -1, has ? A.scale[c.t] : 1.0f, pp, ps);
+            if (mixed && lane == 0) {
+                PlaneDesc d;
+                d.voff = (uint16_t)voff;
+                d.prec = (uint8_t)pp;
+                d.pad = 0;
+                d.scale = ps;
+                pd[k] = d;
+            }
+            if (has) {
+                const int t = c.t;
+                const int q = c.q;
+                const bool start = t != prev_t;
+                prev_t = t;
+                const bool low = mixed && A.prec[t] != MF_PREC_FP64;
+                const int colx = A.tile_col[t];
+                const int cin = A.col[q];
+                if (gather) {
+                    uint32_t id = (uint32_t)(colx * 16 + cin);
+                    if (start) id |= IDX32_START;
+                    if (low) id |= IDX32_LOW;
+                    reinterpret_cast<uint32_t *>(idxb)[k * 16 + lane] = id;
+                } else {
+                    int a = 0, b = P.nseg - 1;
+                    while (a < b) {
+                        const int mid = (a + b) >> 1;
+                        if (segs[P.seg_off + mid] < colx) a = mid + 1; else b = mid;
+                    }
+                    uint32_t id = (uint32_t)(a * 16 + cin);
+                    if (start) id |= IDX16_START;
+                    if (low) id |= IDX16_LOW;
+                    reinterpret_cast<uint16_t *>(idxb)[k * 16 + lane] = (uint16_t)id;
                 }
-                sv = (uint32_t)a;
-            } else {
-                sv = (uint32_t)tile_col[t];
+                const double v = mixed ? dequant(A, t, q) : A.val[q];
+                uint8_t *pv = vals + voff;
+                if (pp == MF_PREC_FP64) {
+                    reinterpret_cast<double *>(pv)[lane] = v;
+                } else if (pp == MF_PREC_FP32) {
+                    reinterpret_cast<float *>(pv)[lane] = (float)v;  // exact: v is a dequantized value
+                } else if (pp == MF_PREC_FP16) {
+                    reinterpret_cast<__half *>(pv)[lane] = __double2half(v / (double)ps);  // exact
+                } else {
+                    pv[lane] = (uint8_t)__nv_cvt_double_to_fp8(v / (double)ps, __NV_SATFINITE, __NV_E4M3);
+                }
+                cursor_next(A, c);
             }
-            slot[j] = sv | ((uint32_t)p << 30);
+            voff += 16u * prec_width(pp);
         }
-        if (lane < 16) {
-            const int r = lane;
-            const int cc = csrptr_off[t];
-            int e;
-            if (r + 1 < rl) e = bptr[cc + r + 1];
-            else e = nk;
-            rowend[16 * j + r] = (uint8_t)(e & 255);
-        }
-        // values: maximum magnitude for the scale of FP16 / FP8 tiles
-        double mx = 0.0;
-        for (int k = lane; k < nk; k += 32) mx = fmax(mx, fabs(val[vo + k]));
-        for (int d = 16; d > 0; d >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, d));
-        double scale = 1.0;
-        if (p >= MF_PREC_FP16 && mx > 0.0) {
-            int e;
-            frexp(mx, &e);
-            if (p == MF_PREC_FP16) {
-                scale = ldexp(1.0, e - 15);
-            } else {
-                const double ratio = mx / 448.0;
-                int k2;
-                frexp(ratio, &k2);
-                if (ldexp(1.0, k2 - 1) == ratio) k2 -= 1;
-                scale = ldexp(1.0, k2);
-            }
-        }
-        if (lane == 0) scale_out[t] = (float)scale;
-        uint8_t *vb = vals + s_voff[j];
-        const double inv = 1.0 / scale;  // exact: power of two
-        if (p == MF_PREC_FP64) {
-            for (int k = lane; k < nk; k += 32) reinterpret_cast<double *>(vb)[k] = val[vo + k];
-        } else if (p == MF_PREC_FP32) {
-            for (int k = lane; k < nk; k += 32) reinterpret_cast<float *>(vb)[k] = __double2float_rn(val[vo + k]);
-        } else if (p == MF_PREC_FP16) {
-            if (lane == 0) *reinterpret_cast<float *>(vb) = (float)scale;
-            for (int k = lane; k < nk; k += 32)
-                reinterpret_cast<__half *>(vb + 4)[k] = __double2half(val[vo + k] * inv);
-        } else {
-            if (lane == 0) *reinterpret_cast<float *>(vb) = (float)scale;
-            for (int k = lane; k < nk; k += 32)
-                vb[4 + k] = (uint8_t)__nv_cvt_double_to_fp8(val[vo + k] * inv, __NV_SATFINITE, __NV_E4M3);
-        }
-        for (int k = lane; k < nk; k += 32) cols[s_coff[j] + k] = col[vo + k];
     }
 }
 
@@ -218,19 +347,39 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
     const auto &tn = t->h_tile_nnz;
     std::vector<uint8_t> prec(prec_in);
     if ((int)prec.size() != tilenum) prec.assign(tilenum, MF_PREC_FP64);
+    bool mixed = false;
+    for (auto p : prec)
+        if (p != MF_PREC_FP64) {
+            mixed = true;
+            break;
+        }
 
-    // per row block: encoded bytes (without the slab header) and cost
-    std::vector<uint32_t> rbbytes(tilem);
-    std::vector<double> pref(tilem + 1, 0.0);
-    for (int rb = 0; rb < tilem; ++rb) {
-        uint64_t b = 8;
-        for (int k = tp[rb]; k < tp[rb + 1]; ++k) b += 4 + 16 + tile_val_bytes(prec[k], tn[k]) + tn[k];
-        rbbytes[rb] = (uint32_t)std::min<uint64_t>(b, 0xffffffffu);
-        pref[rb + 1] = pref[rb] + (double)b + 16.0 * 72.0;
+    // device: tile scales, row-block plane counts and value bytes
+    if (L.prec_dev.alloc(tilenum) || L.scale_dev.alloc(tilenum)) return MF_ERR_NOMEM;
+    DevArray<int> d_rbW;
+    DevArray<unsigned> d_rbvb;
+    if (d_rbW.alloc(tilem) || d_rbvb.alloc(tilem)) return MF_ERR_NOMEM;
+    if (tilenum > 0) {
+        MF_CUDA_TRY(cudaMemcpyAsync(L.prec_dev.p, prec.data(), tilenum, cudaMemcpyHostToDevice, st));
+        k_tile_scales<<<(tilenum + 7) / 8, 256, 0, st>>>(tilenum, t->tile_off.p, t->val.p, L.prec_dev.p,
+                                                        L.scale_dev.p);
     }
+    TileArgs A{t->tile_ptr.p, t->tile_col.p, t->tile_off.p, t->csrptr_off.p, t->ptr.p, t->val.p, t->col.p,
+               L.prec_dev.p, L.scale_dev.p, tilem, t->rowA};
+    k_rb_info<<<(tilem + 7) / 8, 256, 0, st>>>(A, mixed, d_rbW.p, d_rbvb.p);
+    MF_CUDA_TRY(cudaGetLastError());
+    std::vector<int> rbW(tilem);
+    std::vector<unsigned> rbvb(tilem);
+    MF_CUDA_TRY(cudaMemcpyAsync(rbW.data(), d_rbW.p, sizeof(int) * tilem, cudaMemcpyDeviceToHost, st));
+    MF_CUDA_TRY(cudaMemcpyAsync(rbvb.data(), d_rbvb.p, sizeof(unsigned) * tilem, cudaMemcpyDeviceToHost, st));
+    MF_CUDA_TRY(cudaStreamSynchronize(st));
+
+    auto rb_bytes = [&](int rb, bool gather) { return rb_block_bytes(rbW[rb], mixed, gather, rbvb[rb]); };
     // CTA ranges of equal cost, computed once per matrix and shared by every
     // layout so that all layouts give each CTA the same rows
     if ((int)t->h_cta_rb.size() != G + 1) {
+        std::vector<double> pref(tilem + 1, 0.0);
+        for (int rb = 0; rb < tilem; ++rb) pref[rb + 1] = pref[rb] + (double)rb_bytes(rb, false) + 16.0 * 72.0;
         std::vector<int> part(G + 1, tilem);
         part[0] = 0;
         int rb = 0;
@@ -263,48 +412,29 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
         while (rb < cta_rb[g + 1]) {
             SlabPlan P{};
             P.rb0 = rb;
-            P.t0 = tp[rb];
-            cur.clear();
-            // first row block decides the mode
-            const int ntl = tp[rb + 1] - tp[rb];
-            int nnz0 = 0;
-            uint32_t vb0 = 0;
-            for (int k = tp[rb]; k < tp[rb + 1]; ++k) {
-                nnz0 += tn[k];
-                vb0 += tile_val_bytes(prec[k], tn[k]);
-            }
-            const uint32_t tot0 = slab_offsets(1, ntl, vb0, nnz0).total;
             rbsegs.assign(tc.begin() + tp[rb], tc.begin() + tp[rb + 1]);  // ascending already
-            if (tot0 > (uint32_t)slab_max || ntl > MAXT) {
+            const bool staged0 = (int)rbsegs.size() <= XSEG_MAX && count_runs(rbsegs) <= MAXRUNS;
+            const uint32_t tot0 = slab_blocks_off(1) + rb_bytes(rb, !staged0);
+            if (tot0 > (uint32_t)slab_max || rbW[rb] > MAXW) {
                 P.mode = SLAB_OVERSIZE;
                 P.nrb = 1;
-                P.ntiles = 0;
-                P.nnz = 0;
-                P.valbytes = 0;
-                P.bytes = slab_offsets(1, 0, 0, 0).total;
+                P.ntiles = tp[rb + 1] - tp[rb];
+                P.bytes = slab_blocks_off(0);
                 for (int k = tp[rb]; k < tp[rb + 1]; ++k) prec[k] = MF_PREC_FP64;
                 ++n_over;
                 rb += 1;
             } else {
-                const bool staged = (int)rbsegs.size() <= XSEG_MAX && count_runs(rbsegs) <= MAXRUNS;
+                const bool staged = staged0;
                 P.mode = staged ? SLAB_STAGED : SLAB_GATHER;
                 if (staged) cur = rbsegs;
                 P.nrb = 1;
-                P.ntiles = ntl;
-                P.nnz = nnz0;
-                P.valbytes = vb0;
+                P.ntiles = tp[rb + 1] - tp[rb];
+                uint32_t body = rb_bytes(rb, !staged);
                 int nx = rb + 1;
                 while (nx < cta_rb[g + 1] && P.nrb < rbps) {
-                    const int ntx = tp[nx + 1] - tp[nx];
-                    int nnzx = 0;
-                    uint32_t vbx = 0;
-                    for (int k = tp[nx]; k < tp[nx + 1]; ++k) {
-                        nnzx += tn[k];
-                        vbx += tile_val_bytes(prec[k], tn[k]);
-                    }
-                    if (P.ntiles + ntx > MAXT) break;
-                    const uint32_t tot = slab_offsets(P.nrb + 1, P.ntiles + ntx, P.valbytes + vbx, P.nnz + nnzx).total;
-                    if (tot > (uint32_t)slab_max) break;
+                    if (rbW[nx] > MAXW) break;
+                    const uint32_t bx = rb_bytes(nx, !staged);
+                    if (slab_blocks_off(P.nrb + 1) + body + bx > (uint32_t)slab_max) break;
                     if (staged) {
                         merged.clear();
                         std::set_union(cur.begin(), cur.end(), tc.begin() + tp[nx], tc.begin() + tp[nx + 1],
@@ -313,12 +443,11 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
                         cur.swap(merged);
                     }
                     P.nrb += 1;
-                    P.ntiles += ntx;
-                    P.nnz += nnzx;
-                    P.valbytes += vbx;
+                    P.ntiles += tp[nx + 1] - tp[nx];
+                    body += bx;
                     ++nx;
                 }
-                P.bytes = slab_offsets(P.nrb, P.ntiles, P.valbytes, P.nnz).total;
+                P.bytes = slab_blocks_off(P.nrb) + body;
                 if (!staged) ++n_gather;
                 rb = nx;
             }
@@ -348,6 +477,12 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
         set_last_error("slab layout exceeds 64 GiB");
         return MF_ERR_UNSUPPORTED;
     }
+    // oversize row blocks are computed in FP64 from the tile arrays
+    if (n_over > 0 && tilenum > 0) {
+        MF_CUDA_TRY(cudaMemcpyAsync(L.prec_dev.p, prec.data(), tilenum, cudaMemcpyHostToDevice, st));
+        k_tile_scales<<<(tilenum + 7) / 8, 256, 0, st>>>(tilenum, t->tile_off.p, t->val.p, L.prec_dev.p,
+                                                        L.scale_dev.p);
+    }
     // issue records of the first STAGES slabs of every CTA
     std::vector<uint8_t> head((size_t)G * STAGES * ISSUE_REC, 0);
     for (int g = 0; g < G; ++g)
@@ -360,8 +495,7 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
             rec[1] = P.bytes;
             rec[2] = P.mode == SLAB_STAGED ? (uint32_t)P.nseg * 128u : 0u;
             rec[3] = P.mode == SLAB_STAGED ? (uint32_t)P.nruns : 0u;
-            if (P.mode == SLAB_STAGED)
-                std::memcpy(&rec[4], &run_all[P.run_off], sizeof(XRun) * P.nruns);
+            if (P.mode == SLAB_STAGED) std::memcpy(&rec[4], &run_all[P.run_off], sizeof(XRun) * P.nruns);
         }
     // dependency ranges: CTAs owning the x segments a CTA reads
     std::vector<int> dep(2 * G);
@@ -391,22 +525,18 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
         alg += tile_alg_bytes(prec[k], tn[k]);
         cnt[prec[k]] += 1;
     }
-    // upload
+    // upload and fill
     DevArray<SlabPlan> d_plans;
     DevArray<int> d_slab_cta, d_segs;
     DevArray<XRun> d_runs;
     if (L.slabs.alloc(off + 16) || L.head.alloc(head.size()) || L.cta_slab.alloc(G + 1) ||
-        L.cta_rb.alloc(G + 1) || L.cta_dep.alloc(2 * G) || L.prec_dev.alloc(tilenum) ||
-        L.scale_dev.alloc(tilenum) || d_plans.alloc(ns) || d_slab_cta.alloc(ns) ||
+        L.cta_rb.alloc(G + 1) || L.cta_dep.alloc(2 * G) || d_plans.alloc(ns) || d_slab_cta.alloc(ns) ||
         d_segs.alloc(seg_all.size()) || d_runs.alloc(run_all.size()))
         return MF_ERR_NOMEM;
     MF_CUDA_TRY(cudaMemcpyAsync(L.head.p, head.data(), head.size(), cudaMemcpyHostToDevice, st));
     MF_CUDA_TRY(cudaMemcpyAsync(L.cta_slab.p, cta_slab.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice, st));
     MF_CUDA_TRY(cudaMemcpyAsync(L.cta_rb.p, cta_rb.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice, st));
     MF_CUDA_TRY(cudaMemcpyAsync(L.cta_dep.p, dep.data(), sizeof(int) * 2 * G, cudaMemcpyHostToDevice, st));
-    if (tilenum > 0)
-        MF_CUDA_TRY(cudaMemcpyAsync(L.prec_dev.p, prec.data(), tilenum, cudaMemcpyHostToDevice, st));
-    MF_CUDA_TRY(cudaMemsetAsync(L.scale_dev.p, 0, sizeof(float) * std::max(tilenum, 1), st));
     if (ns > 0) {
         MF_CUDA_TRY(cudaMemcpyAsync(d_plans.p, plans.data(), sizeof(SlabPlan) * ns, cudaMemcpyHostToDevice, st));
         MF_CUDA_TRY(cudaMemcpyAsync(d_slab_cta.p, slab_cta.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, st));
@@ -416,10 +546,8 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
     if (!run_all.empty())
         MF_CUDA_TRY(cudaMemcpyAsync(d_runs.p, run_all.data(), sizeof(XRun) * run_all.size(), cudaMemcpyHostToDevice, st));
     if (ns > 0)
-        fill_slabs<<<ns, FILL_THREADS, 0, st>>>(d_plans.p, d_slab_cta.p, L.cta_slab.p, d_segs.p, d_runs.p,
-                                               t->tile_ptr.p, t->tile_col.p, t->tile_off.p, t->csrptr_off.p,
-                                               t->ptr.p, t->val.p, t->col.p, L.prec_dev.p, L.scale_dev.p, tilem,
-                                               t->rowA, L.slabs.p);
+        k_fill_slabs<<<ns, FILL_THREADS, 0, st>>>(d_plans.p, d_slab_cta.p, L.cta_slab.p, d_segs.p, d_runs.p, A,
+                                                 d_rbW.p, d_rbvb.p, mixed, L.slabs.p);
     MF_CUDA_TRY(cudaGetLastError());
     MF_CUDA_TRY(cudaStreamSynchronize(st));
     L.prec.swap(prec);
@@ -429,6 +557,7 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
     L.n_oversize = n_over;
     L.slab_max = slab_max;
     L.rb_per_slab = rbps;
+    L.mixed = mixed;
     L.bytes = off;
     L.alg_bytes = alg;
     for (int p = 0; p < 4; ++p) L.tile_frac[p] = tilenum > 0 ? cnt[p] / tilenum : 0.0;

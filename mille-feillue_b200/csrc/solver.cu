@@ -37,11 +37,12 @@ namespace mf {
 
 // ---------------------------------------------------------------- smem
 struct __align__(16) Smem {
-    uint64_t full[STAGES];
+    uint64_t full[STAGES];   // slab + x runs landed (producer arrive + tx bytes)
+    uint64_t empty[STAGES];  // every consumer warp is done with the stage
     uint32_t abort;
     uint32_t pad;
     int slab0[KMAX_LAYOUTS], slab1[KMAX_LAYOUTS];
-    double red[NWARPS][4];
+    double red[NWARPS + 1][4];
     double bres[4];
     uint8_t head[KMAX_LAYOUTS][STAGES][ISSUE_REC];
 };
@@ -66,85 +67,105 @@ __device__ void issue_slab(Smem &S, uint8_t *stage, int slab_area, int k, uint32
     bulk_g2s(stage, slabs + (size_t)off16 * 16, bytes, &S.full[k], pol_m);
 }
 
-__device__ bool wait_full(Smem &S, int k, uint32_t parity, uint64_t limit_ns) {
-    if (mbar_try_wait(&S.full[k], parity)) return true;
+// Pipeline state kept in registers across SpMV calls: consumer parity of
+// each stage's full barrier, producer parity of each stage's empty barrier,
+// and the stages filled at least once (whose refill must wait for empty).
+struct Pipe {
+    uint32_t fph = 0, eph = 0, filled = 0;
+};
+
+__device__ bool wait_bar(uint64_t *bar, uint32_t parity, uint64_t limit_ns) {
+    if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = globaltimer();
     for (uint32_t spin = 1;; ++spin) {
-        if (mbar_try_wait(&S.full[k], parity)) return true;
+        if (mbar_try_wait(bar, parity)) return true;
         if ((spin & 15u) == 0 && globaltimer() - t0 > limit_ns) return false;
     }
 }
 
-// Sum of one row over the tiles [t0, t1) of a staged / gather slab.
+// Sum of row r of row block j of a staged / gather slab (row-sliced planes).
+// FP64 tiles: sum = 0, sum += x*v in order, acc += sum at each tile start,
+// exactly blockspmv_cpu's order. Tiles below FP64 (mixed layouts): the
+// dequantized value in FP32, sumf = fmaf(x, v, sumf), acc += sumf.
 template <bool MIXED>
 __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &h, int j, int r, const double *xstage,
                                            const double *__restrict__ xg) {
-    const SlabOffsets o = slab_offsets(h.nrb, h.ntiles, 0, 0);
-    const RbDir *rbd = reinterpret_cast<const RbDir *>(st + o.rbdir);
-    const uint32_t *slot = reinterpret_cast<const uint32_t *>(st + o.slot);
-    const uint8_t *rowend = st + o.rowend;
-    const uint8_t *vals = st + o.vals;
-    const uint8_t *cols = st + (uint32_t)h.cols16 * 16u;
-    const RbDir d0 = rbd[j], d1 = rbd[j + 1];
-    uint32_t coff = d0.col0, voff = d0.val_off;
-    const bool staged = h.mode == SLAB_STAGED;
-    double acc = 0.0;
-    for (int t = d0.tile0; t < d1.tile0; ++t) {
-        const uint32_t sw = slot[t];
-        const uint8_t *re = rowend + 16 * t;
-        const int e15 = re[15];
-        const int nk = e15 ? e15 : 256;
-        const int s = r ? re[r - 1] : 0;
-        const int e = r == 15 ? nk : re[r];
-        const uint32_t idx = sw & 0x3fffffffu;
-        const int prec = MIXED ? (int)(sw >> 30) : 0;
-        const uint8_t *cb = cols + coff;
-        if (prec == MF_PREC_FP64) {
-            const double *vb = reinterpret_cast<const double *>(vals + voff);
-            double sum = 0.0;
-            if (staged) {
-                const double *xs = xstage + idx * 16;
-                for (int q = s; q < e; ++q) sum = dadd(sum, dmul(xs[cb[q]], vb[q]));
-            } else {
-                const double *xs = xg + (size_t)idx * 16;
-                for (int q = s; q < e; ++q) sum = dadd(sum, dmul(__ldcg(xs + cb[q]), vb[q]));
+    const RbDir d = reinterpret_cast<const RbDir *>(st + slab_rbdir_off())[j];
+    const uint8_t *blk = st + d.off;
+    const int W = (int)d.W;
+    const int len = blk[r];
+    const bool gather = h.mode == SLAB_GATHER;
+    double acc = 0.0, sum = 0.0;
+    if (!MIXED) {
+        const double *vals = reinterpret_cast<const double *>(blk + rb_vals_off(W, false, gather));
+        if (!gather) {
+            const uint16_t *idx = reinterpret_cast<const uint16_t *>(blk + rb_idx_off(W, false));
+#pragma unroll 4
+            for (int k = 0; k < len; ++k) {
+                const uint32_t id = idx[k * 16 + r];
+                const double v = vals[k * 16 + r];
+                const double x = xstage[id & IDX16_POS];
+                if (id & IDX16_START) {
+                    acc = dadd(acc, sum);
+                    sum = 0.0;
+                }
+                sum = dadd(sum, dmul(x, v));
             }
-            acc = dadd(acc, sum);
-            voff += 8u * nk;
         } else {
-            const double *xs = staged ? xstage + idx * 16 : xg + (size_t)idx * 16;
-            float sum = 0.0f;
-            float scale = 1.0f;
-            if (prec == MF_PREC_FP32) {
-                const float *vb = reinterpret_cast<const float *>(vals + voff);
-                for (int q = s; q < e; ++q) {
-                    const double xv = staged ? xs[cb[q]] : __ldcg(xs + cb[q]);
-                    sum = __fmaf_rn(__double2float_rn(xv), vb[q], sum);
+            const uint32_t *idx = reinterpret_cast<const uint32_t *>(blk + rb_idx_off(W, false));
+#pragma unroll 4
+            for (int k = 0; k < len; ++k) {
+                const uint32_t id = idx[k * 16 + r];
+                const double v = vals[k * 16 + r];
+                const double x = __ldcg(xg + (id & IDX32_POS));
+                if (id & IDX32_START) {
+                    acc = dadd(acc, sum);
+                    sum = 0.0;
                 }
-                voff += align8u(4u * nk);
-            } else if (prec == MF_PREC_FP16) {
-                scale = *reinterpret_cast<const float *>(vals + voff);
-                const __half *vb = reinterpret_cast<const __half *>(vals + voff + 4);
-                for (int q = s; q < e; ++q) {
-                    const double xv = staged ? xs[cb[q]] : __ldcg(xs + cb[q]);
-                    sum = __fmaf_rn(__double2float_rn(xv), __half2float(vb[q]), sum);
-                }
-                voff += align8u(4u + 2u * nk);
-            } else {
-                scale = *reinterpret_cast<const float *>(vals + voff);
-                const uint8_t *vb = vals + voff + 4;
-                for (int q = s; q < e; ++q) {
-                    const double xv = staged ? xs[cb[q]] : __ldcg(xs + cb[q]);
-                    const __half_raw hr = __nv_cvt_fp8_to_halfraw((__nv_fp8_storage_t)vb[q], __NV_E4M3);
-                    sum = __fmaf_rn(__double2float_rn(xv), __half2float(__half(hr)), sum);
-                }
-                voff += align8u(4u + (uint32_t)nk);
+                sum = dadd(sum, dmul(x, v));
             }
-            acc = dadd(acc, dmul((double)sum, (double)scale));
         }
-        coff += nk;
+        return dadd(acc, sum);
     }
-    return acc;
+    const PlaneDesc *pd = reinterpret_cast<const PlaneDesc *>(blk + rb_pdesc_off());
+    const uint8_t *idxb = blk + rb_idx_off(W, true);
+    const uint8_t *vals = blk + rb_vals_off(W, true, gather);
+    float sumf = 0.0f;
+    bool low = false;
+    for (int k = 0; k < len; ++k) {
+        const PlaneDesc p = pd[k];
+        double x;
+        bool start, lowk;
+        if (!gather) {
+            const uint32_t id = reinterpret_cast<const uint16_t *>(idxb)[k * 16 + r];
+            x = xstage[id & IDX16_POS];
+            start = id & IDX16_START;
+            lowk = id & IDX16_LOW;
+        } else {
+            const uint32_t id = reinterpret_cast<const uint32_t *>(idxb)[k * 16 + r];
+            x = __ldcg(xg + (id & IDX32_POS));
+            start = id & IDX32_START;
+            lowk = id & IDX32_LOW;
+        }
+        if (start) {
+            acc = dadd(acc, low ? (double)sumf : sum);
+            sum = 0.0;
+            sumf = 0.0f;
+            low = lowk;
+        }
+        const uint8_t *pv = vals + p.voff;
+        if (low) {
+            float vf;
+            if (p.prec == MF_PREC_FP64) vf = __double2float_rn(reinterpret_cast<const double *>(pv)[r]);
+            else if (p.prec == MF_PREC_FP32) vf = reinterpret_cast<const float *>(pv)[r];
+            else if (p.prec == MF_PREC_FP16) vf = __half2float(reinterpret_cast<const __half *>(pv)[r]) * p.scale;
+            else vf = __half2float(__half(__nv_cvt_fp8_to_halfraw((__nv_fp8_storage_t)pv[r], __NV_E4M3))) * p.scale;
+            sumf = __fmaf_rn(__double2float_rn(x), vf, sumf);
+        } else {
+            sum = dadd(sum, dmul(x, reinterpret_cast<const double *>(pv)[r]));
+        }
+    }
+    return dadd(acc, low ? (double)sumf : sum);
 }
 
 // Row sum of an oversize row block straight from the global tile arrays.
@@ -167,11 +188,16 @@ __device__ double global_row(const KParams &P, int rb, int r, const double *__re
 }
 
 // Tiled SpMV of this CTA's row range with layout `lay` and input vector xv.
-// For every row < rowA: v = epi.pre(row) is loaded before the row's tiles,
-// then epi(row, acc, v) runs with the row sum. Returns false on abort.
+// Warp PRODUCER_WARP (one lane) streams the CTA's slabs into the STAGES-deep
+// ring: it waits until the consumers released a stage, then issues the x
+// runs and the slab of the next slab with 1D bulk copies. The NWARPS
+// consumer warps wait for a stage's full barrier, compute their row blocks
+// (one half-warp per row block, one lane per row) and release the stage.
+// For every row < rowA: v = epi.pre(row) is loaded before the row's
+// entries, then epi(row, acc, v) runs with the row sum. Returns false on
+// abort.
 template <bool MIXED, class Epi>
-__device__ bool cta_spmv(const KParams &P, int lay, const double *xv, Smem &S, uint8_t *dyn, uint32_t &ph,
-                         Epi &epi) {
+__device__ bool cta_spmv(const KParams &P, int lay, const double *xv, Smem &S, uint8_t *dyn, Pipe &pp, Epi &epi) {
     const int ns = S.slab1[lay] - S.slab0[lay];
     const int stride = P.stage_stride;
     const int slab_area = P.slab_area;
@@ -179,50 +205,80 @@ __device__ bool cta_spmv(const KParams &P, int lay, const double *xv, Smem &S, u
     const int tid = threadIdx.x;
     const int w = tid >> 5, lane = tid & 31;
     const int half = lane >> 4, r = lane & 15;
-    if (tid == 0) {
-        const uint64_t pm = policy_evict_first(), pv = policy_evict_last();
-        fence_proxy_async_global();
-        for (int k = 0; k < STAGES && k < ns; ++k) {
-            const uint32_t *rec = reinterpret_cast<const uint32_t *>(S.head[lay][k]);
-            issue_slab(S, stage_ptr(dyn, k, stride), slab_area, k, rec[0], rec[1], rec[2], (int)rec[3],
-                       reinterpret_cast<const XRun *>(rec + 4), L.slabs, xv, pm, pv);
-        }
-    }
-    for (int i = 0; i < ns; ++i) {
-        const int k = i % STAGES;
-        uint8_t *st = stage_ptr(dyn, k, stride);
-        if (!wait_full(S, k, (ph >> k) & 1u, P.limit_ns)) {
-            set_error(P, (uint32_t)MF_ERR_TIMEOUT, 100 + lay);
-            return false;
-        }
-        ph ^= 1u << k;
-        const SlabHeader h = *reinterpret_cast<const SlabHeader *>(st);
-        if (h.mode == SLAB_OVERSIZE) {
-            if (w == 0 && half == 0) {
-                const int row = h.rb0 * 16 + r;
-                const double pv = row < P.rowA ? epi.pre(row) : 0.0;
-                const double acc = global_row(P, h.rb0, r, xv);
-                if (row < P.rowA) epi(row, acc, pv);
-            }
-        } else {
-            for (int j = 2 * w + half; j < h.nrb; j += 2 * NWARPS) {
-                const int row = (h.rb0 + j) * 16 + r;
-                const bool live = row < P.rowA;
-                const double pv = live ? epi.pre(row) : 0.0;
-                const double acc =
-                    slab_row<MIXED>(st, h, j, r, reinterpret_cast<const double *>(st + slab_area), xv);
-                if (live) epi(row, acc, pv);
-            }
-        }
-        __syncthreads();
-        if (tid == 0 && h.next_bytes != 0u) {
+    if (w == PRODUCER_WARP) {
+        if (lane == 0) {
             const uint64_t pm = policy_evict_first(), pv = policy_evict_last();
-            fence_proxy_async_smem();
-            issue_slab(S, st, slab_area, k, h.next_off16, h.next_bytes, h.next_xbytes, h.next_nruns,
-                       reinterpret_cast<const XRun *>(st + 32), L.slabs, xv, pm, pv);
+            fence_proxy_async_global();
+            for (int i = 0; i < ns; ++i) {
+                const int k = i % STAGES;
+                uint8_t *st = stage_ptr(dyn, k, stride);
+                if ((pp.filled >> k) & 1u) {
+                    if (!wait_bar(&S.empty[k], (pp.eph >> k) & 1u, P.limit_ns)) {
+                        set_error(P, (uint32_t)MF_ERR_TIMEOUT, 110 + lay);
+                        S.abort = 1;
+                        break;
+                    }
+                    pp.eph ^= 1u << k;
+                }
+                pp.filled |= 1u << k;
+                uint32_t off16, bytes, xbytes;
+                int nruns;
+                const XRun *runs;
+                if (i < STAGES) {
+                    const uint32_t *rec = reinterpret_cast<const uint32_t *>(S.head[lay][i]);
+                    off16 = rec[0];
+                    bytes = rec[1];
+                    xbytes = rec[2];
+                    nruns = (int)rec[3];
+                    runs = reinterpret_cast<const XRun *>(rec + 4);
+                } else {
+                    // the slab consumed from this stage carries the record of slab i
+                    const SlabHeader *h = reinterpret_cast<const SlabHeader *>(st);
+                    off16 = h->next_off16;
+                    bytes = h->next_bytes;
+                    xbytes = h->next_xbytes;
+                    nruns = h->next_nruns;
+                    runs = reinterpret_cast<const XRun *>(st + 32);
+                }
+                fence_proxy_async_smem();
+                issue_slab(S, st, slab_area, k, off16, bytes, xbytes, nruns, runs, L.slabs, xv, pm, pv);
+            }
+        }
+        __syncwarp();
+    } else {
+        for (int i = 0; i < ns; ++i) {
+            const int k = i % STAGES;
+            uint8_t *st = stage_ptr(dyn, k, stride);
+            if (!wait_bar(&S.full[k], (pp.fph >> k) & 1u, P.limit_ns)) {
+                set_error(P, (uint32_t)MF_ERR_TIMEOUT, 100 + lay);
+                S.abort = 1;
+                break;
+            }
+            pp.fph ^= 1u << k;
+            const SlabHeader h = *reinterpret_cast<const SlabHeader *>(st);
+            if (h.mode == SLAB_OVERSIZE) {
+                if (w == 0 && half == 0) {
+                    const int row = h.rb0 * 16 + r;
+                    const double pv = row < P.rowA ? epi.pre(row) : 0.0;
+                    const double acc = global_row(P, h.rb0, r, xv);
+                    if (row < P.rowA) epi(row, acc, pv);
+                }
+            } else {
+                for (int j = 2 * w + half; j < h.nrb; j += 2 * NWARPS) {
+                    const int row = (h.rb0 + j) * 16 + r;
+                    const bool live = row < P.rowA;
+                    const double pv = live ? epi.pre(row) : 0.0;
+                    const double acc =
+                        slab_row<MIXED>(st, h, j, r, reinterpret_cast<const double *>(st + slab_area), xv);
+                    if (live) epi(row, acc, pv);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&S.empty[k]);
         }
     }
-    return true;
+    __syncthreads();
+    return S.abort == 0;
 }
 
 // Block reduction of NV partials in a fixed order, then the grid-wide sum.
@@ -247,7 +303,7 @@ __device__ bool grid_sum(const KParams &P, Smem &S, const double (&v)[NV], doubl
 #pragma unroll
         for (int k = 0; k < NV; ++k) {
             p[k] = 0.0;
-            for (int q = 0; q < NWARPS; ++q) p[k] += S.red[q][k];
+            for (int q = 0; q <= NWARPS; ++q) p[k] += S.red[q][k];
             P.partial[((size_t)slot * G + blockIdx.x) * 4 + k] = p[k];
         }
         red_release_add(P.sync + SYNC_ARRIVE, 1u);
@@ -336,7 +392,10 @@ __device__ bool wait_deps(const KParams &P, Smem &S, int lay, uint32_t ep) {
 __device__ void kernel_setup(const KParams &P, Smem &S, int nlay) {
     const int tid = threadIdx.x;
     if (tid == 0) {
-        for (int k = 0; k < STAGES; ++k) mbar_init(&S.full[k], 1);
+        for (int k = 0; k < STAGES; ++k) {
+            mbar_init(&S.full[k], 1);
+            mbar_init(&S.empty[k], NWARPS);
+        }
         mbar_fence_init();
         S.abort = 0;
     }
@@ -351,6 +410,18 @@ __device__ void kernel_setup(const KParams &P, Smem &S, int nlay) {
     __syncthreads();
 }
 
+// Vector passes run over the CTA's own row blocks [lo, hi) (16-row aligned,
+// zero padded past rowA) in pairs of rows with 16-byte loads, VB pairs per
+// thread per batch so that all loads of a batch are in flight together.
+#define MF_PAIRS(VB, lo, hi, ...)                                                     \
+    for (int _b = ((lo) >> 1) + threadIdx.x; _b < ((hi) >> 1); _b += NTHREADS * (VB)) { \
+        constexpr int _vb = (VB);                                                     \
+        __VA_ARGS__                                                                   \
+    }
+#define MF_FOR_VB for (int u = 0; u < _vb; ++u)
+#define MF_PI(u) (_b + (u) * NTHREADS)
+#define MF_LIVE(u, hi) (MF_PI(u) < ((hi) >> 1))
+
 // ------------------------------------------------------------------ SpMV
 struct EpiStore {
     double *y;
@@ -363,22 +434,25 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_spmv(KParams P, const double *x
     extern __shared__ __align__(128) uint8_t dyn[];
     __shared__ Smem S;
     kernel_setup(P, S, lay + 1);
-    uint32_t ph = 0;
+    Pipe pp;
     EpiStore epi{y};
     for (int it = 0; it < reps; ++it) {
-        if (!cta_spmv<MIXED>(P, lay, x, S, dyn, ph, epi)) return;
+        if (!cta_spmv<MIXED>(P, lay, x, S, dyn, pp, epi)) return;
     }
 }
 
 // -------------------------------------------------------------------- CG
+// The solver's vectors are read and written with an L2 evict_last policy
+// so they stay resident in L2 while the matrix streams with evict_first.
 struct EpiResidual {  // r = b - A x, rr += r*r
     const double *b;
     double *r;
     double rr;
-    __device__ double pre(int row) const { return __ldcg(b + row); }
+    uint64_t pol;
+    __device__ double pre(int row) const { return ld_hint(b + row, pol); }
     __device__ void operator()(int row, double acc, double bv) {
         const double v = bv - acc;
-        r[row] = v;
+        st_hint(r + row, v, pol);
         rr += v * v;
     }
 };
@@ -386,9 +460,10 @@ struct EpiQ {  // q = A d, dq += d*q
     const double *d;
     double *q;
     double dq;
-    __device__ double pre(int row) const { return __ldcg(d + row); }
+    uint64_t pol;
+    __device__ double pre(int row) const { return ld_hint(d + row, pol); }
     __device__ void operator()(int row, double acc, double dv) {
-        q[row] = acc;
+        st_hint(q + row, acc, pol);
         dq += dv * acc;
     }
 };
@@ -399,11 +474,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cg(KParams P) {
     __shared__ Smem S;
     kernel_setup(P, S, P.nlay);
     const int G = gridDim.x, g = blockIdx.x, tid = threadIdx.x;
-    uint32_t ph = 0, phase = 0;
+    Pipe pp;
+    uint32_t phase = 0;
+    const uint64_t vpol = policy_evict_last();
     const int lay64 = 0;
     int lay = P.start_layout;
     const int rb_lo = P.lay[0].cta_rb[g], rb_hi = P.lay[0].cta_rb[g + 1];
-    const int row_lo = rb_lo * 16, row_hi = min(rb_hi * 16, P.rowA);
+    const int vlo = rb_lo * 16, vhi = rb_hi * 16;  // own rows, zero padded past rowA
     double *x = P.x, *r = P.r, *d = P.d, *q = P.q;
     const double *b = P.b;
     if (P.inject_wait) {
@@ -412,14 +489,23 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cg(KParams P) {
         if (!wait_deps(P, S, 0, 0xffffffffu)) return;
     }
     // r = b - A x0, d = r; (rr, bb)
-    EpiResidual er{b, r, 0.0};
-    if (!cta_spmv<false>(P, lay64, x, S, dyn, ph, er)) return;
+    EpiResidual er{b, r, 0.0, vpol};
+    if (!cta_spmv<false>(P, lay64, x, S, dyn, pp, er)) return;
     __syncthreads();
     double bbp = 0.0;
-    for (int i = row_lo + tid; i < row_hi; i += NTHREADS) {
-        d[i] = r[i];
-        bbp += b[i] * b[i];
-    }
+    MF_PAIRS(4, vlo, vhi, {
+        double2 rv[_vb], bv[_vb];
+#pragma unroll
+        MF_FOR_VB if (MF_LIVE(u, vhi)) {
+            rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+            bv[u] = ld2_hint(b + 2 * MF_PI(u), vpol);
+        }
+#pragma unroll
+        MF_FOR_VB if (MF_LIVE(u, vhi)) {
+            st2_hint(d + 2 * MF_PI(u), rv[u], vpol);
+            bbp += bv[u].x * bv[u].x + bv[u].y * bv[u].y;
+        }
+    })
     double v2[2] = {er.rr, bbp}, o2[2];
     if (!grid_sum<2>(P, S, v2, o2, phase)) return;
     double rr = o2[0];
@@ -436,8 +522,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cg(KParams P) {
         // periodic true-residual replacement r = b - A x (FP64 layout)
         if (P.replace_every > 0 && it > 0 && it % P.replace_every == 0) {
             if (!wait_deps(P, S, lay64, ep)) return;
-            EpiResidual e2{b, r, 0.0};
-            if (!cta_spmv<false>(P, lay64, x, S, dyn, ph, e2)) return;
+            EpiResidual e2{b, r, 0.0, vpol};
+            if (!cta_spmv<false>(P, lay64, x, S, dyn, pp, e2)) return;
             double v1[1] = {e2.rr}, o1[1];
             if (!grid_sum<1>(P, S, v1, o1, phase)) return;
             rr = o1[0];
@@ -452,10 +538,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cg(KParams P) {
             }
         }
         if (!wait_deps(P, S, lay, ep)) return;
-        EpiQ eq{d, q, 0.0};
+        EpiQ eq{d, q, 0.0, vpol};
         bool ok;
-        if (MIXED && lay != lay64) ok = cta_spmv<true>(P, lay, d, S, dyn, ph, eq);
-        else ok = cta_spmv<false>(P, lay64, d, S, dyn, ph, eq);
+        if (MIXED && lay != lay64) ok = cta_spmv<true>(P, lay, d, S, dyn, pp, eq);
+        else ok = cta_spmv<false>(P, lay64, d, S, dyn, pp, eq);
         if (!ok) return;
         double v1[1] = {eq.dq}, o1[1];
         if (!grid_sum<1>(P, S, v1, o1, phase)) return;
@@ -466,11 +552,22 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cg(KParams P) {
         }
         const double alpha = rr / dq;
         double rrp = 0.0;
-        for (int i = row_lo + tid; i < row_hi; i += NTHREADS) {
-            const double ri = r[i] - alpha * q[i];
-            r[i] = ri;
-            rrp += ri * ri;
-        }
+        MF_PAIRS(4, vlo, vhi, {
+            double2 rv[_vb], qv[_vb];
+#pragma unroll
+            MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+                qv[u] = ld2_hint(q + 2 * MF_PI(u), vpol);
+            }
+#pragma unroll
+            MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                double2 o;
+                o.x = rv[u].x - alpha * qv[u].x;
+                o.y = rv[u].y - alpha * qv[u].y;
+                st2_hint(r + 2 * MF_PI(u), o, vpol);
+                rrp += o.x * o.x + o.y * o.y;
+            }
+        })
         double w1[1] = {rrp}, u1[1];
         if (!grid_sum<1>(P, S, w1, u1, phase)) return;
         const double rrn = u1[0];
@@ -478,11 +575,27 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cg(KParams P) {
         rel = bnorm > 0 ? sqrt(rrn) / bnorm : 0.0;
         const double beta = rrn / rr;
         const bool done = !fixed && rel <= tol;
-        for (int i = row_lo + tid; i < row_hi; i += NTHREADS) {
-            const double di = d[i];
-            x[i] += alpha * di;
-            if (!done) d[i] = r[i] + beta * di;
-        }
+        MF_PAIRS(4, vlo, vhi, {
+            double2 dv[_vb], xv[_vb], rv[_vb];
+#pragma unroll
+            MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                dv[u] = ld2_hint(d + 2 * MF_PI(u), vpol);
+                xv[u] = ld2_hint(x + 2 * MF_PI(u), vpol);
+                rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+            }
+#pragma unroll
+            MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                double2 xo, dn;
+                xo.x = xv[u].x + alpha * dv[u].x;
+                xo.y = xv[u].y + alpha * dv[u].y;
+                st2_hint(x + 2 * MF_PI(u), xo, vpol);
+                if (!done) {
+                    dn.x = rv[u].x + beta * dv[u].x;
+                    dn.y = rv[u].y + beta * dv[u].y;
+                    st2_hint(d + 2 * MF_PI(u), dn, vpol);
+                }
+            }
+        })
         rr = rrn;
         ++ep;
         publish(P, ep);
@@ -509,9 +622,10 @@ struct EpiDot {  // y = A p, dot += z*y
     const double *z;
     double *y;
     double dot;
-    __device__ double pre(int row) const { return __ldcg(z + row); }
+    uint64_t pol;
+    __device__ double pre(int row) const { return ld_hint(z + row, pol); }
     __device__ void operator()(int row, double acc, double zv) {
-        y[row] = acc;
+        st_hint(y + row, acc, pol);
         dot += zv * acc;
     }
 };
@@ -519,9 +633,10 @@ struct EpiDot2 {  // t = A s, ts += t*s, tt += t*t
     const double *s;
     double *t;
     double ts, tt;
-    __device__ double pre(int row) const { return __ldcg(s + row); }
+    uint64_t pol;
+    __device__ double pre(int row) const { return ld_hint(s + row, pol); }
     __device__ void operator()(int row, double acc, double sv) {
-        t[row] = acc;
+        st_hint(t + row, acc, pol);
         ts += acc * sv;
         tt += acc * acc;
     }
@@ -532,22 +647,32 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_bicgstab(KParams P) {
     __shared__ Smem S;
     kernel_setup(P, S, 1);
     const int g = blockIdx.x, tid = threadIdx.x;
-    uint32_t ph = 0, phase = 0;
+    Pipe pp;
+    uint32_t phase = 0;
+    const uint64_t vpol = policy_evict_last();
     const int rb_lo = P.lay[0].cta_rb[g], rb_hi = P.lay[0].cta_rb[g + 1];
-    const int row_lo = rb_lo * 16, row_hi = min(rb_hi * 16, P.rowA);
+    const int vlo = rb_lo * 16, vhi = rb_hi * 16;  // own rows, zero padded past rowA
     double *x = P.x, *r = P.r, *p = P.d, *v = P.q, *s = P.s, *t = P.t, *rh = P.rh;
     const double *b = P.b;
-    EpiResidual er{b, r, 0.0};
-    if (!cta_spmv<false>(P, 0, x, S, dyn, ph, er)) return;
+    EpiResidual er{b, r, 0.0, vpol};
+    if (!cta_spmv<false>(P, 0, x, S, dyn, pp, er)) return;
     __syncthreads();
     double bbp = 0.0, rhop = 0.0;
-    for (int i = row_lo + tid; i < row_hi; i += NTHREADS) {
-        const double ri = r[i];
-        rh[i] = ri;
-        p[i] = ri;
-        bbp += b[i] * b[i];
-        rhop += ri * ri;
-    }
+    MF_PAIRS(4, vlo, vhi, {
+        double2 rv[_vb], bv[_vb];
+#pragma unroll
+        MF_FOR_VB if (MF_LIVE(u, vhi)) {
+            rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+            bv[u] = ld2_hint(b + 2 * MF_PI(u), vpol);
+        }
+#pragma unroll
+        MF_FOR_VB if (MF_LIVE(u, vhi)) {
+            st2_hint(rh + 2 * MF_PI(u), rv[u], vpol);
+            st2_hint(p + 2 * MF_PI(u), rv[u], vpol);
+            bbp += bv[u].x * bv[u].x + bv[u].y * bv[u].y;
+            rhop += rv[u].x * rv[u].x + rv[u].y * rv[u].y;
+        }
+    })
     double v3[3] = {er.rr, bbp, rhop}, o3[3];
     if (!grid_sum<3>(P, S, v3, o3, phase)) return;
     double rr = o3[0];
@@ -563,8 +688,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_bicgstab(KParams P) {
     const int maxit = fixed ? P.fixed_iterations : P.maxiter;
     while (it < maxit && (fixed || rel > tol)) {
         if (!wait_deps(P, S, 0, ep)) return;
-        EpiDot ev{rh, v, 0.0};
-        if (!cta_spmv<false>(P, 0, p, S, dyn, ph, ev)) return;
+        EpiDot ev{rh, v, 0.0, vpol};
+        if (!cta_spmv<false>(P, 0, p, S, dyn, pp, ev)) return;
         double a1[1] = {ev.dot}, b1[1];
         if (!grid_sum<1>(P, S, a1, b1, phase)) return;
         if (!(b1[0] != 0.0) || !isfinite(b1[0])) {
@@ -572,12 +697,26 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_bicgstab(KParams P) {
             break;
         }
         const double alpha = rho / b1[0];
-        for (int i = row_lo + tid; i < row_hi; i += NTHREADS) s[i] = r[i] - alpha * v[i];
+        MF_PAIRS(4, vlo, vhi, {
+            double2 rv[_vb], vv[_vb];
+#pragma unroll
+            MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+                vv[u] = ld2_hint(v + 2 * MF_PI(u), vpol);
+            }
+#pragma unroll
+            MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                double2 o;
+                o.x = rv[u].x - alpha * vv[u].x;
+                o.y = rv[u].y - alpha * vv[u].y;
+                st2_hint(s + 2 * MF_PI(u), o, vpol);
+            }
+        })
         ++ep;
         publish(P, ep);
         if (!wait_deps(P, S, 0, ep)) return;
-        EpiDot2 et{s, t, 0.0, 0.0};
-        if (!cta_spmv<false>(P, 0, s, S, dyn, ph, et)) return;
+        EpiDot2 et{s, t, 0.0, 0.0, vpol};
+        if (!cta_spmv<false>(P, 0, s, S, dyn, pp, et)) return;
         double a2[2] = {et.ts, et.tt}, b2[2];
         if (!grid_sum<2>(P, S, a2, b2, phase)) return;
         if (!(b2[1] != 0.0) || !isfinite(b2[1])) {
@@ -586,14 +725,29 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_bicgstab(KParams P) {
         }
         const double omega = b2[0] / b2[1];
         double rrp = 0.0, rhp = 0.0;
-        for (int i = row_lo + tid; i < row_hi; i += NTHREADS) {
-            const double si = s[i];
-            x[i] = x[i] + alpha * p[i] + omega * si;
-            const double ri = si - omega * t[i];
-            r[i] = ri;
-            rrp += ri * ri;
-            rhp += ri * rh[i];
-        }
+        MF_PAIRS(2, vlo, vhi, {
+            double2 sv[_vb], xv[_vb], pv[_vb], tv[_vb], hv[_vb];
+#pragma unroll
+            MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                sv[u] = ld2_hint(s + 2 * MF_PI(u), vpol);
+                xv[u] = ld2_hint(x + 2 * MF_PI(u), vpol);
+                pv[u] = ld2_hint(p + 2 * MF_PI(u), vpol);
+                tv[u] = ld2_hint(t + 2 * MF_PI(u), vpol);
+                hv[u] = ld2_hint(rh + 2 * MF_PI(u), vpol);
+            }
+#pragma unroll
+            MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                double2 xo, ro;
+                xo.x = xv[u].x + alpha * pv[u].x + omega * sv[u].x;
+                xo.y = xv[u].y + alpha * pv[u].y + omega * sv[u].y;
+                st2_hint(x + 2 * MF_PI(u), xo, vpol);
+                ro.x = sv[u].x - omega * tv[u].x;
+                ro.y = sv[u].y - omega * tv[u].y;
+                st2_hint(r + 2 * MF_PI(u), ro, vpol);
+                rrp += ro.x * ro.x + ro.y * ro.y;
+                rhp += ro.x * hv[u].x + ro.y * hv[u].y;
+            }
+        })
         double a3[2] = {rhp, rrp}, b3[2];
         if (!grid_sum<2>(P, S, a3, b3, phase)) return;
         const double rho1 = b3[0];
@@ -606,7 +760,22 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_bicgstab(KParams P) {
         }
         if (!fixed && rel <= tol) break;
         const double beta = (rho1 * alpha) / (rho * omega);
-        for (int i = row_lo + tid; i < row_hi; i += NTHREADS) p[i] = r[i] + beta * (p[i] - omega * v[i]);
+        MF_PAIRS(4, vlo, vhi, {
+            double2 rv[_vb], pv[_vb], vv[_vb];
+#pragma unroll
+            MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+                pv[u] = ld2_hint(p + 2 * MF_PI(u), vpol);
+                vv[u] = ld2_hint(v + 2 * MF_PI(u), vpol);
+            }
+#pragma unroll
+            MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                double2 o;
+                o.x = rv[u].x + beta * (pv[u].x - omega * vv[u].x);
+                o.y = rv[u].y + beta * (pv[u].y - omega * vv[u].y);
+                st2_hint(p + 2 * MF_PI(u), o, vpol);
+            }
+        })
         rho = rho1;
         ++ep;
         publish(P, ep);
@@ -648,6 +817,12 @@ static int dyn_smem(int slab_max) { return STAGES * stage_stride_of(slab_max); }
 int kernel_config(mf_tiles *t, int *G_out) {
     const int slab_max = t->opt.slab_bytes > 0 ? t->opt.slab_bytes : SLAB_MAX_DEFAULT;
     const int dyn = dyn_smem(slab_max);
+    int optin = 0;
+    MF_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, t->device));
+    if (dyn + (int)sizeof(Smem) > optin) {
+        set_last_error("slab_bytes too large: the stage ring does not fit shared memory");
+        return MF_ERR_ARG;
+    }
     const void *kerns[] = {(const void *)k_cg<false>, (const void *)k_cg<true>, (const void *)k_bicgstab,
                            (const void *)k_spmv<false>, (const void *)k_spmv<true>};
     int occ_min = 1 << 30;

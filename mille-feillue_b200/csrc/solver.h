@@ -9,8 +9,9 @@
 
 namespace mf {
 
-constexpr int NWARPS = 16;                 // compute warps per CTA (2 row blocks each)
-constexpr int NTHREADS = NWARPS * 32;
+constexpr int NWARPS = 15;                 // consumer warps per CTA (2 row blocks each)
+constexpr int PRODUCER_WARP = NWARPS;      // one more warp issues the bulk copies
+constexpr int NTHREADS = (NWARPS + 1) * 32;
 constexpr int KMAX_LAYOUTS = 1 + MF_NLEVELS;
 constexpr int FLAG_STRIDE = 8;             // one 32-byte sector per CTA flag
 enum { SYNC_ARRIVE = 0, SYNC_ERROR = 32, SYNC_SITE = 33, SYNC_FLAGS = 64 };

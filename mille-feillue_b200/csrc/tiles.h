@@ -53,25 +53,30 @@ struct DevArray {
 // 16-byte aligned byte range so that one bulk copy brings it into shared
 // memory. Byte layout (every section 16-byte aligned):
 //   SlabHeader (32 B)
-//   runs[MAXRUNS]           x-segment runs to stage for the slab that the
-//                           CTA consumes STAGES slabs later (issue record)
-//   rbdir[nrb + 1]          per row block: value byte offset, first tile,
-//                           first column byte
-//   slot[ntiles]  (u32)     staged x-segment slot (or, in gather mode, the
-//                           tile column) | precision << 30
-//   rowend[ntiles][16] (u8) inclusive end of each row inside the tile
-//                           (row 15's end 256 stored as 0)
-//   vals                    per tile: FP64 8n | FP32 4n | FP16 4+2n | FP8 4+n
-//                           bytes, each block 8-byte aligned, FP16/FP8 blocks
-//                           start with a float power-of-two scale
-//   cols[nnz]     (u8)      intra-tile column (Tile_csr_Col)
-constexpr int STAGES = 3;
+//   runs[MAXRUNS]       x-segment runs to stage for the slab that the CTA
+//                       consumes STAGES slabs later (issue record)
+//   rbdir[nrb + 1]      per row block: byte offset of its block, plane count
+//   row-block blocks    one per row block, "row-sliced planes":
+//     rowlen[16]  (u8)  entries of each of the 16 rows
+//     pdesc[W]          (mixed layouts only) per plane: value offset, storage
+//                       precision, power-of-two scale
+//     idx[W][16]        u16 x-window position (staged) or u32 column
+//                       (gather) of entry k of row r, with the flags
+//                       TILE_START (first entry of a new tile in this row)
+//                       and LOW (the entry's tile is below FP64)
+//     vals              plane k holds entry k of the 16 rows: FP64 16x8 B,
+//                       or in mixed layouts FP64/FP32/FP16/FP8 16xwidth B
+// Entry k of row r is the k-th entry of the row in the reference's order:
+// tiles in ascending column, entries of the row inside a tile in CSR order.
+constexpr int STAGES = 4;
 constexpr int MAXRUNS = 24;
-constexpr int XSEG_MAX = 128;      // staged x segments per slab (16 KB)
-constexpr int MAXT = 2048;         // tiles per slab
+constexpr int XSEG_MAX = 112;      // staged x segments per slab (14 KB)
+constexpr int MAXW = 255;          // planes per row block (rowlen is u8)
 constexpr int SLAB_MAX_DEFAULT = 40960;
-constexpr int RB_PER_SLAB_MAX = 32;
+constexpr int RB_PER_SLAB_MAX = 30;  // 2 per consumer warp
 constexpr int ISSUE_REC = 16 + MAXRUNS * 8;
+constexpr uint32_t IDX16_START = 0x8000u, IDX16_LOW = 0x4000u, IDX16_POS = 0x3fffu;
+constexpr uint32_t IDX32_START = 0x80000000u, IDX32_LOW = 0x40000000u, IDX32_POS = 0x3fffffffu;
 
 enum { SLAB_STAGED = 0, SLAB_GATHER = 1, SLAB_OVERSIZE = 2 };
 
@@ -79,7 +84,7 @@ struct SlabHeader {
     int32_t rb0;
     uint16_t nrb, ntiles;
     uint16_t nxseg, mode;
-    uint16_t next_nruns, cols16;  // cols16: byte offset of cols / 16
+    uint16_t next_nruns, mixed;
     uint32_t next_off16;  // issue record of the slab consumed STAGES later
     uint32_t next_bytes;  // 0 = none
     uint32_t next_xbytes;
@@ -93,37 +98,33 @@ struct XRun {
 };
 
 struct RbDir {
-    uint32_t val_off;
-    uint16_t tile0, col0;
+    uint32_t off;  // byte offset of the row-block block from the slab start
+    uint32_t W;    // planes
 };
 
-struct SlabOffsets {
-    uint32_t runs, rbdir, slot, rowend, vals, cols, total;
+struct PlaneDesc {
+    uint16_t voff;  // value offset inside the block's vals section
+    uint8_t prec, pad;
+    float scale;
 };
 
 __host__ __device__ inline uint32_t align16u(uint32_t v) { return (v + 15u) & ~15u; }
 __host__ __device__ inline uint32_t align8u(uint32_t v) { return (v + 7u) & ~7u; }
 
-__host__ __device__ inline SlabOffsets slab_offsets(int nrb, int ntiles, uint32_t valbytes, int nnz) {
-    SlabOffsets o;
-    o.runs = 32;
-    o.rbdir = align16u(o.runs + 8u * MAXRUNS);
-    o.slot = align16u(o.rbdir + 8u * (uint32_t)(nrb + 1));
-    o.rowend = align16u(o.slot + 4u * (uint32_t)ntiles);
-    o.vals = o.rowend + 16u * (uint32_t)ntiles;
-    o.cols = align16u(o.vals + valbytes);
-    o.total = align16u(o.cols + (uint32_t)nnz);
-    return o;
-}
+__host__ __device__ inline uint32_t slab_rbdir_off() { return align16u(32u + 8u * MAXRUNS); }
+__host__ __device__ inline uint32_t slab_blocks_off(int nrb) { return align16u(slab_rbdir_off() + 8u * (nrb + 1)); }
 
-// Bytes of one tile's value block in the slab layout.
-__host__ __device__ inline uint32_t tile_val_bytes(int prec, int nnz) {
-    switch (prec) {
-        case MF_PREC_FP64: return 8u * nnz;
-        case MF_PREC_FP32: return align8u(4u * nnz);
-        case MF_PREC_FP16: return align8u(4u + 2u * nnz);
-        default: return align8u(4u + (uint32_t)nnz);
-    }
+// Offsets inside one row-block block.
+__host__ __device__ inline uint32_t rb_pdesc_off() { return 16u; }
+__host__ __device__ inline uint32_t rb_idx_off(int W, bool mixed) { return mixed ? align16u(16u + 8u * W) : 16u; }
+__host__ __device__ inline uint32_t rb_vals_off(int W, bool mixed, bool gather) {
+    return align16u(rb_idx_off(W, mixed) + (uint32_t)W * 16u * (gather ? 4u : 2u));
+}
+__host__ __device__ inline uint32_t rb_block_bytes(int W, bool mixed, bool gather, uint32_t valbytes) {
+    return align16u(rb_vals_off(W, mixed, gather) + valbytes);
+}
+__host__ __device__ inline uint32_t prec_width(int prec) {
+    return prec == MF_PREC_FP64 ? 8u : prec == MF_PREC_FP32 ? 4u : prec == MF_PREC_FP16 ? 2u : 1u;
 }
 
 // Algorithmic bytes of one tile (value bytes + 1 column byte per nnz + 8 per
@@ -144,6 +145,7 @@ struct Layout {
     std::vector<uint8_t> prec;   // host copy of the precisions
     int G = 0, nslabs = 0, n_gather = 0, n_oversize = 0;
     int slab_max = 0, rb_per_slab = 0;  // stage size / row blocks the planner used
+    bool mixed = false;                  // plane descriptors present
     size_t bytes = 0;
     double alg_bytes = 0;        // algorithmic bytes of one SpMV
     double tile_frac[4] = {0, 0, 0, 0};

@@ -543,6 +543,10 @@ double mfo_tile_scale(int prec, double maxabs) {
 
 void mfo_mixed_spmv(const mfo_tiles *t, const unsigned char *prec, const double *x,
                     double *y) {
+    /* Per tile: FP64 tiles sum = 0; sum += x * v; acc += sum. Tiles below
+     * FP64 use the dequantized value v_q (FP32: (float)v; FP16 / FP8:
+     * decode(encode(v / s)) * s with the tile's power-of-two scale s), and
+     * sumf = fmaf((float)x, (float)v_q, sumf); acc += (double)sumf. */
 #pragma omp parallel for schedule(static)
     for (int rb = 0; rb < t->tilem; ++rb) {
         int rl = rowlen_of(t, rb);
@@ -565,22 +569,21 @@ void mfo_mixed_spmv(const mfo_tiles *t, const unsigned char *prec, const double 
                 int sp = ri == rl - 1 ? nk : bp[ri + 1];
                 if (p == 0) {
                     double sum = 0.0;
-                    for (int q = st; q < sp; ++q) {
+                    for (int q = st; q < sp; ++q)
                         sum += x[xo + t->Tile_csr_Col[vo + q]] * t->Blockcsr_Val[vo + q];
-                    }
                     acc[ri] += sum;
                 } else {
                     float sum = 0.0f;
                     for (int q = st; q < sp; ++q) {
                         double v = t->Blockcsr_Val[vo + q];
-                        float vf;
-                        if (p == 1) vf = (float)v;
-                        else if (p == 2) vf = (float)mfo_fp16_decode(mfo_fp16_encode(v / scale));
-                        else vf = (float)mfo_fp8_e4m3_decode(mfo_fp8_e4m3_encode(v / scale));
+                        double vq;
+                        if (p == 1) vq = (float)v;
+                        else if (p == 2) vq = mfo_fp16_decode(mfo_fp16_encode(v / scale)) * scale;
+                        else vq = mfo_fp8_e4m3_decode(mfo_fp8_e4m3_encode(v / scale)) * scale;
                         float xf = (float)x[xo + t->Tile_csr_Col[vo + q]];
-                        sum = fmaf(xf, vf, sum);
+                        sum = fmaf(xf, (float)vq, sum);
                     }
-                    acc[ri] += (double)sum * scale;
+                    acc[ri] += (double)sum;
                 }
             }
         }

@@ -82,8 +82,9 @@ double mfo_fp16_decode(uint16_t h);
 double mfo_tile_scale(int prec, double maxabs);
 
 /* Mixed-precision tiled SpMV: tile t stored at prec[t] (0 fp64, 1 fp32,
- * 2 fp16, 3 fp8) with scale 2^e; low-precision tiles multiply in FP32 with
- * fmaf accumulation in CSR order, then add sum*scale to the FP64 row total. */
+ * 2 fp16, 3 fp8) with scale 2^e; low-precision tiles multiply their
+ * dequantized values in FP32 with fmaf accumulation in CSR order, then add
+ * the FP32 tile sum to the FP64 row total. */
 void mfo_mixed_spmv(const mfo_tiles *t, const unsigned char *prec, const double *x,
                     double *y);
 

@@ -67,7 +67,17 @@ def test_encoder_matches_golden(mf, golden):
             assert np.array_equal(ex[name], g[name]), (case, name)
         assert np.array_equal(ex["ptroffset1"], g["ptroffset1"]) and np.array_equal(ex["ptroffset2"], g["ptroffset2"])
         if rowA == n:
-            assert np.array_equal(t.spmv(g["x"]), g["y"]), case
+            y = t.spmv(g["x"])
+            if rowA % 16 == 1:
+                # Tile_create copies no values for a 1-row tail block
+                # (csr2block.h:237-251), so the reference returns 0 there;
+                # the device tiles keep the row and return the true product.
+                assert np.array_equal(y[:-1], g["y"][:-1]) and g["y"][-1] == 0.0, case
+                rp_, ci_, v_ = g["row_ptr"], g["col_idx"], g["val"]
+                last = sum(v_[k] * g["x"][ci_[k]] for k in range(rp_[rowA - 1], rp_[rowA]))
+                assert np.isclose(y[-1], last, rtol=1e-13, atol=1e-13), case
+            else:
+                assert np.array_equal(y, g["y"]), case
 
 
 def test_encoder_matches_oracle(mf, O, cases):
