@@ -182,6 +182,28 @@ def cpu_reference_arm(args, rank):
     }
 
 
+def _time_solves(torch, tiles, bd, xd, opts, steps, warmup, dist):
+    res = None
+    for _ in range(warmup):
+        xd.zero_()
+        res = tiles.solve_cg_dev(bd.data_ptr(), xd.data_ptr(), TOL, MAXITER, opts)
+    torch.cuda.synchronize()
+    _barrier(dist)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    kernel_ms = []
+    e0.record()
+    for _ in range(steps):
+        xd.zero_()
+        res = tiles.solve_cg_dev(bd.data_ptr(), xd.data_ptr(), TOL, MAXITER, opts)
+        kernel_ms.append(res["time_ms"])
+    e1.record()
+    torch.cuda.synchronize()
+    _barrier(dist)
+    ms = _max_over_ranks(dist, e0.elapsed_time(e1) / steps)
+    return ms, statistics.median(kernel_ms), res
+
+
 def gpu_arm(args, world, rank, local, dist):
     import torch
 
@@ -193,51 +215,37 @@ def gpu_arm(args, world, rank, local, dist):
     rp, ci, v = A.csr()
     b = A.b()
     xstar = A.xstar()
-    mode = args.mode
-    popts = dict(device=dev)
-    if mode == "mixed":
-        popts.update(precision_mode=mf.MODE_MIXED_RULE)
-    opts = mf.options(**popts)
+    opts64 = mf.options(device=dev)
+    optsmx = mf.options(device=dev, precision_mode=mf.MODE_MIXED_RULE)
     t_enc0 = time.perf_counter()
-    tiles = mf.Tiles(A, opts)
+    tiles = mf.Tiles(A, optsmx)  # FP64 layout + mixed-precision levels
     enc_s = time.perf_counter() - t_enc0
     info = tiles.info()
     bd = torch.tensor(b, device=f"cuda:{dev}")
     xd = torch.zeros(n, dtype=torch.float64, device=f"cuda:{dev}")
     launches_per_solve = 3  # persistent solver kernel + true-residual SpMV + norm kernel
+    headline = args.mode
+    opts = optsmx if headline == "mixed" else opts64
 
-    # ---- standalone SpMV (FP64 layout): roofline of the streamed kernel
+    # ---- standalone SpMV: roofline of the streamed kernel (FP64 and level 0)
     xs = torch.tensor(xstar, device=f"cuda:{dev}")
     ys = torch.zeros(n, dtype=torch.float64, device=f"cuda:{dev}")
     spmv_ms, spmv_bytes = tiles.spmv_bench(xs.data_ptr(), ys.data_ptr(), 50)
+    spmv_mx_ms, spmv_mx_bytes = tiles.spmv_bench(xs.data_ptr(), ys.data_ptr(), 50, level=0)
     peak, peak_kind = _peaks()
 
-    # ---- warm-up solves
-    for _ in range(args.warmup):
-        xd.zero_()
-        res = tiles.solve_cg_dev(bd.data_ptr(), xd.data_ptr(), TOL, MAXITER, opts)
-    torch.cuda.synchronize()
-    _barrier(dist)
     clocks = ClockSampler(dev)
     clocks.start()
-    torch.cuda.synchronize()
-    _barrier(dist)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    kernel_ms = []
-    e0.record()
-    for _ in range(args.steps):
-        xd.zero_()
-        res = tiles.solve_cg_dev(bd.data_ptr(), xd.data_ptr(), TOL, MAXITER, opts)
-        kernel_ms.append(res["time_ms"])
-    e1.record()
-    torch.cuda.synchronize()
-    _barrier(dist)
-    ms = e0.elapsed_time(e1) / args.steps
-    ms = _max_over_ranks(dist, ms)
+    ms64, k64, res64 = _time_solves(torch, tiles, bd, xd, opts64, args.steps, args.warmup, dist)
+    x64 = xd.cpu().numpy()
+    msmx, kmx, resmx = _time_solves(torch, tiles, bd, xd, optsmx, args.steps, args.warmup, dist)
+    xmx = xd.cpu().numpy()
     clk = clocks.stop()
-    x = xd.cpu().numpy()
-    err = float(np.linalg.norm(x - xstar) / np.linalg.norm(xstar))
+    nx = np.linalg.norm(x64)
+    err64 = float(np.linalg.norm(x64 - xstar) / np.linalg.norm(xstar))
+    errmx = float(np.linalg.norm(xmx - xstar) / np.linalg.norm(xstar))
+    mx_vs_64 = float(np.linalg.norm(xmx - x64) / nx)
+    ms, kms, res = (msmx, kmx, resmx) if headline == "mixed" else (ms64, k64, res64)
 
     # ---- end to end through the C ABI with pinned host buffers:
     # CSR + b host->device, GPU encode, persistent solve, x device->host
@@ -267,9 +275,11 @@ def gpu_arm(args, world, rank, local, dist):
     h2d = rp.nbytes + ci.nbytes + v.nbytes + b.nbytes + n * 8  # CSR, b, x0
     d2h = n * 8 + 8  # x and the result scalars
 
-    iters = res["iterations"]
-    it_bytes = spmv_bytes + 56.0 * n  # per-iteration algorithmic bytes (SpMV + fused vector pass)
-    solve_gbs = iters * it_bytes / (statistics.median(kernel_ms) * 1e-3) / 1e9
+    def roof(r, kernel_ms):
+        gbs = r["total_bytes"] / (kernel_ms * 1e-3) / 1e9
+        return gbs
+
+    gbs = roof(res, kms)
     out = None
     if rank == 0:
         out = {
@@ -277,17 +287,30 @@ def gpu_arm(args, world, rank, local, dist):
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "varpoisson3d_128 CG to 1e-10 true residual", "n": n, "nnz": int(len(v)),
-                       "mode": mode, "x0": "zeros", "tol": TOL, "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "matrix (%.0f MB) larger than L2; not flushed" % (spmv_bytes / 1e6),
+                       "mode": headline, "x0": "zeros", "tol": TOL,
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "matrix (%.0f MB FP64) larger than L2; not flushed" % (spmv_bytes / 1e6),
                        "ctas": info["nctas"], "slabs": info["nslabs"]},
-            "iterations": iters, "rel_residual_true": res["rel_residual_true"], "x_err_vs_xstar": err,
-            "kernel_ms": statistics.median(kernel_ms),
-            "roofline": {"bound": "hbm", "achieved": solve_gbs, "peak": peak, "unit": "GB/s",
-                         "frac": solve_gbs / peak, "traffic": None, "peak_kind": peak_kind,
-                         "kernel": "k_cg (persistent solve), bytes = iterations x (B_spmv + 56 n)"},
-            "spmv": {"ms": spmv_ms, "alg_bytes": spmv_bytes, "gbs": spmv_bytes / spmv_ms / 1e6,
-                     "frac": spmv_bytes / spmv_ms / 1e6 / peak,
-                     "gflops": 2.0 * len(v) / spmv_ms / 1e6},
+            "iterations": res["iterations"], "rel_residual_true": res["rel_residual_true"],
+            "mixed": {"ms": msmx, "kernel_ms": kmx, "iterations": resmx["iterations"],
+                      "iters_per_level": resmx["iters_level"], "replacements": resmx["replacements"],
+                      "level_switches": resmx["level_switches"], "tile_frac_final": resmx["tile_frac"],
+                      "rel_residual_true": resmx["rel_residual_true"], "x_err_vs_xstar": errmx,
+                      "x_diff_vs_fp64": mx_vs_64, "spmv_bytes_level": resmx["spmv_bytes_level"]},
+            "fp64": {"ms": ms64, "kernel_ms": k64, "iterations": res64["iterations"],
+                     "rel_residual_true": res64["rel_residual_true"], "x_err_vs_xstar": err64,
+                     "roofline_gbs": roof(res64, k64), "roofline_frac": roof(res64, k64) / peak},
+            "speedup_mixed_vs_fp64": ms64 / msmx,
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                         "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "k_cg (persistent solve); bytes = every SpMV's algorithmic bytes "
+                                   "+ 56 n per iteration"},
+            "spmv": {"fp64": {"ms": spmv_ms, "alg_bytes": spmv_bytes, "gbs": spmv_bytes / spmv_ms / 1e6,
+                              "frac": spmv_bytes / spmv_ms / 1e6 / peak, "gflops": 2.0 * len(v) / spmv_ms / 1e6},
+                     "mixed_level0": {"ms": spmv_mx_ms, "alg_bytes": spmv_mx_bytes,
+                                      "gbs": spmv_mx_bytes / spmv_mx_ms / 1e6,
+                                      "frac": spmv_mx_bytes / spmv_mx_ms / 1e6 / peak,
+                                      "gflops": 2.0 * len(v) / spmv_mx_ms / 1e6}},
             "clocks": clk,
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "path": "mf_encode(host CSR) + mf_solve_cg(host b, host x) + mf_free"},
@@ -297,17 +320,91 @@ def gpu_arm(args, world, rank, local, dist):
     return out
 
 
+def batch_arm(args, world, rank, local, dist):
+    """512 random SPD systems, n log-uniform in [1e3, 2e5] (seed 2), FP64 CG
+    to 1e-10: one persistent launch (CUDA-graph replay) against one
+    single-system launch per system. With N ranks the systems are split by
+    longest-processing-time on nnz (no collective in the solve)."""
+    import torch
+
+    mf = importlib.import_module("mille-feillue_b200")
+    dev = local
+    torch.cuda.set_device(dev)
+    sizes = mf.batch_sizes(512, 1000, 200000, 2)
+    # LPT split of the systems over ranks by estimated nnz (17 per row)
+    loads = [0.0] * world
+    mine = []
+    for s in sorted(range(len(sizes)), key=lambda i: -sizes[i]):
+        rk = min(range(world), key=lambda k: loads[k])
+        loads[rk] += float(sizes[s])
+        if rk == rank:
+            mine.append(s)
+    mine.sort()
+    t0 = time.perf_counter()
+    mats = mf.generate_spd_batch([sizes[s] for s in mine], seed=2)
+    # generate_spd_batch seeds by position; reseed by global index
+    mats = [mf.Matrix.spd_random(int(sizes[s]), 2 * 1000003 + s + 1) for s in mine] if world > 1 else mats
+    gen_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    B = mf.Batch(mats, mf.options(device=dev), with_baseline=not args.no_each)
+    enc_s = time.perf_counter() - t0
+    b = np.concatenate([m.b() for m in mats])
+    bd = torch.tensor(b, device=f"cuda:{dev}")
+    xd = torch.zeros_like(bd)
+    for _ in range(args.warmup):
+        B.solve_cg_dev(bd.data_ptr(), xd.data_ptr(), TOL, 10000)
+    torch.cuda.synchronize()
+    _barrier(dist)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        B.solve_cg_dev(bd.data_ptr(), xd.data_ptr(), TOL, 10000)
+    e1.record()
+    torch.cuda.synchronize()
+    _barrier(dist)
+    clk = clocks.stop()
+    ms = _max_over_ranks(dist, e0.elapsed_time(e1) / args.steps)
+    it, st, rel = B.results()
+    each_ms = None
+    if not args.no_each:
+        xe = torch.zeros_like(bd)
+        B.solve_cg_each_dev(bd.data_ptr(), xe.data_ptr(), TOL, 10000)  # warm
+        each_ms = _max_over_ranks(dist, B.solve_cg_each_dev(bd.data_ptr(), xe.data_ptr(), TOL, 10000))
+    inf = B.info()
+    if rank != 0:
+        return None
+    return {
+        "metric": "batched solve time to 1e-10 (512 SPD systems)", "value": ms, "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "batch512_spd n~logU[1e3,2e5] seed 2, CG to 1e-10", "systems": len(mats),
+                   "rows_rank0": inf["rows"], "nnz_rank0": inf["nnz"], "grid": inf["grid"],
+                   "parallelism": f"systems split over {world} ranks (LPT)" if world > 1 else "single"},
+        "iterations_min_max": [int(it.min()), int(it.max())], "all_converged": bool(np.all(st == 0)),
+        "max_rel_residual": float(rel.max()),
+        "one_launch_per_system_ms": each_ms,
+        "speedup_vs_one_launch_per_system": (each_ms / ms) if each_ms else None,
+        "clocks": clk, "gen_s": gen_s, "encode_s": enc_s,
+        "gpu_launches": args.steps * 3,
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--mode", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-sample-iters", type=int, default=20)
     ap.add_argument("--fp64-iters", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="poisson128", choices=["poisson128", "batch"])
+    ap.add_argument("--no-each", action="store_true", help="batch: skip the one-launch-per-system comparison")
     args = ap.parse_args()
     world, rank, local, dist = _dist_setup(args)
     if args.impl == "reference":
@@ -315,11 +412,19 @@ def main():
         if out is not None:
             print(json.dumps(out))
         return
+    if args.workload == "batch":
+        out = batch_arm(args, world, rank, local, dist)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        if out is not None:
+            print(json.dumps(out))
+        return
     out = gpu_arm(args, world, rank, local, dist)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         a2 = argparse.Namespace(**vars(args))
         a2.steps, a2.warmup = 1, 1
-        a2.fp64_iters = args.fp64_iters or out["iterations"] if args.mode == "fp64" else args.fp64_iters
+        a2.fp64_iters = args.fp64_iters or out["fp64"]["iterations"]
         ref = cpu_reference_arm(a2, 0)
         out["cpu_baseline"] = ref["cpu_baseline"]
     if dist is not None:

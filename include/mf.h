@@ -67,7 +67,7 @@ typedef struct {
     int replace_every;       /* true-residual replacement period of the mixed
                                 precision modes (FP64 mode never replaces)    */
     int ctas_per_sm;         /* persistent CTAs per SM, 0 = autotune           */
-    int rb_per_slab;         /* row blocks per slab, 0 = default (30)          */
+    int rb_per_slab;         /* row blocks per slab, 0 = default (60 at most)  */
     int slab_bytes;          /* max bytes of one streamed slab, 0 = default    */
     double timeout_s;        /* limit of every device spin-wait, 0 = 2 s       */
     int check_true_residual; /* confirm convergence with b - A x (default 1)   */
@@ -76,7 +76,12 @@ typedef struct {
     int device;              /* CUDA device ordinal                            */
     int reserved[7];         /* reserved[0] == 0x5741: test hook, the CG kernel
                                 first waits on a flag nothing sets, so the
-                                bounded wait must end it with MF_ERR_TIMEOUT */
+                                bounded wait must end it with MF_ERR_TIMEOUT;
+                                reserved[1] = N > 0: trace the first N CG
+                                iterations (see mf_trace); reserved[2] = 1:
+                                mixed layouts use the classic two-reduction
+                                CG instead of the single-reduction
+                                (Chronopoulos-Gear) form                      */
 } mf_options;
 void mf_options_default(mf_options *opt);
 
@@ -93,7 +98,16 @@ typedef struct {
     double spmv_bytes_fp64;  /* algorithmic bytes of one FP64 SpMV             */
     double tile_frac[4];     /* fraction of tiles per MF_PREC_* at the end     */
     int error_site;          /* device error site code (0 = none)              */
-    int reserved[7];
+    int iters_fp64;          /* iterations whose SpMV used the FP64 layout     */
+    int iters_level[3];      /* iterations per mixed-precision level           */
+    double spmv_bytes_level[3]; /* algorithmic bytes of one SpMV per level     */
+    double total_bytes;      /* algorithmic bytes of the whole solve: every
+                                SpMV (replacements included) + 56 n per
+                                iteration of vector traffic                   */
+    int fell_back_fp64;      /* 1 if a low-precision level let the true
+                                residual grow and the solve finished on the
+                                FP64 layout                                   */
+    int reserved2;
 } mf_result;
 
 /* ---- opaque handles --------------------------------------------------- */
@@ -219,9 +233,37 @@ int mf_solve_bicgstab(mf_tiles *t, const double *b_host, double *x_host,
 int mf_solve_bicgstab_dev(mf_tiles *t, const double *b_dev, double *x_dev,
                           double tol, int maxiter, const mf_options *opt,
                           mf_result *res);
+/* Phase timestamps (ns, %globaltimer of CTA 0) of the last traced CG solve:
+ * out[8*i + s] for iteration i, slot s = 0 iteration start, 1 halo ready,
+ * 2 SpMV done, 3 alpha known, 4 r updated, 5 beta known, 6 x / d published.
+ * Returns the number of iterations written.                                 */
+int mf_trace(const mf_tiles *t, unsigned long long *out, int max_iters);
 /* ||b - A x|| / ||b|| with the FP64 tiled SpMV (device vectors).             */
 int mf_true_residual(mf_tiles *t, const double *b_dev, const double *x_dev,
                      double *rel);
+
+/* ---- batched solve of many independent systems ------------------------- */
+/* Encodes `count` square systems (host CSR) for one persistent launch in
+ * which every CTA solves whole systems taken from a device queue, largest
+ * first. with_baseline != 0 also builds whole-GPU layouts for
+ * mf_batch_solve_cg_each_dev (one launch per system, for comparison).       */
+typedef struct mf_batch mf_batch;
+int mf_batch_create(int count, const mf_csr *systems, const mf_options *opt,
+                    int with_baseline, mf_batch **out);
+/* FP64 CG on every system. b / x: device arrays holding the systems' vectors
+ * back to back in creation order (x0 = 0). The solve is captured in a CUDA
+ * graph on first use and replayed; *ms = device time of the replay.         */
+int mf_batch_solve_cg_dev(mf_batch *B, const double *b_dev, double *x_dev,
+                          double tol, int maxiter, double *ms);
+/* The same systems with one single-system solver launch each.               */
+int mf_batch_solve_cg_each_dev(mf_batch *B, const double *b_dev, double *x_dev,
+                               double tol, int maxiter, double *ms);
+/* Per-system iterations, status and recursive relative residual.            */
+int mf_batch_results(const mf_batch *B, int *iterations, int *status,
+                     double *rel_residual);
+int mf_batch_info(const mf_batch *B, long long *total_rows,
+                  long long *total_nnz, int *grid);
+void mf_batch_free(mf_batch *B);
 
 /* ---- drop-in replacements of the reference entry points --------------- */
 /* Same signature as the reference. n is truncated to a multiple of 16 as

@@ -57,7 +57,9 @@ class MfResult(C.Structure):
     _fields_ = [
         ("status", _i), ("iterations", _i), ("replacements", _i), ("level_switches", _i),
         ("rel_residual_true", _d), ("rel_residual_rec", _d), ("time_ms", _d), ("spmv_bytes", _d),
-        ("spmv_bytes_fp64", _d), ("tile_frac", _d * 4), ("error_site", _i), ("reserved", _i * 7),
+        ("spmv_bytes_fp64", _d), ("tile_frac", _d * 4), ("error_site", _i), ("iters_fp64", _i),
+        ("iters_level", _i * 3), ("spmv_bytes_level", _d * 3), ("total_bytes", _d),
+        ("fell_back_fp64", _i), ("reserved2", _i),
     ]
 
     def as_dict(self):
@@ -66,7 +68,9 @@ class MfResult(C.Structure):
             "level_switches": self.level_switches, "rel_residual_true": self.rel_residual_true,
             "rel_residual_rec": self.rel_residual_rec, "time_ms": self.time_ms,
             "spmv_bytes": self.spmv_bytes, "spmv_bytes_fp64": self.spmv_bytes_fp64,
-            "tile_frac": list(self.tile_frac), "error_site": self.error_site,
+            "tile_frac": list(self.tile_frac), "error_site": self.error_site, "iters_fp64": self.iters_fp64,
+            "iters_level": list(self.iters_level), "spmv_bytes_level": list(self.spmv_bytes_level),
+            "total_bytes": self.total_bytes, "fell_back_fp64": self.fell_back_fp64,
         }
 
 
@@ -103,7 +107,8 @@ EXPORTED = [
     "mf_tiles_export", "mf_tiles_precisions", "mf_tiles_set_precisions", "mf_balance_twopointer", "mf_spmv",
     "mf_spmv_host", "mf_spmv_bench", "mf_solve_cg", "mf_solve_cg_dev", "mf_solve_bicgstab",
     "mf_solve_bicgstab_dev", "mf_true_residual", "cg_solve_inc", "bicgstab", "mf_version", "mf_last_error",
-    "mf_spmv_level", "mf_spmv_bench_level",
+    "mf_spmv_level", "mf_spmv_bench_level", "mf_trace", "mf_batch_create", "mf_batch_solve_cg_dev",
+    "mf_batch_solve_cg_each_dev", "mf_batch_results", "mf_batch_info", "mf_batch_free",
 ]
 
 _lib = None
@@ -155,6 +160,13 @@ def lib():
     for f in ("mf_solve_cg", "mf_solve_cg_dev", "mf_solve_bicgstab", "mf_solve_bicgstab_dev"):
         getattr(L, f).argtypes = [_p, _p, _p, _d, _i, C.POINTER(MfOptions), C.POINTER(MfResult)]
     L.mf_true_residual.argtypes = [_p, _p, _p, C.POINTER(_d)]
+    L.mf_trace.argtypes = [_p, _p, _i]
+    L.mf_batch_create.argtypes = [_i, _p, C.POINTER(MfOptions), _i, C.POINTER(_p)]
+    L.mf_batch_solve_cg_dev.argtypes = [_p, _p, _p, _d, _i, C.POINTER(_d)]
+    L.mf_batch_solve_cg_each_dev.argtypes = [_p, _p, _p, _d, _i, C.POINTER(_d)]
+    L.mf_batch_results.argtypes = [_p, _p, _p, _p]
+    L.mf_batch_info.argtypes = [_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(_i)]
+    L.mf_batch_free.argtypes = [_p]
     L.cg_solve_inc.argtypes = [_p, _p, _p, _p, _p, _p, _i, C.POINTER(_i), _i, _d, C.c_char_p, _i, _i, _i]
     L.cg_solve_inc.restype = None
     L.bicgstab.argtypes = [_p, _p, _p, _p, _p, _i, C.c_char_p, _i, _i]
@@ -402,10 +414,72 @@ class Tiles:
     def solve_bicgstab_dev(self, b_ptr, x_ptr, tol=1e-10, maxiter=10000, opts=None):
         return self._solve_dev(lib().mf_solve_bicgstab_dev, b_ptr, x_ptr, tol, maxiter, opts)
 
+    def trace(self, max_iters=4096):
+        """Phase timestamps of the last traced CG solve, shape (iters, 8)."""
+        buf = np.zeros(max_iters * 8, np.uint64)
+        n = lib().mf_trace(self.h, _ptr(buf), max_iters)
+        return buf[: max(n, 0) * 8].reshape(-1, 8)
+
     def __del__(self):
         try:
             if self.h:
                 lib().mf_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def generate_spd_batch(sizes, seed=2, threads=16):
+    """The random SPD systems of a batch (system s drawn with seed
+    seed * 1000003 + s + 1), generated in parallel host threads."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        return list(ex.map(lambda a: Matrix.spd_random(int(a[1]), seed * 1000003 + a[0] + 1), enumerate(sizes)))
+
+
+class Batch:
+    """Many independent systems solved by one persistent launch (mf_batch)."""
+
+    def __init__(self, matrices, opts=None, with_baseline=False):
+        self._mats = list(matrices)
+        arr = (MfCsr * len(self._mats))(*[m.csr_struct() for m in self._mats])
+        self.h = _p()
+        o = opts if opts is not None else options()
+        _check(lib().mf_batch_create(len(self._mats), C.cast(arr, _p), C.byref(o), 1 if with_baseline else 0,
+                                     C.byref(self.h)), "mf_batch_create")
+        self.sizes = np.array([m.n for m in self._mats], np.int64)
+        self.offsets = np.concatenate([[0], np.cumsum(self.sizes)])
+
+    def info(self):
+        r, z, g = C.c_longlong(), C.c_longlong(), _i()
+        lib().mf_batch_info(self.h, C.byref(r), C.byref(z), C.byref(g))
+        return {"rows": r.value, "nnz": z.value, "grid": g.value}
+
+    def solve_cg_dev(self, b_ptr, x_ptr, tol=1e-10, maxiter=10000):
+        ms = _d()
+        rc = lib().mf_batch_solve_cg_dev(self.h, _p(b_ptr), _p(x_ptr), tol, maxiter, C.byref(ms))
+        _check(rc, "mf_batch_solve_cg_dev")
+        return ms.value
+
+    def solve_cg_each_dev(self, b_ptr, x_ptr, tol=1e-10, maxiter=10000):
+        ms = _d()
+        _check(lib().mf_batch_solve_cg_each_dev(self.h, _p(b_ptr), _p(x_ptr), tol, maxiter, C.byref(ms)),
+               "mf_batch_solve_cg_each_dev")
+        return ms.value
+
+    def results(self):
+        n = len(self._mats)
+        it = np.zeros(n, np.int32)
+        st = np.zeros(n, np.int32)
+        rel = np.zeros(n, np.float64)
+        _check(lib().mf_batch_results(self.h, _ptr(it), _ptr(st), _ptr(rel)), "mf_batch_results")
+        return it, st, rel
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().mf_batch_free(self.h)
                 self.h = None
         except Exception:
             pass

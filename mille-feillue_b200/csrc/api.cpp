@@ -76,8 +76,13 @@ static int fetch_host_tiles(mf_tiles *t) {
     return MF_OK;
 }
 
-int mf_encode_dev(int n, int ncols, int nnz, const int *rp, const int *ci, const double *val,
-                  const mf_options *opt, mf_tiles **out) {
+}  // extern "C"
+
+namespace mf {
+// Encodes a device CSR; G > 0 forces the number of CTA ranges of the layout
+// (1 for the batched solver, whose CTAs each own a whole system).
+int encode_dev_impl(int n, int ncols, int nnz, const int *rp, const int *ci, const double *val,
+                    const mf_options *opt, int G_force, mf_tiles **out) {
     if (!out || n <= 0 || ncols <= 0 || nnz < 0 || !rp || (nnz > 0 && (!ci || !val))) return MF_ERR_ARG;
     auto *t = new mf_tiles;
     if (opt) t->opt = *opt;
@@ -89,6 +94,7 @@ int mf_encode_dev(int n, int ncols, int nnz, const int *rp, const int *ci, const
     MF_CUDA_TRY(cudaGetDeviceProperties(&prop, t->device));
     t->nsm = prop.multiProcessorCount;
     if ((rc = kernel_config(t, &t->G)) != MF_OK) { delete t; return rc; }
+    if (G_force > 0) t->G = G_force;
     cudaStream_t s = 0;
     if ((rc = encode_device(t, n, ncols, nnz, rp, ci, val, s)) != MF_OK) { delete t; return rc; }
     if ((rc = fetch_host_tiles(t)) != MF_OK) { delete t; return rc; }
@@ -99,6 +105,14 @@ int mf_encode_dev(int n, int ncols, int nnz, const int *rp, const int *ci, const
     }
     *out = t;
     return MF_OK;
+}
+}  // namespace mf
+
+extern "C" {
+
+int mf_encode_dev(int n, int ncols, int nnz, const int *rp, const int *ci, const double *val,
+                  const mf_options *opt, mf_tiles **out) {
+    return mf::encode_dev_impl(n, ncols, nnz, rp, ci, val, opt, 0, out);
 }
 
 int mf_encode(const mf_csr *A, const mf_options *opt, mf_tiles **out) {
@@ -210,6 +224,8 @@ int mf_tiles_set_precisions(mf_tiles *t, const unsigned char *prec) {
     int rc = build_layout(t, t->Lmix[0], p, 0);
     if (rc) return rc;
     for (int l = 1; l < MF_NLEVELS; ++l) t->Lmix[l].built = false;
+    t->nlevels = 1;
+    t->level_switch[0] = 0.0;
     t->mixed_ready = true;
     return MF_OK;
 }
@@ -382,11 +398,18 @@ static int solve_dev(mf_tiles *t, int kind, const double *b_dev, double *x_dev, 
     P.replace_every = opt.replace_every;
     P.res = v.res;
     P.inject_wait = opt.reserved[0] == 0x5741 ? 1 : 0;
+    if (opt.reserved[1] > 0) {
+        const int ti = opt.reserved[1] > 4096 ? 4096 : opt.reserved[1];
+        if (t->trace.n < (size_t)ti * 8 && t->trace.alloc((size_t)ti * 8)) return MF_ERR_NOMEM;
+        MF_CUDA_TRY(cudaMemsetAsync(t->trace.p, 0, sizeof(uint64_t) * ti * 8));
+        P.trace = t->trace.p;
+        P.trace_iters = ti;
+        t->trace_iters = ti;
+    }
     const bool mixed = kind == 0 && opt.precision_mode != MF_MODE_FP64 && t->mixed_ready;
     if (mixed) {
         int nl = 1;
-        static const double level_rel[MF_NLEVELS] = {1e-4, 1e-7, 0.0};
-        for (int l = 0; l < MF_NLEVELS; ++l) {
+        for (int l = 0; l < t->nlevels; ++l) {
             if (!t->Lmix[l].built) break;
             LayoutArgs &a = P.lay[nl];
             a.slabs = t->Lmix[l].slabs.p;
@@ -394,11 +417,13 @@ static int solve_dev(mf_tiles *t, int kind, const double *b_dev, double *x_dev, 
             a.cta_slab = t->Lmix[l].cta_slab.p;
             a.cta_rb = t->Lmix[l].cta_rb.p;
             a.cta_dep = t->Lmix[l].cta_dep.p;
-            P.level_rel[nl] = level_rel[l];
+            a.kind = t->Lmix[l].kind;
+            P.level_rel[nl] = t->level_switch[l];
             ++nl;
         }
         P.nlay = nl;
         P.start_layout = 1;
+        P.true_check = 1;
         if (P.replace_every <= 0) P.replace_every = 50;
     } else {
         P.replace_every = 0;  // the FP64 recurrence of the reference never replaces
@@ -407,7 +432,10 @@ static int solve_dev(mf_tiles *t, int kind, const double *b_dev, double *x_dev, 
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, 0);
-    rc = launch_solver(t, kind, P, 0);
+    // mixed layouts run the single-reduction CG unless the classic
+    // recurrence is asked for (mf_options.reserved[2] == 1)
+    const int launch_kind = (mixed && opt.reserved[2] != 1) ? 2 : kind;
+    rc = launch_solver(t, launch_kind, P, 0);
     cudaEventRecord(e1, 0);
     cudaError_t ce = cudaEventSynchronize(e1);
     float ms = 0;
@@ -439,6 +467,19 @@ static int solve_dev(mf_tiles *t, int kind, const double *b_dev, double *x_dev, 
     if (mixed && dr.final_layout >= 1 && t->Lmix[dr.final_layout - 1].built) Lf = &t->Lmix[dr.final_layout - 1];
     R.spmv_bytes = Lf->alg_bytes;
     for (int p = 0; p < 4; ++p) R.tile_frac[p] = Lf->tile_frac[p];
+    R.iters_fp64 = dr.it_layout[0];
+    R.fell_back_fp64 = kind == 0 ? dr.pad : 0;
+    for (int l = 0; l < 3; ++l) {
+        R.iters_level[l] = dr.it_layout[l + 1];
+        R.spmv_bytes_level[l] = (mixed && t->Lmix[l].built) ? t->Lmix[l].alg_bytes : 0.0;
+    }
+    {
+        const double vec = 56.0 * (double)n;
+        double tb = (double)(1 + dr.replacements) * (t->L64.alg_bytes + 16.0 * n);  // initial + replacements
+        tb += (double)dr.it_layout[0] * (t->L64.alg_bytes + vec);
+        for (int l = 0; l < 3; ++l) tb += (double)dr.it_layout[l + 1] * (R.spmv_bytes_level[l] + vec);
+        R.total_bytes = tb;
+    }
     R.rel_residual_true = NAN;
     if (!err[0] && opt.check_true_residual) {
         double rel = 0;
@@ -479,6 +520,14 @@ int mf_solve_cg(mf_tiles *t, const double *b, double *x, double tol, int maxiter
 int mf_solve_bicgstab(mf_tiles *t, const double *b, double *x, double tol, int maxiter, const mf_options *opt,
                       mf_result *res) {
     return solve_host(t, 1, b, x, tol, maxiter, opt, res);
+}
+
+int mf_trace(const mf_tiles *t, unsigned long long *out, int max_iters) {
+    if (!t || !out || max_iters <= 0) return MF_ERR_ARG;
+    const int n = std::min(max_iters, t->trace_iters);
+    if (n <= 0) return 0;
+    MF_CUDA_TRY(cudaMemcpy(out, t->trace.p, sizeof(uint64_t) * 8 * n, cudaMemcpyDeviceToHost));
+    return n;
 }
 
 int mf_true_residual(mf_tiles *t, const double *b, const double *x, double *rel) {

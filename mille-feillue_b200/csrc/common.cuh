@@ -60,6 +60,10 @@ MF_DEV void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar, 
         "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
         : "memory");
 }
+// Bulk prefetch of a global range into L2 (no shared memory, no barrier).
+MF_DEV void bulk_prefetch_l2(const void *src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
 MF_DEV void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
 MF_DEV void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
@@ -102,6 +106,22 @@ MF_DEV double2 ld2_hint(const double *p, uint64_t pol) {
 MF_DEV void st2_hint(double *p, double2 v, uint64_t pol) {
     asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(p), "d"(v.x), "d"(v.y), "l"(pol)
                  : "memory");
+}
+
+MF_DEV float2 ldf2_hint(const float *p, uint64_t pol) {
+    float2 v;
+    asm volatile("ld.global.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
+                 : "=f"(v.x), "=f"(v.y)
+                 : "l"(p), "l"(pol)
+                 : "memory");
+    return v;
+}
+MF_DEV void stf2_hint(float *p, float2 v, uint64_t pol) {
+    asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(p), "f"(v.x), "f"(v.y), "l"(pol)
+                 : "memory");
+}
+MF_DEV void stf_hint(float *p, float v, uint64_t pol) {
+    asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(pol) : "memory");
 }
 
 // Exact FP64 multiply-add without contraction (matches a CPU that rounds the

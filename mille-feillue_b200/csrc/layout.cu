@@ -101,6 +101,7 @@ __device__ void plane_format(int prec, float scale, int &pprec, float &pscale) {
     const bool any32 = __any_sync(full, has && prec == MF_PREC_FP32);
     const bool any16 = __any_sync(full, has && prec == MF_PREC_FP16);
     const bool anyl = __any_sync(full, has);
+    // the plane scale is stored as an int8 exponent of a normal float
     pscale = 1.0f;
     if (!anyl || any64) {
         pprec = MF_PREC_FP64;
@@ -113,7 +114,9 @@ __device__ void plane_format(int prec, float scale, int &pprec, float &pscale) {
     const int e = has ? scale_exp(scale) + 1024 : 1 << 20;
     const int emin = (int)__reduce_min_sync(full, (unsigned)e);
     const int emax = (int)__reduce_max_sync(full, has ? (unsigned)e : 0u);
-    if (emin == emax) {
+    if (emin - 1024 < -126 || emax - 1024 > 127) {
+        pprec = MF_PREC_FP32;
+    } else if (emin == emax) {
         pprec = any16 ? MF_PREC_FP16 : MF_PREC_FP8;
         pscale = ldexpf(1.0f, emin - 1024);
     } else if (!any16 && emax - emin <= 7) {
@@ -237,8 +240,13 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_slabs(const SlabPlan *__r
             h.next_bytes = Q.bytes;
             h.next_xbytes = Q.mode == SLAB_STAGED ? (uint32_t)Q.nseg * 128u : 0u;
             h.next_nruns = Q.mode == SLAB_STAGED ? (uint16_t)Q.nruns : 0;
-            XRun *dst = reinterpret_cast<XRun *>(base + 32);
+            XRun *dst = reinterpret_cast<XRun *>(base + SLAB_HDR);
             for (int k = 0; k < h.next_nruns; ++k) dst[k] = runs[Q.run_off + k];
+        }
+        const int pf = s + 2 * STAGES;
+        if (pf < cta_slab[g + 1]) {
+            h.pf_off16 = plans[pf].off16;
+            h.pf_bytes = plans[pf].bytes;
         }
         *reinterpret_cast<SlabHeader *>(base) = h;
         uint32_t off = slab_blocks_off(P.mode == SLAB_OVERSIZE ? 0 : P.nrb);
@@ -274,7 +282,8 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_slabs(const SlabPlan *__r
             }
         }
         if (lane < 16) blk[lane] = (uint8_t)len;
-        PlaneDesc *pd = reinterpret_cast<PlaneDesc *>(blk + rb_pdesc_off());
+        uint64_t pbits = 0;
+        int8_t *sexp = reinterpret_cast<int8_t *>(blk + rb_pinfo_off() + 8);
         uint8_t *idxb = blk + rb_idx_off(W, mixed);
         uint8_t *vals = blk + rb_vals_off(W, mixed, gather);
         uint32_t voff = 0;
@@ -284,13 +293,9 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_slabs(const SlabPlan *__r
             int pp = MF_PREC_FP64;
             float ps = 1.0f;
             if (mixed) plane_format(has ? (int)A.prec[c.t] : -1, has ? A.scale[c.t] : 1.0f, pp, ps);
-            if (mixed && lane == 0) {
-                PlaneDesc d;
-                d.voff = (uint16_t)voff;
-                d.prec = (uint8_t)pp;
-                d.pad = 0;
-                d.scale = ps;
-                pd[k] = d;
+            if (mixed) {
+                pbits |= (uint64_t)pp << (2 * k);
+                if (lane == 0) sexp[k] = (int8_t)(pp >= MF_PREC_FP16 ? scale_exp(ps) : 0);
             }
             if (has) {
                 const int t = c.t;
@@ -331,6 +336,7 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_slabs(const SlabPlan *__r
             }
             voff += 16u * prec_width(pp);
         }
+        if (mixed && lane == 0) *reinterpret_cast<uint64_t *>(blk + rb_pinfo_off()) = pbits;
     }
 }
 
@@ -375,6 +381,7 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
     MF_CUDA_TRY(cudaStreamSynchronize(st));
 
     auto rb_bytes = [&](int rb, bool gather) { return rb_block_bytes(rbW[rb], mixed, gather, rbvb[rb]); };
+    const int maxw = mixed ? MAXW_MIXED : MAXW;
     // CTA ranges of equal cost, computed once per matrix and shared by every
     // layout so that all layouts give each CTA the same rows
     if ((int)t->h_cta_rb.size() != G + 1) {
@@ -415,7 +422,7 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
             rbsegs.assign(tc.begin() + tp[rb], tc.begin() + tp[rb + 1]);  // ascending already
             const bool staged0 = (int)rbsegs.size() <= XSEG_MAX && count_runs(rbsegs) <= MAXRUNS;
             const uint32_t tot0 = slab_blocks_off(1) + rb_bytes(rb, !staged0);
-            if (tot0 > (uint32_t)slab_max || rbW[rb] > MAXW) {
+            if (tot0 > (uint32_t)slab_max || rbW[rb] > maxw) {
                 P.mode = SLAB_OVERSIZE;
                 P.nrb = 1;
                 P.ntiles = tp[rb + 1] - tp[rb];
@@ -432,7 +439,7 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
                 uint32_t body = rb_bytes(rb, !staged);
                 int nx = rb + 1;
                 while (nx < cta_rb[g + 1] && P.nrb < rbps) {
-                    if (rbW[nx] > MAXW) break;
+                    if (rbW[nx] > maxw) break;
                     const uint32_t bx = rb_bytes(nx, !staged);
                     if (slab_blocks_off(P.nrb + 1) + body + bx > (uint32_t)slab_max) break;
                     if (staged) {
@@ -518,6 +525,16 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
         dep[2 * g] = owner(cmin);
         dep[2 * g + 1] = owner(cmax);
     }
+    // layout kind (oversize row blocks run in FP64 from the tile arrays and
+    // do not count)
+    int kind = LAYOUT_FP64;
+    if (mixed) {
+        bool any64 = false;
+        for (const auto &P : plans)
+            if (P.mode != SLAB_OVERSIZE)
+                for (int k = tp[P.rb0]; k < tp[P.rb0 + P.nrb] && !any64; ++k) any64 = prec[k] == MF_PREC_FP64;
+        kind = any64 ? LAYOUT_ANY : LAYOUT_LOW;
+    }
     // algorithmic bytes and precision fractions
     double alg = 16.0 * (double)t->rowA;
     double cnt[4] = {0, 0, 0, 0};
@@ -558,6 +575,7 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
     L.slab_max = slab_max;
     L.rb_per_slab = rbps;
     L.mixed = mixed;
+    L.kind = kind;
     L.bytes = off;
     L.alg_bytes = alg;
     for (int p = 0; p < 4; ++p) L.tile_frac[p] = tilenum > 0 ? cnt[p] / tilenum : 0.0;

@@ -49,9 +49,10 @@ struct __align__(16) Smem {
 
 __device__ __forceinline__ uint8_t *stage_ptr(uint8_t *dyn, int k, int stride) { return dyn + (size_t)k * stride; }
 
-__device__ void set_error(const KParams &P, uint32_t code, uint32_t site) {
-    if (atomicCAS(P.sync + SYNC_ERROR, 0u, code) == 0u) atomicExch(P.sync + SYNC_SITE, site);
+__device__ void set_error_w(uint32_t *sync, uint32_t code, uint32_t site) {
+    if (atomicCAS(sync + SYNC_ERROR, 0u, code) == 0u) atomicExch(sync + SYNC_SITE, site);
 }
+__device__ void set_error(const KParams &P, uint32_t code, uint32_t site) { set_error_w(P.sync, code, site); }
 
 // Thread 0: issue the bulk copies of one slab (x runs first, slab last: the
 // issue record may live inside the stage the slab overwrites).
@@ -87,7 +88,7 @@ __device__ bool wait_bar(uint64_t *bar, uint32_t parity, uint64_t limit_ns) {
 // FP64 tiles: sum = 0, sum += x*v in order, acc += sum at each tile start,
 // exactly blockspmv_cpu's order. Tiles below FP64 (mixed layouts): the
 // dequantized value in FP32, sumf = fmaf(x, v, sumf), acc += sumf.
-template <bool MIXED>
+template <int KIND>
 __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &h, int j, int r, const double *xstage,
                                            const double *__restrict__ xg) {
     const RbDir d = reinterpret_cast<const RbDir *>(st + slab_rbdir_off())[j];
@@ -96,7 +97,7 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
     const int len = blk[r];
     const bool gather = h.mode == SLAB_GATHER;
     double acc = 0.0, sum = 0.0;
-    if (!MIXED) {
+    if (KIND == LAYOUT_FP64) {
         const double *vals = reinterpret_cast<const double *>(blk + rb_vals_off(W, false, gather));
         if (!gather) {
             const uint16_t *idx = reinterpret_cast<const uint16_t *>(blk + rb_idx_off(W, false));
@@ -127,13 +128,102 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
         }
         return dadd(acc, sum);
     }
-    const PlaneDesc *pd = reinterpret_cast<const PlaneDesc *>(blk + rb_pdesc_off());
+    // mixed layouts: packed plane precisions, value offset kept in a register
+    const uint64_t pbits = *reinterpret_cast<const uint64_t *>(blk + rb_pinfo_off());
+    const int8_t *sexp = reinterpret_cast<const int8_t *>(blk + rb_pinfo_off() + 8);
     const uint8_t *idxb = blk + rb_idx_off(W, true);
     const uint8_t *vals = blk + rb_vals_off(W, true, gather);
+    uint32_t voff = 0;
     float sumf = 0.0f;
+    if (KIND == LAYOUT_LOW && W > 0 && W <= 32 && pbits == (0x5555555555555555ull & ((2ull << (2 * W - 1)) - 1ull))) {
+        // every plane of the row block stored in FP32
+        const float *v32 = reinterpret_cast<const float *>(vals);
+        if (!gather) {
+            const uint16_t *idx = reinterpret_cast<const uint16_t *>(idxb);
+#pragma unroll 4
+            for (int k = 0; k < len; ++k) {
+                const uint32_t id = idx[k * 16 + r];
+                const float v = v32[k * 16 + r];
+                const double x = xstage[id & IDX16_POS];
+                if (id & IDX16_START) {
+                    acc = dadd(acc, (double)sumf);
+                    sumf = 0.0f;
+                }
+                sumf = __fmaf_rn(__double2float_rn(x), v, sumf);
+            }
+        } else {
+            const uint32_t *idx = reinterpret_cast<const uint32_t *>(idxb);
+#pragma unroll 4
+            for (int k = 0; k < len; ++k) {
+                const uint32_t id = idx[k * 16 + r];
+                const float v = v32[k * 16 + r];
+                const double x = __ldcg(xg + (id & IDX32_POS));
+                if (id & IDX32_START) {
+                    acc = dadd(acc, (double)sumf);
+                    sumf = 0.0f;
+                }
+                sumf = __fmaf_rn(__double2float_rn(x), v, sumf);
+            }
+        }
+        return dadd(acc, (double)sumf);
+    }
+    if (KIND == LAYOUT_LOW) {
+        // every tile below FP64: FP32 products, FP32 tile sums, FP64 row sum.
+        // Branch-free: each lane loads the 32-bit word holding its value
+        // (plane width 4, 2 or 1 bytes) and decodes all three forms.
+        if (!gather) {
+            const uint16_t *idx = reinterpret_cast<const uint16_t *>(idxb);
+#pragma unroll 4
+            for (int k = 0; k < len; ++k) {
+                const uint32_t pr = (uint32_t)(pbits >> (2 * k)) & 3u;
+                const uint32_t wlog = 3u - pr;
+                const uint32_t id = idx[k * 16 + r];
+                const double x = xstage[id & IDX16_POS];
+                const uint32_t boff = voff + ((uint32_t)r << wlog);
+                const uint32_t wrd = *reinterpret_cast<const uint32_t *>(vals + (boff & ~3u));
+                const uint32_t sh = (boff & 3u) * 8u;
+                const float sc = __int_as_float((sexp[k] + 127) << 23);
+                const float v16 = __half2float(__ushort_as_half((unsigned short)(wrd >> sh)));
+                const float v8 = __half2float(
+                    __half(__nv_cvt_fp8_to_halfraw((__nv_fp8_storage_t)((wrd >> sh) & 0xffu), __NV_E4M3)));
+                const float v = (pr == MF_PREC_FP32 ? __uint_as_float(wrd) : pr == MF_PREC_FP16 ? v16 : v8) * sc;
+                if (id & IDX16_START) {
+                    acc = dadd(acc, (double)sumf);
+                    sumf = 0.0f;
+                }
+                sumf = __fmaf_rn(__double2float_rn(x), v, sumf);
+                voff += 16u << wlog;
+            }
+        } else {
+            const uint32_t *idx = reinterpret_cast<const uint32_t *>(idxb);
+#pragma unroll 4
+            for (int k = 0; k < len; ++k) {
+                const uint32_t pr = (uint32_t)(pbits >> (2 * k)) & 3u;
+                const uint32_t wlog = 3u - pr;
+                const uint32_t id = idx[k * 16 + r];
+                const double x = __ldcg(xg + (id & IDX32_POS));
+                const uint32_t boff = voff + ((uint32_t)r << wlog);
+                const uint32_t wrd = *reinterpret_cast<const uint32_t *>(vals + (boff & ~3u));
+                const uint32_t sh = (boff & 3u) * 8u;
+                const float sc = __int_as_float((sexp[k] + 127) << 23);
+                const float v16 = __half2float(__ushort_as_half((unsigned short)(wrd >> sh)));
+                const float v8 = __half2float(
+                    __half(__nv_cvt_fp8_to_halfraw((__nv_fp8_storage_t)((wrd >> sh) & 0xffu), __NV_E4M3)));
+                const float v = (pr == MF_PREC_FP32 ? __uint_as_float(wrd) : pr == MF_PREC_FP16 ? v16 : v8) * sc;
+                if (id & IDX32_START) {
+                    acc = dadd(acc, (double)sumf);
+                    sumf = 0.0f;
+                }
+                sumf = __fmaf_rn(__double2float_rn(x), v, sumf);
+                voff += 16u << wlog;
+            }
+        }
+        return dadd(acc, (double)sumf);
+    }
+    // some tiles FP64, some below: each tile sums in its own type
     bool low = false;
     for (int k = 0; k < len; ++k) {
-        const PlaneDesc p = pd[k];
+        const uint32_t pr = (uint32_t)(pbits >> (2 * k)) & 3u;
         double x;
         bool start, lowk;
         if (!gather) {
@@ -153,23 +243,43 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
             sumf = 0.0f;
             low = lowk;
         }
-        const uint8_t *pv = vals + p.voff;
+        const uint8_t *pv = vals + voff;
         if (low) {
             float vf;
-            if (p.prec == MF_PREC_FP64) vf = __double2float_rn(reinterpret_cast<const double *>(pv)[r]);
-            else if (p.prec == MF_PREC_FP32) vf = reinterpret_cast<const float *>(pv)[r];
-            else if (p.prec == MF_PREC_FP16) vf = __half2float(reinterpret_cast<const __half *>(pv)[r]) * p.scale;
-            else vf = __half2float(__half(__nv_cvt_fp8_to_halfraw((__nv_fp8_storage_t)pv[r], __NV_E4M3))) * p.scale;
+            if (pr == MF_PREC_FP64) vf = __double2float_rn(reinterpret_cast<const double *>(pv)[r]);
+            else if (pr == MF_PREC_FP32) vf = reinterpret_cast<const float *>(pv)[r];
+            else {
+                const float sc = __int_as_float((sexp[k] + 127) << 23);
+                if (pr == MF_PREC_FP16) vf = __half2float(reinterpret_cast<const __half *>(pv)[r]) * sc;
+                else vf = __half2float(__half(__nv_cvt_fp8_to_halfraw((__nv_fp8_storage_t)pv[r], __NV_E4M3))) * sc;
+            }
             sumf = __fmaf_rn(__double2float_rn(x), vf, sumf);
         } else {
             sum = dadd(sum, dmul(x, reinterpret_cast<const double *>(pv)[r]));
         }
+        voff += 16u << (3u - pr);
     }
     return dadd(acc, low ? (double)sumf : sum);
 }
 
+// Global tile arrays (the oversize path) and the source of one SpMV.
+struct SpmvSrc {
+    const uint8_t *slabs;
+    const uint8_t *head;  // STAGES issue records (shared memory)
+    int ns, kind, site;
+    GTiles gt;
+};
+struct PipeCfg {
+    int stage_stride, slab_area;
+    uint64_t limit_ns;
+    uint32_t *sync;
+};
+__device__ __forceinline__ GTiles gtiles_of(const KParams &P) {
+    return GTiles{P.tile_ptr, P.tile_col, P.tile_off, P.csrptr_off, P.ptr, P.val, P.col, P.tilem, P.rowA};
+}
+
 // Row sum of an oversize row block straight from the global tile arrays.
-__device__ double global_row(const KParams &P, int rb, int r, const double *__restrict__ xg) {
+__device__ double global_row(const GTiles &P, int rb, int r, const double *__restrict__ xg) {
     const int rl = rb == P.tilem - 1 ? P.rowA - (P.tilem - 1) * 16 : 16;
     if (r >= rl) return 0.0;
     double acc = 0.0;
@@ -197,11 +307,11 @@ __device__ double global_row(const KParams &P, int rb, int r, const double *__re
 // entries, then epi(row, acc, v) runs with the row sum. Returns false on
 // abort.
 template <bool MIXED, class Epi>
-__device__ bool cta_spmv(const KParams &P, int lay, const double *xv, Smem &S, uint8_t *dyn, Pipe &pp, Epi &epi) {
-    const int ns = S.slab1[lay] - S.slab0[lay];
-    const int stride = P.stage_stride;
-    const int slab_area = P.slab_area;
-    const LayoutArgs &L = P.lay[lay];
+__device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const double *xv, Smem &S, uint8_t *dyn,
+                             Pipe &pp, Epi &epi) {
+    const int ns = L.ns;
+    const int stride = C.stage_stride;
+    const int slab_area = C.slab_area;
     const int tid = threadIdx.x;
     const int w = tid >> 5, lane = tid & 31;
     const int half = lane >> 4, r = lane & 15;
@@ -213,8 +323,8 @@ __device__ bool cta_spmv(const KParams &P, int lay, const double *xv, Smem &S, u
                 const int k = i % STAGES;
                 uint8_t *st = stage_ptr(dyn, k, stride);
                 if ((pp.filled >> k) & 1u) {
-                    if (!wait_bar(&S.empty[k], (pp.eph >> k) & 1u, P.limit_ns)) {
-                        set_error(P, (uint32_t)MF_ERR_TIMEOUT, 110 + lay);
+                    if (!wait_bar(&S.empty[k], (pp.eph >> k) & 1u, C.limit_ns)) {
+                        set_error_w(C.sync, (uint32_t)MF_ERR_TIMEOUT, 110 + L.site);
                         S.abort = 1;
                         break;
                     }
@@ -225,7 +335,7 @@ __device__ bool cta_spmv(const KParams &P, int lay, const double *xv, Smem &S, u
                 int nruns;
                 const XRun *runs;
                 if (i < STAGES) {
-                    const uint32_t *rec = reinterpret_cast<const uint32_t *>(S.head[lay][i]);
+                    const uint32_t *rec = reinterpret_cast<const uint32_t *>(L.head + i * ISSUE_REC);
                     off16 = rec[0];
                     bytes = rec[1];
                     xbytes = rec[2];
@@ -238,7 +348,8 @@ __device__ bool cta_spmv(const KParams &P, int lay, const double *xv, Smem &S, u
                     bytes = h->next_bytes;
                     xbytes = h->next_xbytes;
                     nruns = h->next_nruns;
-                    runs = reinterpret_cast<const XRun *>(st + 32);
+                    runs = reinterpret_cast<const XRun *>(st + SLAB_HDR);
+                    if (h->pf_bytes) bulk_prefetch_l2(L.slabs + (size_t)h->pf_off16 * 16, h->pf_bytes);
                 }
                 fence_proxy_async_smem();
                 issue_slab(S, st, slab_area, k, off16, bytes, xbytes, nruns, runs, L.slabs, xv, pm, pv);
@@ -249,8 +360,8 @@ __device__ bool cta_spmv(const KParams &P, int lay, const double *xv, Smem &S, u
         for (int i = 0; i < ns; ++i) {
             const int k = i % STAGES;
             uint8_t *st = stage_ptr(dyn, k, stride);
-            if (!wait_bar(&S.full[k], (pp.fph >> k) & 1u, P.limit_ns)) {
-                set_error(P, (uint32_t)MF_ERR_TIMEOUT, 100 + lay);
+            if (!wait_bar(&S.full[k], (pp.fph >> k) & 1u, C.limit_ns)) {
+                set_error_w(C.sync, (uint32_t)MF_ERR_TIMEOUT, 100 + L.site);
                 S.abort = 1;
                 break;
             }
@@ -259,17 +370,20 @@ __device__ bool cta_spmv(const KParams &P, int lay, const double *xv, Smem &S, u
             if (h.mode == SLAB_OVERSIZE) {
                 if (w == 0 && half == 0) {
                     const int row = h.rb0 * 16 + r;
-                    const double pv = row < P.rowA ? epi.pre(row) : 0.0;
-                    const double acc = global_row(P, h.rb0, r, xv);
-                    if (row < P.rowA) epi(row, acc, pv);
+                    const double pv = row < L.gt.rowA ? epi.pre(row) : 0.0;
+                    const double acc = global_row(L.gt, h.rb0, r, xv);
+                    if (row < L.gt.rowA) epi(row, acc, pv);
                 }
             } else {
                 for (int j = 2 * w + half; j < h.nrb; j += 2 * NWARPS) {
                     const int row = (h.rb0 + j) * 16 + r;
-                    const bool live = row < P.rowA;
+                    const bool live = row < L.gt.rowA;
                     const double pv = live ? epi.pre(row) : 0.0;
-                    const double acc =
-                        slab_row<MIXED>(st, h, j, r, reinterpret_cast<const double *>(st + slab_area), xv);
+                    const double *xsg = reinterpret_cast<const double *>(st + slab_area);
+                    double acc;
+                    if (!MIXED || L.kind == LAYOUT_FP64) acc = slab_row<LAYOUT_FP64>(st, h, j, r, xsg, xv);
+                    else if (L.kind == LAYOUT_LOW) acc = slab_row<LAYOUT_LOW>(st, h, j, r, xsg, xv);
+                    else acc = slab_row<LAYOUT_ANY>(st, h, j, r, xsg, xv);
                     if (live) epi(row, acc, pv);
                 }
             }
@@ -279,6 +393,21 @@ __device__ bool cta_spmv(const KParams &P, int lay, const double *xv, Smem &S, u
     }
     __syncthreads();
     return S.abort == 0;
+}
+
+
+// Grid-kernel form: layout `lay` of the kernel parameters, this CTA's slabs.
+template <bool MIXED, class Epi>
+__device__ bool cta_spmv(const KParams &P, int lay, const double *xv, Smem &S, uint8_t *dyn, Pipe &pp, Epi &epi) {
+    SpmvSrc L;
+    L.slabs = P.lay[lay].slabs;
+    L.head = &S.head[lay][0][0];
+    L.ns = S.slab1[lay] - S.slab0[lay];
+    L.kind = P.lay[lay].kind;
+    L.site = lay;
+    L.gt = gtiles_of(P);
+    const PipeCfg C{P.stage_stride, P.slab_area, P.limit_ns, P.sync};
+    return cta_spmv_src<MIXED>(L, C, xv, S, dyn, pp, epi);
 }
 
 // Block reduction of NV partials in a fixed order, then the grid-wide sum.
@@ -468,6 +597,13 @@ struct EpiQ {  // q = A d, dq += d*q
     }
 };
 
+// Phase trace: CTA 0 thread 0 writes %globaltimer at slot s of iteration it.
+#define MF_TRACE(it, s)                                                                   \
+    do {                                                                                  \
+        if (P.trace && blockIdx.x == 0 && threadIdx.x == 0 && (it) < P.trace_iters)       \
+            P.trace[(size_t)(it) * 8 + (s)] = globaltimer();                              \
+    } while (0)
+
 template <bool MIXED>
 __global__ void __launch_bounds__(NTHREADS, 1) k_cg(KParams P) {
     extern __shared__ __align__(128) uint8_t dyn[];
@@ -518,9 +654,16 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cg(KParams P) {
     double rel = bnorm > 0 ? sqrt(rr) / bnorm : 0.0;
     const bool fixed = P.fixed_iterations > 0;
     const int maxit = fixed ? P.fixed_iterations : P.maxiter;
-    while (it < maxit && (fixed || rel > tol)) {
-        // periodic true-residual replacement r = b - A x (FP64 layout)
-        if (P.replace_every > 0 && it > 0 && it % P.replace_every == 0) {
+    // With true_check, a recursive residual under tol is confirmed with the
+    // FP64 true residual b - A x before the solve stops (mixed layouts).
+    bool pending = false;
+    int it_lay[KMAX_LAYOUTS] = {0, 0, 0, 0};
+    double rr_best = rr;
+    int fellback = 0;
+    while (it < maxit && (fixed || rel > tol || pending)) {
+        // true-residual replacement r = b - A x (FP64 layout): periodic, or
+        // to confirm convergence
+        if (pending || (P.replace_every > 0 && it > 0 && it % P.replace_every == 0)) {
             if (!wait_deps(P, S, lay64, ep)) return;
             EpiResidual e2{b, r, 0.0, vpol};
             if (!cta_spmv<false>(P, lay64, x, S, dyn, pp, e2)) return;
@@ -528,23 +671,42 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cg(KParams P) {
             if (!grid_sum<1>(P, S, v1, o1, phase)) return;
             rr = o1[0];
             ++repl;
+            if (pending) {
+                pending = false;
+                rel = bnorm > 0 ? sqrt(rr) / bnorm : 0.0;
+                if (rel <= tol) break;
+            }
+            // a low-precision operator that lets the true residual grow
+            // 100x above the best seen falls back to the FP64 layout
+            if (MIXED && lay != lay64) {
+                if (rr < rr_best) rr_best = rr;
+                if (!(rr <= 1e4 * rr_best)) {
+                    lay = lay64;
+                    fellback = 1;
+                }
+            }
             // tighten the precision level as the true residual falls
             if (MIXED) {
                 const double relt = bnorm > 0 ? sqrt(rr) / bnorm : 0.0;
-                while (lay < P.nlay - 1 && relt < P.level_rel[lay]) {
+                while (lay != lay64 && lay < P.nlay - 1 && relt < P.level_rel[lay]) {
                     ++lay;
                     ++switches;
                 }
             }
         }
+        MF_TRACE(it, 0);
         if (!wait_deps(P, S, lay, ep)) return;
+        MF_TRACE(it, 1);
+        ++it_lay[lay];
         EpiQ eq{d, q, 0.0, vpol};
         bool ok;
         if (MIXED && lay != lay64) ok = cta_spmv<true>(P, lay, d, S, dyn, pp, eq);
         else ok = cta_spmv<false>(P, lay64, d, S, dyn, pp, eq);
         if (!ok) return;
+        MF_TRACE(it, 2);
         double v1[1] = {eq.dq}, o1[1];
         if (!grid_sum<1>(P, S, v1, o1, phase)) return;
+        MF_TRACE(it, 3);
         const double dq = o1[0];
         if (!(dq != 0.0) || !isfinite(dq)) {
             status = MF_ERR_BREAKDOWN;
@@ -568,13 +730,16 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cg(KParams P) {
                 rrp += o.x * o.x + o.y * o.y;
             }
         })
+        MF_TRACE(it, 4);
         double w1[1] = {rrp}, u1[1];
         if (!grid_sum<1>(P, S, w1, u1, phase)) return;
+        MF_TRACE(it, 5);
         const double rrn = u1[0];
         ++it;
         rel = bnorm > 0 ? sqrt(rrn) / bnorm : 0.0;
         const double beta = rrn / rr;
-        const bool done = !fixed && rel <= tol;
+        const bool done = !fixed && rel <= tol && !P.true_check;
+        if (!fixed && rel <= tol && P.true_check) pending = true;
         MF_PAIRS(4, vlo, vhi, {
             double2 dv[_vb], xv[_vb], rv[_vb];
 #pragma unroll
@@ -599,6 +764,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cg(KParams P) {
         rr = rrn;
         ++ep;
         publish(P, ep);
+        MF_TRACE(it - 1, 6);
         if (!isfinite(rrn)) {
             status = MF_ERR_BREAKDOWN;
             break;
@@ -613,8 +779,186 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cg(KParams P) {
         P.res->rr = rr;
         P.res->bb = bb;
         P.res->final_layout = lay;
+        for (int l = 0; l < KMAX_LAYOUTS; ++l) P.res->it_layout[l] = it_lay[l];
+        P.res->pad = fellback;
     }
     (void)G;
+}
+
+// ------------------------------------------------- CG, single reduction
+// Chronopoulos-Gear form of CG for the mixed-precision layouts: one grid
+// reduction and one fused vector pass per iteration. w = A r comes from the
+// low-precision SpMV; the directions p and s = A p, and w, are stored in
+// FP32; x and r (and the dots and scalars) stay FP64; r is replaced by the
+// FP64 true residual b - A x every replace_every iterations and before the
+// solve stops.
+//   p = r + beta p;  s = w + beta s;  x += alpha p;  r -= alpha s;
+//   w = A r;  gamma = r.r;  delta = w.r;
+//   beta = gamma / gamma_old;  alpha = gamma / (delta - beta gamma / alpha_old)
+struct EpiW {  // w = A r (FP32), gamma += r*r, delta += w*r
+    const double *r;
+    float *w;
+    double g, dl;
+    uint64_t pol;
+    __device__ double pre(int row) const { return ld_hint(r + row, pol); }
+    __device__ void operator()(int row, double acc, double rv) {
+        const float wf = __double2float_rn(acc);
+        stf_hint(w + row, wf, pol);
+        g += rv * rv;
+        dl += (double)wf * rv;
+    }
+};
+
+__global__ void __launch_bounds__(NTHREADS, 1) k_cgcg(KParams P) {
+    extern __shared__ __align__(128) uint8_t dyn[];
+    __shared__ Smem S;
+    kernel_setup(P, S, P.nlay);
+    const int g = blockIdx.x, tid = threadIdx.x;
+    Pipe pp;
+    uint32_t phase = 0;
+    const uint64_t vpol = policy_evict_last();
+    const int lay64 = 0;
+    int lay = P.start_layout;
+    const int rb_lo = P.lay[0].cta_rb[g], rb_hi = P.lay[0].cta_rb[g + 1];
+    const int vlo = rb_lo * 16, vhi = rb_hi * 16;
+    double *x = P.x, *r = P.r;
+    float *pv32 = reinterpret_cast<float *>(P.d), *sv32 = reinterpret_cast<float *>(P.q),
+          *wv32 = reinterpret_cast<float *>(P.s);
+    const double *b = P.b;
+    // r = b - A x0; p = s = 0
+    EpiResidual er{b, r, 0.0, vpol};
+    if (!cta_spmv<false>(P, lay64, x, S, dyn, pp, er)) return;
+    double bbp = 0.0;
+    MF_PAIRS(4, vlo, vhi, {
+        double2 bv[_vb];
+#pragma unroll
+        MF_FOR_VB if (MF_LIVE(u, vhi)) bv[u] = ld2_hint(b + 2 * MF_PI(u), vpol);
+#pragma unroll
+        MF_FOR_VB if (MF_LIVE(u, vhi)) {
+            bbp += bv[u].x * bv[u].x + bv[u].y * bv[u].y;
+            stf2_hint(pv32 + 2 * MF_PI(u), make_float2(0.f, 0.f), vpol);
+            stf2_hint(sv32 + 2 * MF_PI(u), make_float2(0.f, 0.f), vpol);
+        }
+    })
+    double v1[1] = {bbp}, o1[1];
+    if (!grid_sum<1>(P, S, v1, o1, phase)) return;
+    const double bb = o1[0];
+    const double bnorm = sqrt(bb);
+    const double tol = P.tol;
+    uint32_t ep = 1;
+    publish(P, ep);
+    int it = 0, status = MF_OK, repl = 0, switches = 0, fellback = 0;
+    int it_lay[KMAX_LAYOUTS] = {0, 0, 0, 0};
+    double gamma_old = 0.0, alpha_old = 1.0, rel = 1.0, rr_best = 1e300, gam = 0.0;
+    bool first = true, pending = false;
+    const bool fixed = P.fixed_iterations > 0;
+    const int maxit = fixed ? P.fixed_iterations : P.maxiter;
+    while (true) {
+        const bool repl_now = pending || (P.replace_every > 0 && it > 0 && it % P.replace_every == 0);
+        if (repl_now) {
+            if (!wait_deps(P, S, lay64, ep)) return;
+            EpiResidual e2{b, r, 0.0, vpol};
+            if (!cta_spmv<false>(P, lay64, x, S, dyn, pp, e2)) return;
+            double a1[1] = {e2.rr}, c1[1];
+            if (!grid_sum<1>(P, S, a1, c1, phase)) return;
+            ++repl;
+            ++ep;
+            publish(P, ep);
+            const double relt = bnorm > 0 ? sqrt(c1[0]) / bnorm : 0.0;
+            if (pending) {
+                pending = false;
+                rel = relt;
+                if (rel <= tol) break;
+            }
+            if (lay != lay64) {
+                if (c1[0] < rr_best) rr_best = c1[0];
+                if (!(c1[0] <= 1e4 * rr_best)) {
+                    lay = lay64;
+                    fellback = 1;
+                }
+                while (lay != lay64 && lay < P.nlay - 1 && relt < P.level_rel[lay]) {
+                    ++lay;
+                    ++switches;
+                }
+            }
+        }
+        if (it >= maxit) break;
+        if (!wait_deps(P, S, lay, ep)) return;
+        ++it_lay[lay];
+        EpiW ew{r, wv32, 0.0, 0.0, vpol};
+        bool ok;
+        if (lay != lay64) ok = cta_spmv<true>(P, lay, r, S, dyn, pp, ew);
+        else ok = cta_spmv<false>(P, lay64, r, S, dyn, pp, ew);
+        if (!ok) return;
+        double a2[2] = {ew.g, ew.dl}, c2[2];
+        if (!grid_sum<2>(P, S, a2, c2, phase)) return;
+        gam = c2[0];
+        const double delta = c2[1];
+        rel = bnorm > 0 ? sqrt(gam) / bnorm : 0.0;
+        if (!fixed && rel <= tol) {
+            pending = true;  // confirm with the FP64 true residual
+            continue;
+        }
+        double alpha, beta;
+        if (first) {
+            beta = 0.0;
+            alpha = gam / delta;
+            first = false;
+        } else {
+            beta = gam / gamma_old;
+            alpha = gam / (delta - beta * gam / alpha_old);
+        }
+        if (!isfinite(alpha) || !isfinite(beta) || alpha == 0.0) {
+            status = MF_ERR_BREAKDOWN;
+            break;
+        }
+        MF_PAIRS(2, vlo, vhi, {
+            double2 rv[_vb], xv[_vb];
+            float2 pw[_vb], sw[_vb], ww[_vb];
+#pragma unroll
+            MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+                xv[u] = ld2_hint(x + 2 * MF_PI(u), vpol);
+                pw[u] = ldf2_hint(pv32 + 2 * MF_PI(u), vpol);
+                sw[u] = ldf2_hint(sv32 + 2 * MF_PI(u), vpol);
+                ww[u] = ldf2_hint(wv32 + 2 * MF_PI(u), vpol);
+            }
+#pragma unroll
+            MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                const double px = rv[u].x + beta * (double)pw[u].x, py = rv[u].y + beta * (double)pw[u].y;
+                const double sx = (double)ww[u].x + beta * (double)sw[u].x,
+                             sy = (double)ww[u].y + beta * (double)sw[u].y;
+                const float2 pf = make_float2(__double2float_rn(px), __double2float_rn(py));
+                const float2 sf = make_float2(__double2float_rn(sx), __double2float_rn(sy));
+                stf2_hint(pv32 + 2 * MF_PI(u), pf, vpol);
+                stf2_hint(sv32 + 2 * MF_PI(u), sf, vpol);
+                double2 xo, ro;
+                xo.x = xv[u].x + alpha * (double)pf.x;
+                xo.y = xv[u].y + alpha * (double)pf.y;
+                ro.x = rv[u].x - alpha * (double)sf.x;
+                ro.y = rv[u].y - alpha * (double)sf.y;
+                st2_hint(x + 2 * MF_PI(u), xo, vpol);
+                st2_hint(r + 2 * MF_PI(u), ro, vpol);
+            }
+        })
+        gamma_old = gam;
+        alpha_old = alpha;
+        ++it;
+        ++ep;
+        publish(P, ep);
+    }
+    if (g == 0 && tid == 0) {
+        if (status == MF_OK && !fixed && rel > tol) status = MF_ERR_NOT_CONVERGED;
+        P.res->iterations = it;
+        P.res->status = status;
+        P.res->replacements = repl;
+        P.res->level_switches = switches;
+        P.res->rr = bnorm > 0 ? rel * rel * bb : gam;
+        P.res->bb = bb;
+        P.res->final_layout = lay;
+        for (int l = 0; l < KMAX_LAYOUTS; ++l) P.res->it_layout[l] = it_lay[l];
+        P.res->pad = fellback;
+    }
 }
 
 // -------------------------------------------------------------- BiCGSTAB
@@ -789,6 +1133,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_bicgstab(KParams P) {
         P.res->rr = rr;
         P.res->bb = bb;
         P.res->final_layout = 0;
+        P.res->it_layout[0] = it;
+        for (int l = 1; l < KMAX_LAYOUTS; ++l) P.res->it_layout[l] = 0;
     }
 }
 
@@ -811,6 +1157,172 @@ __global__ void k_residual_norms(int n, const double *b, const double *ax, doubl
     }
 }
 
+// ------------------------------------------------------------ batched CG
+// Deterministic block reduction (fixed order) broadcast to every thread.
+template <int NV>
+__device__ void block_sum(Smem &S, const double (&v)[NV], double (&out)[NV]) {
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    double t[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        t[k] = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t[k] += __shfl_xor_sync(0xffffffffu, t[k], o);
+    }
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) S.red[w][k] = t[k];
+    __syncthreads();
+    if (tid == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double a = 0.0;
+            for (int q = 0; q <= NWARPS; ++q) a += S.red[q][k];
+            S.bres[k] = a;
+        }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) out[k] = S.bres[k];
+    __syncthreads();
+}
+
+// Every CTA takes systems from a queue (largest first) and runs the FP64 CG
+// recurrence of the single-system kernel on it alone: the system's slabs
+// stream through the CTA's ring, the dots are block reductions, and no
+// grid-wide synchronization is needed.
+__global__ void __launch_bounds__(NTHREADS, 1) k_batch_cg(BatchParams B) {
+    extern __shared__ __align__(128) uint8_t dyn[];
+    __shared__ Smem S;
+    __shared__ int s_sys;
+    KParams P0;  // only the fields kernel_setup reads
+    P0.nlay = 0;
+    kernel_setup(P0, S, 0);
+    const int tid = threadIdx.x;
+    Pipe pp;
+    const uint64_t vpol = policy_evict_last();
+    const PipeCfg C{B.stage_stride, B.slab_area, B.limit_ns, B.sync};
+    const bool fixed = B.fixed_iterations > 0;
+    const int maxit = fixed ? B.fixed_iterations : B.maxiter;
+    while (true) {
+        if (tid == 0) {
+            const unsigned qi = atomicAdd(B.queue, 1u);
+            s_sys = (int)qi < B.count ? B.order[qi] : -1;
+        }
+        __syncthreads();
+        const int sys = s_sys;
+        if (sys < 0) break;
+        const SysDesc D = B.sys[sys];
+        for (int i = tid; i < STAGES * ISSUE_REC; i += NTHREADS) (&S.head[0][0][0])[i] = D.head[i];
+        __syncthreads();
+        SpmvSrc L;
+        L.slabs = D.slabs;
+        L.head = &S.head[0][0][0];
+        L.ns = D.ns;
+        L.kind = D.kind;
+        L.site = 40;
+        L.gt = D.gt;
+        double *x = D.x, *r = D.r, *d = D.d, *q = D.q;
+        const double *b = D.b;
+        const int vhi = D.n16;
+        EpiResidual er{b, r, 0.0, vpol};
+        if (!cta_spmv_src<false>(L, C, x, S, dyn, pp, er)) return;
+        double bbp = 0.0;
+        MF_PAIRS(4, 0, vhi, {
+            double2 rv[_vb], bv[_vb];
+#pragma unroll
+            MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+                bv[u] = ld2_hint(b + 2 * MF_PI(u), vpol);
+            }
+#pragma unroll
+            MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                st2_hint(d + 2 * MF_PI(u), rv[u], vpol);
+                bbp += bv[u].x * bv[u].x + bv[u].y * bv[u].y;
+            }
+        })
+        double v2[2] = {er.rr, bbp}, o2[2];
+        block_sum<2>(S, v2, o2);
+        double rr = o2[0];
+        const double bb = o2[1];
+        const double bnorm = sqrt(bb);
+        double rel = bnorm > 0 ? sqrt(rr) / bnorm : 0.0;
+        int it = 0, status = MF_OK;
+        while (it < maxit && (fixed || rel > B.tol)) {
+            EpiQ eq{d, q, 0.0, vpol};
+            if (!cta_spmv_src<false>(L, C, d, S, dyn, pp, eq)) return;
+            double v1[1] = {eq.dq}, o1[1];
+            block_sum<1>(S, v1, o1);
+            const double dq = o1[0];
+            if (!(dq != 0.0) || !isfinite(dq)) {
+                status = MF_ERR_BREAKDOWN;
+                break;
+            }
+            const double alpha = rr / dq;
+            double rrp = 0.0;
+            MF_PAIRS(4, 0, vhi, {
+                double2 rv[_vb], qv[_vb];
+#pragma unroll
+                MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                    rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+                    qv[u] = ld2_hint(q + 2 * MF_PI(u), vpol);
+                }
+#pragma unroll
+                MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                    double2 o;
+                    o.x = rv[u].x - alpha * qv[u].x;
+                    o.y = rv[u].y - alpha * qv[u].y;
+                    st2_hint(r + 2 * MF_PI(u), o, vpol);
+                    rrp += o.x * o.x + o.y * o.y;
+                }
+            })
+            double w1[1] = {rrp}, u1[1];
+            block_sum<1>(S, w1, u1);
+            const double rrn = u1[0];
+            ++it;
+            rel = bnorm > 0 ? sqrt(rrn) / bnorm : 0.0;
+            const double beta = rrn / rr;
+            const bool done = !fixed && rel <= B.tol;
+            MF_PAIRS(4, 0, vhi, {
+                double2 dv[_vb], xv[_vb], rv[_vb];
+#pragma unroll
+                MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                    dv[u] = ld2_hint(d + 2 * MF_PI(u), vpol);
+                    xv[u] = ld2_hint(x + 2 * MF_PI(u), vpol);
+                    rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+                }
+#pragma unroll
+                MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                    double2 xo, dn;
+                    xo.x = xv[u].x + alpha * dv[u].x;
+                    xo.y = xv[u].y + alpha * dv[u].y;
+                    st2_hint(x + 2 * MF_PI(u), xo, vpol);
+                    if (!done) {
+                        dn.x = rv[u].x + beta * dv[u].x;
+                        dn.y = rv[u].y + beta * dv[u].y;
+                        st2_hint(d + 2 * MF_PI(u), dn, vpol);
+                    }
+                }
+            })
+            rr = rrn;
+            __syncthreads();  // d complete before the next SpMV stages it
+            if (!isfinite(rrn)) {
+                status = MF_ERR_BREAKDOWN;
+                break;
+            }
+        }
+        if (tid == 0) {
+            if (status == MF_OK && !fixed && rel > B.tol) status = MF_ERR_NOT_CONVERGED;
+            BatchResult R;
+            R.iterations = it;
+            R.status = status;
+            R.rr = rr;
+            R.bb = bb;
+            B.res[sys] = R;
+        }
+        __syncthreads();
+    }
+}
+
 // ================================================================= host side
 static int dyn_smem(int slab_max) { return STAGES * stage_stride_of(slab_max); }
 
@@ -824,7 +1336,8 @@ int kernel_config(mf_tiles *t, int *G_out) {
         return MF_ERR_ARG;
     }
     const void *kerns[] = {(const void *)k_cg<false>, (const void *)k_cg<true>, (const void *)k_bicgstab,
-                           (const void *)k_spmv<false>, (const void *)k_spmv<true>};
+                           (const void *)k_spmv<false>, (const void *)k_spmv<true>, (const void *)k_cgcg,
+                           (const void *)k_batch_cg};
     int occ_min = 1 << 30;
     for (const void *k : kerns) {
         MF_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
@@ -843,6 +1356,7 @@ int kernel_config(mf_tiles *t, int *G_out) {
 }
 
 static void fill_layout_args(LayoutArgs &a, const Layout &L) {
+    a.kind = L.kind;
     a.slabs = L.slabs.p;
     a.head = L.head.p;
     a.cta_slab = L.cta_slab.p;
@@ -894,9 +1408,17 @@ int launch_spmv(mf_tiles *t, int level, const double *x, double *y, int reps, cu
 int launch_solver(mf_tiles *t, int kind, KParams &P, cudaStream_t s) {
     const int dyn = dyn_smem(t->L64.slab_max);
     void *args[] = {&P};
-    const void *k = kind == 0 ? (P.nlay > 1 ? (const void *)k_cg<true> : (const void *)k_cg<false>)
-                              : (const void *)k_bicgstab;
+    const void *k = kind == 0   ? (P.nlay > 1 ? (const void *)k_cg<true> : (const void *)k_cg<false>)
+                    : kind == 2 ? (const void *)k_cgcg
+                                : (const void *)k_bicgstab;
     MF_CUDA_TRY(cudaLaunchCooperativeKernel(k, dim3(t->G), dim3(NTHREADS), args, dyn, s));
+    return MF_OK;
+}
+
+int launch_batch(const BatchParams &B, int grid, cudaStream_t s) {
+    const int dyn = STAGES * (B.stage_stride);
+    k_batch_cg<<<grid, NTHREADS, dyn, s>>>(B);
+    MF_CUDA_TRY(cudaGetLastError());
     return MF_OK;
 }
 

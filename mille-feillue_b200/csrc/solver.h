@@ -24,11 +24,14 @@ struct LayoutArgs {
     const uint8_t *slabs;
     const uint8_t *head;
     const int *cta_slab, *cta_rb, *cta_dep;
+    int kind;  // LAYOUT_*
+    int pad;
 };
 
 struct DevResult {
     int iterations, status, replacements, level_switches, final_layout, pad;
     double rr, bb;
+    int it_layout[KMAX_LAYOUTS];  // iterations run with each layout
 };
 
 struct KParams {
@@ -48,9 +51,45 @@ struct KParams {
     double tol;
     int maxiter, fixed_iterations, replace_every;
     int inject_wait;  // test hook: wait once on a flag that nothing sets
+    int true_check;   // confirm convergence with the FP64 true residual
+    int trace_iters;  // CTA 0 records %globaltimer at each phase boundary
+    uint64_t *trace;  // [trace_iters][8]
     double level_rel[KMAX_LAYOUTS];
     DevResult *res;
 };
+
+// ---- batched solve: one CTA per system, systems taken from a device queue
+struct GTiles {
+    const int *tile_ptr, *tile_col, *tile_off, *csrptr_off;
+    const uint8_t *ptr;
+    const double *val;
+    const uint8_t *col;
+    int tilem, rowA;
+};
+struct SysDesc {
+    const uint8_t *slabs;  // single-CTA slab layout of the system
+    const uint8_t *head;   // its STAGES issue records
+    int ns, kind;
+    GTiles gt;             // tile arrays (oversize row blocks)
+    double *b, *x, *r, *d, *q;  // 16*tilem entries each
+    int n16, pad;
+};
+struct BatchResult {
+    int iterations, status;
+    double rr, bb;
+};
+struct BatchParams {
+    const SysDesc *sys;
+    const int *order;  // systems, largest first
+    int count, maxiter, fixed_iterations, pad;
+    unsigned *queue;
+    double tol;
+    int stage_stride, slab_area;
+    uint64_t limit_ns;
+    uint32_t *sync;
+    BatchResult *res;
+};
+int launch_batch(const BatchParams &B, int grid, cudaStream_t s);
 
 int kernel_config(mf_tiles *t, int *G_out);
 void base_params(mf_tiles *t, KParams &P);

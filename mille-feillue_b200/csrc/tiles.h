@@ -52,14 +52,15 @@ struct DevArray {
 // A slab is a run of consecutive row blocks of one CTA's range, stored as one
 // 16-byte aligned byte range so that one bulk copy brings it into shared
 // memory. Byte layout (every section 16-byte aligned):
-//   SlabHeader (32 B)
+//   SlabHeader (48 B)
 //   runs[MAXRUNS]       x-segment runs to stage for the slab that the CTA
 //                       consumes STAGES slabs later (issue record)
 //   rbdir[nrb + 1]      per row block: byte offset of its block, plane count
 //   row-block blocks    one per row block, "row-sliced planes":
 //     rowlen[16]  (u8)  entries of each of the 16 rows
-//     pdesc[W]          (mixed layouts only) per plane: value offset, storage
-//                       precision, power-of-two scale
+//     pinfo             (mixed layouts only, W <= 32) u64 storage precision
+//                       of each plane (2 bits per plane) + int8 exponent of
+//                       each plane's power-of-two scale
 //     idx[W][16]        u16 x-window position (staged) or u32 column
 //                       (gather) of entry k of row r, with the flags
 //                       TILE_START (first entry of a new tile in this row)
@@ -72,8 +73,9 @@ constexpr int STAGES = 4;
 constexpr int MAXRUNS = 24;
 constexpr int XSEG_MAX = 112;      // staged x segments per slab (14 KB)
 constexpr int MAXW = 255;          // planes per row block (rowlen is u8)
+constexpr int MAXW_MIXED = 32;     // planes per row block in mixed layouts
 constexpr int SLAB_MAX_DEFAULT = 40960;
-constexpr int RB_PER_SLAB_MAX = 30;  // 2 per consumer warp
+constexpr int RB_PER_SLAB_MAX = 60;  // up to 4 per consumer warp
 constexpr int ISSUE_REC = 16 + MAXRUNS * 8;
 constexpr uint32_t IDX16_START = 0x8000u, IDX16_LOW = 0x4000u, IDX16_POS = 0x3fffu;
 constexpr uint32_t IDX32_START = 0x80000000u, IDX32_LOW = 0x40000000u, IDX32_POS = 0x3fffffffu;
@@ -89,8 +91,12 @@ struct SlabHeader {
     uint32_t next_bytes;  // 0 = none
     uint32_t next_xbytes;
     uint32_t bytes;
+    uint32_t pf_off16;  // slab consumed 2*STAGES later: prefetched into L2
+    uint32_t pf_bytes;  // 0 = none
+    uint32_t pad1, pad2;
 };
-static_assert(sizeof(SlabHeader) == 32, "slab header is 32 bytes");
+static_assert(sizeof(SlabHeader) == 48, "slab header is 48 bytes");
+constexpr uint32_t SLAB_HDR = 48;
 
 struct XRun {
     int32_t seg0;
@@ -102,21 +108,18 @@ struct RbDir {
     uint32_t W;    // planes
 };
 
-struct PlaneDesc {
-    uint16_t voff;  // value offset inside the block's vals section
-    uint8_t prec, pad;
-    float scale;
-};
+// Layout kinds: every tile FP64 / every tile below FP64 / both.
+enum { LAYOUT_FP64 = 0, LAYOUT_LOW = 1, LAYOUT_ANY = 2 };
 
 __host__ __device__ inline uint32_t align16u(uint32_t v) { return (v + 15u) & ~15u; }
 __host__ __device__ inline uint32_t align8u(uint32_t v) { return (v + 7u) & ~7u; }
 
-__host__ __device__ inline uint32_t slab_rbdir_off() { return align16u(32u + 8u * MAXRUNS); }
+__host__ __device__ inline uint32_t slab_rbdir_off() { return align16u(SLAB_HDR + 8u * MAXRUNS); }
 __host__ __device__ inline uint32_t slab_blocks_off(int nrb) { return align16u(slab_rbdir_off() + 8u * (nrb + 1)); }
 
 // Offsets inside one row-block block.
-__host__ __device__ inline uint32_t rb_pdesc_off() { return 16u; }
-__host__ __device__ inline uint32_t rb_idx_off(int W, bool mixed) { return mixed ? align16u(16u + 8u * W) : 16u; }
+__host__ __device__ inline uint32_t rb_pinfo_off() { return 16u; }
+__host__ __device__ inline uint32_t rb_idx_off(int W, bool mixed) { return mixed ? 16u + 48u : 16u; }
 __host__ __device__ inline uint32_t rb_vals_off(int W, bool mixed, bool gather) {
     return align16u(rb_idx_off(W, mixed) + (uint32_t)W * 16u * (gather ? 4u : 2u));
 }
@@ -145,7 +148,8 @@ struct Layout {
     std::vector<uint8_t> prec;   // host copy of the precisions
     int G = 0, nslabs = 0, n_gather = 0, n_oversize = 0;
     int slab_max = 0, rb_per_slab = 0;  // stage size / row blocks the planner used
-    bool mixed = false;                  // plane descriptors present
+    bool mixed = false;                  // plane precision info present
+    int kind = 0;                        // LAYOUT_*
     size_t bytes = 0;
     double alg_bytes = 0;        // algorithmic bytes of one SpMV
     double tile_frac[4] = {0, 0, 0, 0};
@@ -176,6 +180,8 @@ struct mf_tiles {
     mf::Layout L64;
     mf::Layout Lmix[MF_NLEVELS];
     bool mixed_ready = false;
+    int nlevels = 0;                        // mixed levels built
+    double level_switch[MF_NLEVELS] = {0};  // relative residual to leave level l
     double encode_ms = 0, layout_ms = 0;
     // host copies used by the layout planner; h_cta_rb is the CTA row-block
     // partition shared by every layout of this matrix
@@ -184,6 +190,8 @@ struct mf_tiles {
     mf::DevArray<double> ws;
     mf::DevArray<uint32_t> sync;
     mf::DevArray<double> xpad;  // padded copy of a user x for mf_spmv
+    mf::DevArray<uint64_t> trace;  // phase timestamps of the last traced solve
+    int trace_iters = 0;
 };
 
 namespace mf {

@@ -30,6 +30,7 @@ def main():
     ap.add_argument("--rb-per-slab", type=int, default=0)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--time", action="store_true", help="print the CUDA-event time of the launches")
+    ap.add_argument("--trace", type=int, default=0, help="trace the phases of the first N CG iterations")
     args = ap.parse_args()
     import torch
 
@@ -69,8 +70,20 @@ def main():
         print("spmv done", float(x.abs().sum()))
         return
     o = mf.options(fixed_iterations=args.iters, **kw)
+    if args.trace > 0:
+        o.reserved[1] = args.trace
     if args.kernel == "cg":
         res = t.solve_cg_dev(b.data_ptr(), x.data_ptr(), 1e-10, 40000, o)
+        if args.trace > 0:
+            tr = t.trace(args.trace).astype(np.float64)
+            tr = tr[(tr[:, 0] > 0) & (tr[:, 6] > 0)]
+            names = ["halo wait", "SpMV", "dot d.q", "r update", "dot r.r", "x/d update+publish"]
+            d = np.diff(tr[:, :7], axis=1) / 1e3
+            it_us = np.diff(tr[:, 0]) / 1e3
+            print("trace over %d iterations (us, median):" % len(tr))
+            for k, nm in enumerate(names):
+                print("  %-22s %8.2f" % (nm, np.median(d[:, k])))
+            print("  %-22s %8.2f" % ("iteration", np.median(it_us)))
     else:
         res = t.solve_bicgstab_dev(b.data_ptr(), x.data_ptr(), 1e-10, 10000, o)
     torch.cuda.synchronize()

@@ -1,0 +1,45 @@
+"""Batched persistent launch: every system solved by one CTA from a queue,
+compared with the single-system solver and the CPU oracle."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_batch_matches_single_system_solver(mf, O):
+    import torch
+
+    sizes = [1000, 1500, 2333, 4000, 777, 16, 5000, 12000, 3000, 9000]
+    mats = [mf.Matrix.spd_random(n, 100 + i) for i, n in enumerate(sizes)]
+    mats.append(mf.Matrix.poisson2d(40))
+    B = mf.Batch(mats, with_baseline=True)
+    b = np.concatenate([m.b() for m in mats])
+    bd = torch.tensor(b, device="cuda")
+    xd = torch.zeros_like(bd)
+    ms = B.solve_cg_dev(bd.data_ptr(), xd.data_ptr(), 1e-10, 10000)
+    assert ms > 0
+    it, st, rel = B.results()
+    assert np.all(st == 0) and np.all(rel <= 1e-10)
+    x = xd.cpu().numpy()
+    # graph replay gives the identical answer
+    xd2 = torch.zeros_like(bd)
+    B.solve_cg_dev(bd.data_ptr(), xd.data_ptr(), 1e-10, 10000)
+    assert np.array_equal(xd.cpu().numpy(), x)
+    off = B.offsets
+    import scipy.sparse as sp
+
+    for s, m in enumerate(mats):
+        rp, ci, v = m.csr()
+        n = m.n
+        M = sp.csr_matrix((v, ci, rp), shape=(n, n))
+        xs = x[off[s]:off[s + 1]]
+        assert np.linalg.norm(m.b() - M @ xs) / np.linalg.norm(m.b()) <= 1.5e-10
+        o = O.OracleTiles(n, n, rp, ci, v)
+        it_o, _, _ = o.cg(m.b(), 1e-10, 10000)
+        assert abs(int(it[s]) - it_o) <= max(2, 0.02 * it_o), (s, it[s], it_o)
+    # one launch per system
+    B.solve_cg_each_dev(bd.data_ptr(), xd2.data_ptr(), 1e-10, 10000)
+    it2, st2, rel2 = B.results()
+    assert np.all(st2 == 0)
+    assert np.max(np.abs(it2 - it)) <= 2
+    assert np.linalg.norm(xd2.cpu().numpy() - x) / np.linalg.norm(x) < 1e-8

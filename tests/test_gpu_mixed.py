@@ -1,0 +1,68 @@
+"""Mixed-precision layouts: per-tile precision from the magnitude rule,
+bit-exact SpMV against the oracle's definition, and solves that reach the
+FP64 true-residual tolerance."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_rule_layout_spmv_bitexact(mf, O):
+    import torch
+
+    for A in (mf.Matrix.varpoisson3d(24), mf.Matrix.poisson2d(96), mf.Matrix.spd_random(6000, 4)):
+        n = A.n
+        rp, ci, v = A.csr()
+        t = mf.Tiles(A, mf.options(precision_mode=mf.MODE_MIXED_RULE))
+        p, _ = t.precisions()
+        assert p.max() > 0  # some tiles below FP64
+        o = O.OracleTiles(n, n, rp, ci, v)
+        x = np.random.default_rng(5).standard_normal(n)
+        xd = torch.tensor(x, device="cuda")
+        yd = torch.zeros(n, dtype=torch.float64, device="cuda")
+        t.spmv_level_dev(0, xd.data_ptr(), yd.data_ptr())
+        assert np.array_equal(yd.cpu().numpy(), o.mixed_spmv(p, x))
+
+
+def test_random_per_tile_precisions_bitexact(mf, O):
+    """Planes whose entries come from tiles of different precisions / scales
+    are stored at a common width without changing any dequantized value."""
+    import torch
+
+    A = mf.Matrix.spd_random(8000, 6)
+    n = A.n
+    rp, ci, v = A.csr()
+    t = mf.Tiles(A)
+    tn = t.info()["tilenum"]
+    p = np.random.default_rng(1).integers(0, 4, tn).astype(np.uint8)
+    t.set_precisions(p)
+    o = O.OracleTiles(n, n, rp, ci, v)
+    x = np.random.default_rng(2).standard_normal(n)
+    xd = torch.tensor(x, device="cuda")
+    yd = torch.zeros(n, dtype=torch.float64, device="cuda")
+    t.spmv_level_dev(0, xd.data_ptr(), yd.data_ptr())
+    assert np.array_equal(yd.cpu().numpy(), o.mixed_spmv(p, x))
+
+
+@pytest.mark.parametrize("N", [24, 48])
+def test_mixed_cg_reaches_fp64_tolerance(mf, N):
+    A = mf.Matrix.varpoisson3d(N)
+    b = A.b()
+    t = mf.Tiles(A, mf.options(precision_mode=mf.MODE_MIXED_RULE))
+    x64, r64 = t.solve_cg(b, tol=1e-10, maxiter=40000, opts=mf.options())
+    xm, rm = t.solve_cg(b, tol=1e-10, maxiter=40000)
+    assert r64["status"] == 0 and rm["status"] == 0, (r64, rm)
+    assert rm["rel_residual_true"] <= 1e-10, rm
+    assert rm["iterations"] <= 1.15 * r64["iterations"], (rm["iterations"], r64["iterations"])
+    assert np.linalg.norm(xm - x64) / np.linalg.norm(x64) < 1e-6
+    assert rm["replacements"] >= rm["iterations"] // 50
+
+
+def test_mixed_cg_full_size_varpoisson_128(mf):
+    A = mf.Matrix.varpoisson3d(128)
+    b = A.b()
+    t = mf.Tiles(A, mf.options(precision_mode=mf.MODE_MIXED_RULE))
+    xm, rm = t.solve_cg(b, tol=1e-10, maxiter=40000)
+    assert rm["status"] == 0 and rm["rel_residual_true"] <= 1e-10, rm
+    xs = A.xstar()
+    assert np.linalg.norm(xm - xs) / np.linalg.norm(xs) < 1e-4
