@@ -81,7 +81,11 @@ typedef struct {
                                 iterations (see mf_trace); reserved[2] = 1:
                                 mixed layouts use the classic two-reduction
                                 CG instead of the single-reduction
-                                (Chronopoulos-Gear) form                      */
+                                (Chronopoulos-Gear) form; reserved[3] = 1:
+                                L2 prefetch of slabs 2*STAGES ahead of the
+                                copy ring (off by default: on B200 it cost
+                                2-10 us per SpMV; read at encode for
+                                mf_spmv, at solve for the solvers)            */
 } mf_options;
 void mf_options_default(mf_options *opt);
 

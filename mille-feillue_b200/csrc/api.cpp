@@ -398,6 +398,7 @@ static int solve_dev(mf_tiles *t, int kind, const double *b_dev, double *x_dev, 
     P.replace_every = opt.replace_every;
     P.res = v.res;
     P.inject_wait = opt.reserved[0] == 0x5741 ? 1 : 0;
+    P.prefetch = opt.reserved[3] == 1 ? 1 : 0;
     if (opt.reserved[1] > 0) {
         const int ti = opt.reserved[1] > 4096 ? 4096 : opt.reserved[1];
         if (t->trace.n < (size_t)ti * 8 && t->trace.alloc((size_t)ti * 8)) return MF_ERR_NOMEM;

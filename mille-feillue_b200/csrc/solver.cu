@@ -273,6 +273,7 @@ struct PipeCfg {
     int stage_stride, slab_area;
     uint64_t limit_ns;
     uint32_t *sync;
+    int prefetch;  // L2 bulk prefetch of the slab 2*STAGES ahead (off by default: it slowed the ring)
 };
 __device__ __forceinline__ GTiles gtiles_of(const KParams &P) {
     return GTiles{P.tile_ptr, P.tile_col, P.tile_off, P.csrptr_off, P.ptr, P.val, P.col, P.tilem, P.rowA};
@@ -349,7 +350,7 @@ __device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const double *x
                     xbytes = h->next_xbytes;
                     nruns = h->next_nruns;
                     runs = reinterpret_cast<const XRun *>(st + SLAB_HDR);
-                    if (h->pf_bytes) bulk_prefetch_l2(L.slabs + (size_t)h->pf_off16 * 16, h->pf_bytes);
+                    if (C.prefetch && h->pf_bytes) bulk_prefetch_l2(L.slabs + (size_t)h->pf_off16 * 16, h->pf_bytes);
                 }
                 fence_proxy_async_smem();
                 issue_slab(S, st, slab_area, k, off16, bytes, xbytes, nruns, runs, L.slabs, xv, pm, pv);
@@ -406,13 +407,22 @@ __device__ bool cta_spmv(const KParams &P, int lay, const double *xv, Smem &S, u
     L.kind = P.lay[lay].kind;
     L.site = lay;
     L.gt = gtiles_of(P);
-    const PipeCfg C{P.stage_stride, P.slab_area, P.limit_ns, P.sync};
+    const PipeCfg C{P.stage_stride, P.slab_area, P.limit_ns, P.sync, P.prefetch};
     return cta_spmv_src<MIXED>(L, C, xv, S, dyn, pp, epi);
 }
 
 // Block reduction of NV partials in a fixed order, then the grid-wide sum.
+// A group of G CTAs that synchronize with each other (the whole grid for the
+// single-system kernels, a slice of it for the batched one).
+struct Ctx {
+    uint32_t *sync;
+    double *partial;
+    int G, rank;
+    uint64_t limit_ns;
+};
+
 template <int NV>
-__device__ bool grid_sum(const KParams &P, Smem &S, const double (&v)[NV], double (&out)[NV], uint32_t &phase) {
+__device__ bool group_sum(const Ctx &X, Smem &S, const double (&v)[NV], double (&out)[NV], uint32_t &phase) {
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     double t[NV];
 #pragma unroll
@@ -425,7 +435,7 @@ __device__ bool grid_sum(const KParams &P, Smem &S, const double (&v)[NV], doubl
 #pragma unroll
         for (int k = 0; k < NV; ++k) S.red[w][k] = t[k];
     __syncthreads();
-    const int G = gridDim.x;
+    const int G = X.G;
     const int slot = phase & 1;
     if (tid == 0) {
         double p[NV];
@@ -433,21 +443,21 @@ __device__ bool grid_sum(const KParams &P, Smem &S, const double (&v)[NV], doubl
         for (int k = 0; k < NV; ++k) {
             p[k] = 0.0;
             for (int q = 0; q <= NWARPS; ++q) p[k] += S.red[q][k];
-            P.partial[((size_t)slot * G + blockIdx.x) * 4 + k] = p[k];
+            X.partial[((size_t)slot * G + X.rank) * 4 + k] = p[k];
         }
-        red_release_add(P.sync + SYNC_ARRIVE, 1u);
+        red_release_add(X.sync + SYNC_ARRIVE, 1u);
         const uint32_t target = (phase + 1) * (uint32_t)G;
-        if (ld_acquire(P.sync + SYNC_ARRIVE) < target) {
+        if (ld_acquire(X.sync + SYNC_ARRIVE) < target) {
             const uint64_t t0 = globaltimer();
             for (uint32_t spin = 1;; ++spin) {
-                if (ld_acquire(P.sync + SYNC_ARRIVE) >= target) break;
+                if (ld_acquire(X.sync + SYNC_ARRIVE) >= target) break;
                 if ((spin & 63u) == 0) {
-                    if (ld_relaxed(P.sync + SYNC_ERROR) != 0u) {
+                    if (ld_relaxed(X.sync + SYNC_ERROR) != 0u) {
                         S.abort = 1;
                         break;
                     }
-                    if (globaltimer() - t0 > P.limit_ns) {
-                        set_error(P, (uint32_t)MF_ERR_TIMEOUT, 10);
+                    if (globaltimer() - t0 > X.limit_ns) {
+                        set_error_w(X.sync, (uint32_t)MF_ERR_TIMEOUT, 10);
                         S.abort = 1;
                         break;
                     }
@@ -463,7 +473,7 @@ __device__ bool grid_sum(const KParams &P, Smem &S, const double (&v)[NV], doubl
         for (int k = 0; k < NV; ++k) a[k] = 0.0;
         for (int c = lane; c < G; c += 32)
 #pragma unroll
-            for (int k = 0; k < NV; ++k) a[k] += __ldcg(&P.partial[((size_t)slot * G + c) * 4 + k]);
+            for (int k = 0; k < NV; ++k) a[k] += __ldcg(&X.partial[((size_t)slot * G + c) * 4 + k]);
 #pragma unroll
         for (int k = 0; k < NV; ++k)
 #pragma unroll
@@ -479,33 +489,42 @@ __device__ bool grid_sum(const KParams &P, Smem &S, const double (&v)[NV], doubl
     return true;
 }
 
+__device__ __forceinline__ Ctx ctx_of(const KParams &P) {
+    return Ctx{P.sync, P.partial, (int)gridDim.x, (int)blockIdx.x, P.limit_ns};
+}
+template <int NV>
+__device__ bool grid_sum(const KParams &P, Smem &S, const double (&v)[NV], double (&out)[NV], uint32_t &phase) {
+    return group_sum<NV>(ctx_of(P), S, v, out, phase);
+}
+
 // Publish this CTA's rows of the halo vectors under epoch `ep`.
-__device__ void publish(const KParams &P, uint32_t ep) {
+__device__ void publish_x(const Ctx &X, uint32_t ep) {
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
         fence_proxy_async_global();
-        st_release(P.sync + SYNC_FLAGS + blockIdx.x * FLAG_STRIDE, ep);
+        st_release(X.sync + SYNC_FLAGS + X.rank * FLAG_STRIDE, ep);
     }
 }
+__device__ void publish(const KParams &P, uint32_t ep) { publish_x(ctx_of(P), ep); }
 
-// Wait until every CTA whose rows this CTA reads has published epoch `ep`.
-__device__ bool wait_deps(const KParams &P, Smem &S, int lay, uint32_t ep) {
-    const int lo = P.lay[lay].cta_dep[2 * blockIdx.x], hi = P.lay[lay].cta_dep[2 * blockIdx.x + 1];
+// Wait until the group's CTAs lo..hi (whose rows this CTA reads) have
+// published epoch `ep`.
+__device__ bool wait_deps_x(const Ctx &X, Smem &S, int lo, int hi, uint32_t ep) {
     if (threadIdx.x < 32) {
         for (int c = lo + (int)threadIdx.x; c <= hi; c += 32) {
-            const uint32_t *f = P.sync + SYNC_FLAGS + c * FLAG_STRIDE;
+            const uint32_t *f = X.sync + SYNC_FLAGS + c * FLAG_STRIDE;
             if (ld_acquire(f) >= ep) continue;
             const uint64_t t0 = globaltimer();
             for (uint32_t spin = 1;; ++spin) {
                 if (ld_acquire(f) >= ep) break;
                 if ((spin & 63u) == 0) {
-                    if (ld_relaxed(P.sync + SYNC_ERROR) != 0u) {
+                    if (ld_relaxed(X.sync + SYNC_ERROR) != 0u) {
                         S.abort = 1;
                         break;
                     }
-                    if (globaltimer() - t0 > P.limit_ns) {
-                        set_error(P, (uint32_t)MF_ERR_TIMEOUT, 20);
+                    if (globaltimer() - t0 > X.limit_ns) {
+                        set_error_w(X.sync, (uint32_t)MF_ERR_TIMEOUT, 20);
                         S.abort = 1;
                         break;
                     }
@@ -516,6 +535,9 @@ __device__ bool wait_deps(const KParams &P, Smem &S, int lay, uint32_t ep) {
     }
     __syncthreads();
     return S.abort == 0;
+}
+__device__ bool wait_deps(const KParams &P, Smem &S, int lay, uint32_t ep) {
+    return wait_deps_x(ctx_of(P), S, P.lay[lay].cta_dep[2 * blockIdx.x], P.lay[lay].cta_dep[2 * blockIdx.x + 1], ep);
 }
 
 __device__ void kernel_setup(const KParams &P, Smem &S, int nlay) {
@@ -1200,7 +1222,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_batch_cg(BatchParams B) {
     const int tid = threadIdx.x;
     Pipe pp;
     const uint64_t vpol = policy_evict_last();
-    const PipeCfg C{B.stage_stride, B.slab_area, B.limit_ns, B.sync};
+    const PipeCfg C{B.stage_stride, B.slab_area, B.limit_ns, B.sync, 0};
     const bool fixed = B.fixed_iterations > 0;
     const int maxit = fixed ? B.fixed_iterations : B.maxiter;
     while (true) {
@@ -1380,6 +1402,7 @@ void base_params(mf_tiles *t, KParams &P) {
     P.col = t->col.p;
     const double lim = t->opt.timeout_s > 0 ? t->opt.timeout_s : 2.0;
     P.limit_ns = (uint64_t)(lim * 1e9);
+    P.prefetch = t->opt.reserved[3] == 1 ? 1 : 0;
     fill_layout_args(P.lay[0], t->L64);
     P.nlay = 1;
 }

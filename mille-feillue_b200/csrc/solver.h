@@ -53,6 +53,7 @@ struct KParams {
     int inject_wait;  // test hook: wait once on a flag that nothing sets
     int true_check;   // confirm convergence with the FP64 true residual
     int trace_iters;  // CTA 0 records %globaltimer at each phase boundary
+    int prefetch;     // L2 bulk prefetch of slabs ahead of the ring
     uint64_t *trace;  // [trace_iters][8]
     double level_rel[KMAX_LAYOUTS];
     DevResult *res;

@@ -75,7 +75,7 @@ constexpr int XSEG_MAX = 112;      // staged x segments per slab (14 KB)
 constexpr int MAXW = 255;          // planes per row block (rowlen is u8)
 constexpr int MAXW_MIXED = 32;     // planes per row block in mixed layouts
 constexpr int SLAB_MAX_DEFAULT = 40960;
-constexpr int RB_PER_SLAB_MAX = 60;  // up to 4 per consumer warp
+constexpr int RB_PER_SLAB_MAX = 30;  // one per consumer half-warp
 constexpr int ISSUE_REC = 16 + MAXRUNS * 8;
 constexpr uint32_t IDX16_START = 0x8000u, IDX16_LOW = 0x4000u, IDX16_POS = 0x3fffu;
 constexpr uint32_t IDX32_START = 0x80000000u, IDX32_LOW = 0x40000000u, IDX32_POS = 0x3fffffffu;

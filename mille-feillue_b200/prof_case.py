@@ -31,6 +31,7 @@ def main():
     ap.add_argument("--ctas-per-sm", type=int, default=0)
     ap.add_argument("--time", action="store_true", help="print the CUDA-event time of the launches")
     ap.add_argument("--trace", type=int, default=0, help="trace the phases of the first N CG iterations")
+    ap.add_argument("--prefetch", action="store_true", help="L2 prefetch of slabs ahead of the copy ring")
     args = ap.parse_args()
     import torch
 
@@ -49,6 +50,8 @@ def main():
         level = 0
     kw.update(slab_bytes=args.slab_bytes, rb_per_slab=args.rb_per_slab, ctas_per_sm=args.ctas_per_sm)
     opts = mf.options(**kw)
+    if args.prefetch:
+        opts.reserved[3] = 1
     t = mf.Tiles(A, opts)
     n = A.n
     b = torch.tensor(A.b(), device="cuda")
@@ -72,6 +75,8 @@ def main():
     o = mf.options(fixed_iterations=args.iters, **kw)
     if args.trace > 0:
         o.reserved[1] = args.trace
+    if args.prefetch:
+        o.reserved[3] = 1
     if args.kernel == "cg":
         res = t.solve_cg_dev(b.data_ptr(), x.data_ptr(), 1e-10, 40000, o)
         if args.trace > 0:
