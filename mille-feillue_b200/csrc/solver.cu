@@ -49,8 +49,10 @@ struct __align__(16) Smem {
 
 __device__ __forceinline__ uint8_t *stage_ptr(uint8_t *dyn, int k, int stride) { return dyn + (size_t)k * stride; }
 
+// The standalone SpMV launch has no sync block (sync == nullptr): a timeout
+// there only aborts the CTA.
 __device__ void set_error_w(uint32_t *sync, uint32_t code, uint32_t site) {
-    if (atomicCAS(sync + SYNC_ERROR, 0u, code) == 0u) atomicExch(sync + SYNC_SITE, site);
+    if (sync && atomicCAS(sync + SYNC_ERROR, 0u, code) == 0u) atomicExch(sync + SYNC_SITE, site);
 }
 __device__ void set_error(const KParams &P, uint32_t code, uint32_t site) { set_error_w(P.sync, code, site); }
 
