@@ -237,6 +237,19 @@ int mf_solve_bicgstab(mf_tiles *t, const double *b_host, double *x_host,
 int mf_solve_bicgstab_dev(mf_tiles *t, const double *b_dev, double *x_dev,
                           double tol, int maxiter, const mf_options *opt,
                           mf_result *res);
+/* mf_solve_cg_dev without device allocation (no counterpart in the
+ * reference): the FP64 CG with all of its scratch in a static device array,
+ * for callers that cannot allocate at solve time (their allocator holds the
+ * free HBM, or they can't afford cudaMalloc's device-wide synchronization).
+ * Limit: n rounded up to 16 <= MF_NOALLOC_MAX_ROWS, else MF_ERR_ARG.
+ * Always FP64 (mixed layouts unused); time_ms is 0; reserved[1] is ignored.
+ * The first call on a device sets up (looks up the scratch address): make it
+ * before any stream capture. One scratch per device: overlapping calls on one
+ * device race and must be serialized by the caller.                        */
+#define MF_NOALLOC_MAX_ROWS 131072
+int mf_solve_cg_dev_noalloc(mf_tiles *t, const double *b_dev, double *x_dev,
+                            double tol, int maxiter, const mf_options *opt,
+                            mf_result *res);
 /* Phase timestamps (ns, %globaltimer of CTA 0) of the last traced CG solve:
  * out[8*i + s] for iteration i, slot s = 0 iteration start, 1 halo ready,
  * 2 SpMV done, 3 alpha known, 4 r updated, 5 beta known, 6 x / d published.

@@ -35,6 +35,7 @@ MF_ERR_UNSUPPORTED = -9
 
 PREC_FP64, PREC_FP32, PREC_FP16, PREC_FP8 = 0, 1, 2, 3
 MODE_FP64, MODE_MIXED_RULE, MODE_MIXED_MLP, MODE_FIXED = 0, 1, 2, 3
+NOALLOC_MAX_ROWS = 131072  # MF_NOALLOC_MAX_ROWS
 
 _i = C.c_int
 _d = C.c_double
@@ -109,6 +110,7 @@ EXPORTED = [
     "mf_solve_bicgstab_dev", "mf_true_residual", "cg_solve_inc", "bicgstab", "mf_version", "mf_last_error",
     "mf_spmv_level", "mf_spmv_bench_level", "mf_trace", "mf_batch_create", "mf_batch_solve_cg_dev",
     "mf_batch_solve_cg_each_dev", "mf_batch_results", "mf_batch_info", "mf_batch_free",
+    "mf_solve_cg_dev_noalloc",
 ]
 
 _lib = None
@@ -157,7 +159,8 @@ def lib():
     L.mf_spmv_host.argtypes = [_p, _p, _p]
     L.mf_spmv_bench.argtypes = [_p, _p, _p, _i, C.POINTER(_d), C.POINTER(_d)]
     L.mf_spmv_bench_level.argtypes = [_p, _i, _p, _p, _i, C.POINTER(_d), C.POINTER(_d)]
-    for f in ("mf_solve_cg", "mf_solve_cg_dev", "mf_solve_bicgstab", "mf_solve_bicgstab_dev"):
+    for f in ("mf_solve_cg", "mf_solve_cg_dev", "mf_solve_bicgstab", "mf_solve_bicgstab_dev",
+              "mf_solve_cg_dev_noalloc"):
         getattr(L, f).argtypes = [_p, _p, _p, _d, _i, C.POINTER(MfOptions), C.POINTER(MfResult)]
     L.mf_true_residual.argtypes = [_p, _p, _p, C.POINTER(_d)]
     L.mf_trace.argtypes = [_p, _p, _i]
@@ -413,6 +416,10 @@ class Tiles:
 
     def solve_bicgstab_dev(self, b_ptr, x_ptr, tol=1e-10, maxiter=10000, opts=None):
         return self._solve_dev(lib().mf_solve_bicgstab_dev, b_ptr, x_ptr, tol, maxiter, opts)
+
+    def solve_cg_dev_noalloc(self, b_ptr, x_ptr, tol=1e-10, maxiter=10000, opts=None):
+        """FP64 CG with static device scratch (no allocation; n <= NOALLOC_MAX_ROWS)."""
+        return self._solve_dev(lib().mf_solve_cg_dev_noalloc, b_ptr, x_ptr, tol, maxiter, opts)
 
     def trace(self, max_iters=4096):
         """Phase timestamps of the last traced CG solve, shape (iters, 8)."""

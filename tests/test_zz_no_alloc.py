@@ -1,0 +1,84 @@
+"""mf_solve_cg_dev_noalloc (static device scratch, no allocation) against
+mf_solve_cg_dev, called through the C ABI. The file name sorts last so the
+suite also runs it after every other GPU test."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12  # same kernel and reduction order: the solutions agree to rounding
+
+
+def _solve(mf, fn, t, b, x0, opts):
+    import torch
+
+    x = x0.clone()
+    res = mf.MfResult()
+    rc = fn(t.h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), 1e-10, 20000, C.byref(opts), C.byref(res))
+    torch.cuda.synchronize()
+    return rc, x, res.as_dict()
+
+
+@pytest.mark.parametrize("maker", ["varpoisson3d_24", "spd_random_30000"])
+def test_noalloc_matches_cg_dev_twice(mf, maker):
+    import torch
+
+    kind, size = maker.rsplit("_", 1)
+    A = mf.Matrix.varpoisson3d(int(size)) if kind == "varpoisson3d" else mf.Matrix.spd_random(int(size), 9)
+    assert -(-A.n // 16) * 16 <= mf.NOALLOC_MAX_ROWS
+    L = mf.lib()
+    t = mf.Tiles(A)
+    o = mf.options(check_true_residual=1)
+    b = torch.tensor(A.b(), device="cuda")
+    x0 = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    rc, x_ref, r_ref = _solve(mf, L.mf_solve_cg_dev, t, b, x0, o)
+    assert rc == 0 and r_ref["status"] == 0, r_ref
+    scale = float(x_ref.abs().max())
+    for _ in range(2):  # two calls in a row reuse the same scratch
+        rc, x, r = _solve(mf, L.mf_solve_cg_dev_noalloc, t, b, x0, o)
+        assert rc == 0 and r["status"] == 0, (rc, r, L.mf_last_error())
+        assert r["iterations"] == r_ref["iterations"], (r["iterations"], r_ref["iterations"])
+        assert float((x - x_ref).abs().max()) <= RTOL * scale
+        assert r["rel_residual_true"] <= 1.1e-10, r
+        assert abs(r["rel_residual_rec"] - r_ref["rel_residual_rec"]) <= 1e-9 * r_ref["rel_residual_rec"]
+
+
+def test_noalloc_takes_no_device_memory(mf):
+    import torch
+
+    A = mf.Matrix.varpoisson3d(20)
+    L = mf.lib()
+    o = mf.options()
+    b = torch.tensor(A.b(), device="cuda")
+    x0 = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    warm = mf.Tiles(A)
+    assert _solve(mf, L.mf_solve_cg_dev_noalloc, warm, b, x0, o)[0] == 0  # per-device set-up
+    t = mf.Tiles(A)  # fresh handle: mf_solve_cg_dev would allocate its workspace here
+    x = x0.clone()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(2):
+        res = mf.MfResult()
+        rc = L.mf_solve_cg_dev_noalloc(t.h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), 1e-10, 20000,
+                                       C.byref(o), C.byref(res))
+        assert rc == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+
+
+def test_noalloc_rejects_oversize(mf):
+    import torch
+
+    A = mf.Matrix.poisson2d(400)  # 160000 rows > the static limit
+    assert A.n > mf.NOALLOC_MAX_ROWS
+    t = mf.Tiles(A)
+    b = torch.ones(A.n, dtype=torch.float64, device="cuda")
+    x = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    res = mf.MfResult()
+    rc = mf.lib().mf_solve_cg_dev_noalloc(t.h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), 1e-10, 100,
+                                          C.byref(t.opts), C.byref(res))
+    assert rc == mf.MF_ERR_ARG
+    assert b"static scratch limit" in mf.lib().mf_last_error()
+    assert float(x.abs().max()) == 0.0
