@@ -346,7 +346,9 @@ def batch_arm(args, world, rank, local, dist):
     mats = [mf.Matrix.spd_random(int(sizes[s]), 2 * 1000003 + s + 1) for s in mine] if world > 1 else mats
     gen_s = time.perf_counter() - t0
     t0 = time.perf_counter()
-    B = mf.Batch(mats, mf.options(device=dev), with_baseline=not args.no_each)
+    bopt = mf.options(device=dev)
+    bopt.reserved[4] = args.batch_group  # CTAs per system group (0 = library default)
+    B = mf.Batch(mats, bopt, with_baseline=not args.no_each)
     enc_s = time.perf_counter() - t0
     b = np.concatenate([m.b() for m in mats])
     bd = torch.tensor(b, device=f"cuda:{dev}")
@@ -382,6 +384,7 @@ def batch_arm(args, world, rank, local, dist):
         "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "batch512_spd n~logU[1e3,2e5] seed 2, CG to 1e-10", "systems": len(mats),
                    "rows_rank0": inf["rows"], "nnz_rank0": inf["nnz"], "grid": inf["grid"],
+                   "ctas_per_group": args.batch_group or 8,
                    "parallelism": f"systems split over {world} ranks (LPT)" if world > 1 else "single"},
         "iterations_min_max": [int(it.min()), int(it.max())], "all_converged": bool(np.all(st == 0)),
         "max_rel_residual": float(rel.max()),
@@ -405,6 +408,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="poisson128", choices=["poisson128", "batch"])
     ap.add_argument("--no-each", action="store_true", help="batch: skip the one-launch-per-system comparison")
+    ap.add_argument("--batch-group", type=int, default=0, help="batch: CTAs per system group (0 = default)")
     args = ap.parse_args()
     world, rank, local, dist = _dist_setup(args)
     if args.impl == "reference":

@@ -85,7 +85,9 @@ typedef struct {
                                 L2 prefetch of slabs 2*STAGES ahead of the
                                 copy ring (off by default: on B200 it cost
                                 2-10 us per SpMV; read at encode for
-                                mf_spmv, at solve for the solvers)            */
+                                mf_spmv, at solve for the solvers);
+                                reserved[4] = CTAs per system group of
+                                mf_batch_create (0 = 8)                       */
 } mf_options;
 void mf_options_default(mf_options *opt);
 
@@ -260,10 +262,11 @@ int mf_true_residual(mf_tiles *t, const double *b_dev, const double *x_dev,
                      double *rel);
 
 /* ---- batched solve of many independent systems ------------------------- */
-/* Encodes `count` square systems (host CSR) for one persistent launch in
- * which every CTA solves whole systems taken from a device queue, largest
- * first. with_baseline != 0 also builds whole-GPU layouts for
- * mf_batch_solve_cg_each_dev (one launch per system, for comparison).       */
+/* Encodes `count` square systems (host CSR) for one persistent launch. The
+ * grid is split into groups of opt->reserved[4] CTAs (0 = 8); each group
+ * solves whole systems taken from a device queue, largest first, with
+ * reductions local to the group. with_baseline != 0 also builds whole-GPU
+ * layouts for mf_batch_solve_cg_each_dev (one launch per system).          */
 typedef struct mf_batch mf_batch;
 int mf_batch_create(int count, const mf_csr *systems, const mf_options *opt,
                     int with_baseline, mf_batch **out);
@@ -272,12 +275,13 @@ int mf_batch_create(int count, const mf_csr *systems, const mf_options *opt,
  * graph on first use and replayed; *ms = device time of the replay.         */
 int mf_batch_solve_cg_dev(mf_batch *B, const double *b_dev, double *x_dev,
                           double tol, int maxiter, double *ms);
-/* The same systems with one single-system solver launch each.               */
+/* The same systems with one single-system solver launch each (x0 = 0).      */
 int mf_batch_solve_cg_each_dev(mf_batch *B, const double *b_dev, double *x_dev,
                                double tol, int maxiter, double *ms);
 /* Per-system iterations, status and recursive relative residual.            */
 int mf_batch_results(const mf_batch *B, int *iterations, int *status,
                      double *rel_residual);
+/* Totals, and the grid (groups x CTAs per group) of the batched launch.    */
 int mf_batch_info(const mf_batch *B, long long *total_rows,
                   long long *total_nnz, int *grid);
 void mf_batch_free(mf_batch *B);

@@ -1,10 +1,11 @@
 // Batched solve of many independent systems of uneven size in one
-// persistent launch: every system gets a single-CTA slab layout, the
-// persistent CTAs take systems from a device queue in decreasing nnz order
-// (longest-processing-time first) and run the FP64 CG recurrence of the
-// single-system kernel on each, synchronizing only inside the CTA. The whole
-// solve (queue reset, scatter of b, vector reset, the persistent launch,
-// gather of x) is captured once in a CUDA graph and replayed.
+// persistent launch. The grid is split into groups of gs CTAs; every system
+// gets a gs-CTA slab layout, each group takes systems from a device queue in
+// decreasing nnz order (longest-processing-time first) and runs the FP64 CG
+// recurrence of the single-system kernel on them, with reductions and halo
+// flags local to the group. The whole solve (queue reset, scatter of b,
+// vector reset, the persistent launch, gather of x) is captured once in a
+// CUDA graph and replayed.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -24,8 +25,8 @@ int encode_dev_impl(int n, int ncols, int nnz, const int *rp, const int *ci, con
 using namespace mf;
 
 struct mf_batch {
-    int count = 0, device = 0, grid = 0;
-    std::vector<mf_tiles *> one;   // single-CTA layouts (batched launch)
+    int count = 0, device = 0, grid = 0, gs = 1, ngroups = 0;
+    std::vector<mf_tiles *> one;   // gs-CTA layouts (batched launch)
     std::vector<mf_tiles *> full;  // whole-GPU layouts (one launch per system)
     std::vector<int> n;
     std::vector<long long> nnz;
@@ -36,7 +37,8 @@ struct mf_batch {
     DevArray<long long> d_voff, d_poff;
     DevArray<unsigned> d_queue;
     DevArray<BatchResult> d_res;
-    DevArray<uint32_t> d_sync;
+    DevArray<uint32_t> d_sync;    // per group sync words
+    DevArray<double> d_partial;   // per group reduction partials
     DevArray<double> ws;
     cudaStream_t stream = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -56,6 +58,10 @@ struct mf_batch {
 };
 
 namespace {
+
+constexpr int kBatchGroupDefault = 8;  // CTAs per system group
+// group sync words: arrive counter, error word, rank flags (32-byte aligned)
+size_t group_sync_words(int gs) { return (sync_words(gs) + 7) & ~(size_t)7; }
 
 // packed[poff_s + i] <-> ws vector of system s, row i (i < n_s)
 __global__ void k_scatter(const double *packed, double *ws, const long long *voff, const long long *poff,
@@ -111,6 +117,15 @@ int mf_batch_create(int count, const mf_csr *systems, const mf_options *opt_in, 
     }
     B->total_rows = po;
     B->ws_rows = vo;
+    {
+        int nsm = 0;
+        MF_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, opt.device));
+        int gs = opt.reserved[4] > 0 ? opt.reserved[4] : kBatchGroupDefault;
+        if (gs > nsm) gs = nsm;
+        B->gs = gs;
+        B->ngroups = nsm / gs;
+        B->grid = B->ngroups * gs;
+    }
     // per-system encodes: single-CTA layouts (and whole-GPU ones for the
     // one-launch-per-system comparison)
     for (int s = 0; s < count; ++s) {
@@ -125,7 +140,7 @@ int mf_batch_create(int count, const mf_csr *systems, const mf_options *opt_in, 
         MF_CUDA_TRY(cudaMemcpy(ci.p, A.col_idx, sizeof(int) * A.nnz, cudaMemcpyHostToDevice));
         MF_CUDA_TRY(cudaMemcpy(v.p, A.val, sizeof(double) * A.nnz, cudaMemcpyHostToDevice));
         mf_tiles *t1 = nullptr;
-        int rc = encode_dev_impl(A.n, A.n, A.nnz, rp.p, ci.p, v.p, &opt, 1, &t1);
+        int rc = encode_dev_impl(A.n, A.n, A.nnz, rp.p, ci.p, v.p, &opt, B->gs, &t1);
         if (rc) {
             delete B;
             return rc;
@@ -144,7 +159,8 @@ int mf_batch_create(int count, const mf_csr *systems, const mf_options *opt_in, 
     // device descriptors
     if (B->ws.alloc((size_t)5 * B->ws_rows) || B->d_desc.alloc(count) || B->d_order.alloc(count) ||
         B->d_n.alloc(count) || B->d_voff.alloc(count) || B->d_poff.alloc(count) || B->d_queue.alloc(1) ||
-        B->d_res.alloc(count) || B->d_sync.alloc(sync_words(1) + 8)) {
+        B->d_res.alloc(count) || B->d_sync.alloc((size_t)B->ngroups * group_sync_words(B->gs)) ||
+        B->d_partial.alloc((size_t)B->ngroups * 8 * B->gs)) {
         delete B;
         return MF_ERR_NOMEM;
     }
@@ -155,6 +171,9 @@ int mf_batch_create(int count, const mf_csr *systems, const mf_options *opt_in, 
         std::memset(&D, 0, sizeof D);
         D.slabs = t->L64.slabs.p;
         D.head = t->L64.head.p;
+        D.cta_slab = t->L64.cta_slab.p;
+        D.cta_rb = t->L64.cta_rb.p;
+        D.cta_dep = t->L64.cta_dep.p;
         D.ns = t->L64.nslabs;
         D.kind = t->L64.kind;
         D.gt = GTiles{t->tile_ptr.p, t->tile_col.p, t->tile_off.p, t->csrptr_off.p, t->ptr.p, t->val.p,
@@ -175,7 +194,6 @@ int mf_batch_create(int count, const mf_csr *systems, const mf_options *opt_in, 
     MF_CUDA_TRY(cudaMemcpy(B->d_n.p, B->n.data(), sizeof(int) * count, cudaMemcpyHostToDevice));
     MF_CUDA_TRY(cudaMemcpy(B->d_voff.p, B->voff.data(), sizeof(long long) * count, cudaMemcpyHostToDevice));
     MF_CUDA_TRY(cudaMemcpy(B->d_poff.p, B->poff.data(), sizeof(long long) * count, cudaMemcpyHostToDevice));
-    B->grid = B->one[0]->nsm;  // one persistent CTA per SM
     MF_CUDA_TRY(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
     BatchParams &P = B->params;
     std::memset(&P, 0, sizeof P);
@@ -186,7 +204,10 @@ int mf_batch_create(int count, const mf_csr *systems, const mf_options *opt_in, 
     P.stage_stride = stage_stride_of(B->one[0]->L64.slab_max);
     P.slab_area = slab_area_of(B->one[0]->L64.slab_max);
     P.limit_ns = (uint64_t)((opt.timeout_s > 0 ? opt.timeout_s : 2.0) * 1e9);
-    P.sync = B->d_sync.p;
+    P.gs = B->gs;
+    P.gsync_words = (int)group_sync_words(B->gs);
+    P.gsync = B->d_sync.p;
+    P.gpartial = B->d_partial.p;
     P.res = B->d_res.p;
     *out = B;
     return MF_OK;
@@ -211,7 +232,13 @@ int mf_batch_solve_cg_dev(mf_batch *B, const double *b, double *x, double tol, i
         cudaMemsetAsync(B->ws.p, 0, sizeof(double) * 5 * B->ws_rows, s);
         k_scatter<<<std::min(B->count, 1024), 256, 0, s>>>(b, B->ws.p, B->d_voff.p, B->d_poff.p, B->d_n.p,
                                                           B->count, B->ws_rows, 0);
-        launch_batch(P, B->grid, s);
+        const int lrc = launch_batch(P, B->grid, s);
+        if (lrc) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(s, &g);  // leave the stream usable
+            if (g) cudaGraphDestroy(g);
+            return lrc;
+        }
         k_gather<<<std::min(B->count, 1024), 256, 0, s>>>(x, B->ws.p, B->d_voff.p, B->d_poff.p, B->d_n.p,
                                                          B->count, B->ws_rows, 1);
         MF_CUDA_TRY(cudaStreamEndCapture(s, &B->graph));
@@ -233,9 +260,13 @@ int mf_batch_solve_cg_dev(mf_batch *B, const double *b, double *x, double tol, i
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (ms) *ms = f;
-    uint32_t err = 0;
-    MF_CUDA_TRY(cudaMemcpy(&err, B->d_sync.p + SYNC_ERROR, sizeof err, cudaMemcpyDeviceToHost));
-    return err ? (int)err : MF_OK;
+    std::vector<uint32_t> gw((size_t)B->ngroups * group_sync_words(B->gs));
+    MF_CUDA_TRY(cudaMemcpy(gw.data(), B->d_sync.p, sizeof(uint32_t) * gw.size(), cudaMemcpyDeviceToHost));
+    for (int g = 0; g < B->ngroups; ++g) {
+        const uint32_t err = gw[(size_t)g * group_sync_words(B->gs) + SYNC_ERROR];
+        if (err) return (int)err;
+    }
+    return MF_OK;
 }
 
 int mf_batch_solve_cg_each_dev(mf_batch *B, const double *b, double *x, double tol, int maxiter, double *ms) {
@@ -252,6 +283,8 @@ int mf_batch_solve_cg_each_dev(mf_batch *B, const double *b, double *x, double t
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, 0);
+    // x0 = 0, as in the batched solve
+    MF_CUDA_TRY(cudaMemsetAsync(x, 0, sizeof(double) * B->total_rows, 0));
     std::vector<BatchResult> res(B->count);
     for (int s = 0; s < B->count; ++s) {
         mf_result R;

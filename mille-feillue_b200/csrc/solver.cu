@@ -90,7 +90,10 @@ __device__ bool wait_bar(uint64_t *bar, uint32_t parity, uint64_t limit_ns) {
 // FP64 tiles: sum = 0, sum += x*v in order, acc += sum at each tile start,
 // exactly blockspmv_cpu's order. Tiles below FP64 (mixed layouts): the
 // dequantized value in FP32, sumf = fmaf(x, v, sumf), acc += sumf.
-template <int KIND>
+// GB > 1: FP64 gather rows issue GB x loads from L2 before using the first
+// (more gathers in flight, more registers: for kernels with registers to
+// spare; the solver kernels with 128 live registers take GB = 1).
+template <int KIND, int GB>
 __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &h, int j, int r, const double *xstage,
                                            const double *__restrict__ xg) {
     const RbDir d = reinterpret_cast<const RbDir *>(st + slab_rbdir_off())[j];
@@ -114,7 +117,7 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
                 }
                 sum = dadd(sum, dmul(x, v));
             }
-        } else {
+        } else if (GB == 1) {
             const uint32_t *idx = reinterpret_cast<const uint32_t *>(blk + rb_idx_off(W, false));
 #pragma unroll 4
             for (int k = 0; k < len; ++k) {
@@ -126,6 +129,32 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
                     sum = 0.0;
                 }
                 sum = dadd(sum, dmul(x, v));
+            }
+        } else {
+            // x comes from L2 entry by entry: issue GB loads before the
+            // first is used so that a lane keeps GB gathers in flight
+            const uint32_t *idx = reinterpret_cast<const uint32_t *>(blk + rb_idx_off(W, false));
+            for (int k0 = 0; k0 < len; k0 += GB) {
+                uint32_t id[GB];
+                double v[GB], x[GB];
+#pragma unroll
+                for (int u = 0; u < GB; ++u) {
+                    const bool on = k0 + u < len;
+                    id[u] = on ? idx[(k0 + u) * 16 + r] : 0u;
+                    v[u] = on ? vals[(k0 + u) * 16 + r] : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < GB; ++u) x[u] = k0 + u < len ? __ldcg(xg + (id[u] & IDX32_POS)) : 0.0;
+#pragma unroll
+                for (int u = 0; u < GB; ++u) {
+                    if (k0 + u < len) {
+                        if (id[u] & IDX32_START) {
+                            acc = dadd(acc, sum);
+                            sum = 0.0;
+                        }
+                        sum = dadd(sum, dmul(x[u], v[u]));
+                    }
+                }
             }
         }
         return dadd(acc, sum);
@@ -309,7 +338,7 @@ __device__ double global_row(const GTiles &P, int rb, int r, const double *__res
 // For every row < rowA: v = epi.pre(row) is loaded before the row's
 // entries, then epi(row, acc, v) runs with the row sum. Returns false on
 // abort.
-template <bool MIXED, class Epi>
+template <bool MIXED, class Epi, int GB = 1>
 __device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const double *xv, Smem &S, uint8_t *dyn,
                              Pipe &pp, Epi &epi) {
     const int ns = L.ns;
@@ -360,6 +389,11 @@ __device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const double *x
         }
         __syncwarp();
     } else {
+        // half-warp that takes the first row block of the slab: advancing it
+        // by each slab's row-block count spreads slabs of few row blocks
+        // (gather mode) over all half-warps, so that consecutive slabs are
+        // computed at once instead of queueing on the first few warps
+        int base = 0;
         for (int i = 0; i < ns; ++i) {
             const int k = i % STAGES;
             uint8_t *st = stage_ptr(dyn, k, stride);
@@ -378,15 +412,18 @@ __device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const double *x
                     if (row < L.gt.rowA) epi(row, acc, pv);
                 }
             } else {
-                for (int j = 2 * w + half; j < h.nrb; j += 2 * NWARPS) {
+                int j0 = 2 * w + half - base;
+                if (j0 < 0) j0 += 2 * NWARPS;
+                base = (base + h.nrb) % (2 * NWARPS);
+                for (int j = j0; j < h.nrb; j += 2 * NWARPS) {
                     const int row = (h.rb0 + j) * 16 + r;
                     const bool live = row < L.gt.rowA;
                     const double pv = live ? epi.pre(row) : 0.0;
                     const double *xsg = reinterpret_cast<const double *>(st + slab_area);
                     double acc;
-                    if (!MIXED || L.kind == LAYOUT_FP64) acc = slab_row<LAYOUT_FP64>(st, h, j, r, xsg, xv);
-                    else if (L.kind == LAYOUT_LOW) acc = slab_row<LAYOUT_LOW>(st, h, j, r, xsg, xv);
-                    else acc = slab_row<LAYOUT_ANY>(st, h, j, r, xsg, xv);
+                    if (!MIXED || L.kind == LAYOUT_FP64) acc = slab_row<LAYOUT_FP64, GB>(st, h, j, r, xsg, xv);
+                    else if (L.kind == LAYOUT_LOW) acc = slab_row<LAYOUT_LOW, GB>(st, h, j, r, xsg, xv);
+                    else acc = slab_row<LAYOUT_ANY, GB>(st, h, j, r, xsg, xv);
                     if (live) epi(row, acc, pv);
                 }
             }
@@ -400,7 +437,7 @@ __device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const double *x
 
 
 // Grid-kernel form: layout `lay` of the kernel parameters, this CTA's slabs.
-template <bool MIXED, class Epi>
+template <bool MIXED, class Epi, int GB = 1>
 __device__ bool cta_spmv(const KParams &P, int lay, const double *xv, Smem &S, uint8_t *dyn, Pipe &pp, Epi &epi) {
     SpmvSrc L;
     L.slabs = P.lay[lay].slabs;
@@ -410,7 +447,7 @@ __device__ bool cta_spmv(const KParams &P, int lay, const double *xv, Smem &S, u
     L.site = lay;
     L.gt = gtiles_of(P);
     const PipeCfg C{P.stage_stride, P.slab_area, P.limit_ns, P.sync, P.prefetch};
-    return cta_spmv_src<MIXED>(L, C, xv, S, dyn, pp, epi);
+    return cta_spmv_src<MIXED, Epi, GB>(L, C, xv, S, dyn, pp, epi);
 }
 
 // Block reduction of NV partials in a fixed order, then the grid-wide sum.
@@ -590,7 +627,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_spmv(KParams P, const double *x
     Pipe pp;
     EpiStore epi{y};
     for (int it = 0; it < reps; ++it) {
-        if (!cta_spmv<MIXED>(P, lay, x, S, dyn, pp, epi)) return;
+        if (!cta_spmv<MIXED, EpiStore, 8>(P, lay, x, S, dyn, pp, epi)) return;
     }
 }
 
@@ -1210,48 +1247,65 @@ __device__ void block_sum(Smem &S, const double (&v)[NV], double (&out)[NV]) {
     __syncthreads();
 }
 
-// Every CTA takes systems from a queue (largest first) and runs the FP64 CG
-// recurrence of the single-system kernel on it alone: the system's slabs
-// stream through the CTA's ring, the dots are block reductions, and no
-// grid-wide synchronization is needed.
+// The grid is split into groups of B.gs CTAs. Rank 0 of a group takes the
+// next system from a device queue (largest first) and a group reduction
+// hands it to the other ranks; the group then runs the FP64 CG recurrence of
+// the single-system kernel on it with the system's gs-CTA slab layout:
+// reductions and halo flags stay inside the group, so groups never wait for
+// each other and many systems are in flight at once.
 __global__ void __launch_bounds__(NTHREADS, 1) k_batch_cg(BatchParams B) {
     extern __shared__ __align__(128) uint8_t dyn[];
     __shared__ Smem S;
-    __shared__ int s_sys;
+    __shared__ unsigned s_q;
+    __shared__ int s_rng[4];
     KParams P0;  // only the fields kernel_setup reads
     P0.nlay = 0;
     kernel_setup(P0, S, 0);
     const int tid = threadIdx.x;
+    const int grp = blockIdx.x / B.gs, rank = blockIdx.x % B.gs;
+    const Ctx X{B.gsync + (size_t)grp * B.gsync_words, B.gpartial + (size_t)grp * 8 * B.gs, B.gs, rank,
+                B.limit_ns};
     Pipe pp;
+    uint32_t phase = 0, ep = 0;
     const uint64_t vpol = policy_evict_last();
-    const PipeCfg C{B.stage_stride, B.slab_area, B.limit_ns, B.sync, 0};
+    const PipeCfg C{B.stage_stride, B.slab_area, B.limit_ns, X.sync, 0};
     const bool fixed = B.fixed_iterations > 0;
     const int maxit = fixed ? B.fixed_iterations : B.maxiter;
     while (true) {
+        if (rank == 0 && tid == 0) s_q = atomicAdd(B.queue, 1u);
+        __syncthreads();
+        double v0[1] = {(rank == 0 && tid == 0) ? (double)s_q : 0.0}, o0[1];
+        if (!group_sum<1>(X, S, v0, o0, phase)) return;
+        const unsigned qi = (unsigned)o0[0];
+        if (qi >= (unsigned)B.count) break;
+        const int sys = B.order[qi];
+        const SysDesc D = B.sys[sys];
+        const uint8_t *hsrc = D.head + (size_t)rank * STAGES * ISSUE_REC;
+        for (int i = tid; i < STAGES * ISSUE_REC; i += NTHREADS) (&S.head[0][0][0])[i] = hsrc[i];
         if (tid == 0) {
-            const unsigned qi = atomicAdd(B.queue, 1u);
-            s_sys = (int)qi < B.count ? B.order[qi] : -1;
+            s_rng[0] = D.cta_slab[rank + 1] - D.cta_slab[rank];
+            s_rng[1] = D.cta_rb[rank];
+            s_rng[2] = D.cta_rb[rank + 1];
+            s_rng[3] = 0;
         }
         __syncthreads();
-        const int sys = s_sys;
-        if (sys < 0) break;
-        const SysDesc D = B.sys[sys];
-        for (int i = tid; i < STAGES * ISSUE_REC; i += NTHREADS) (&S.head[0][0][0])[i] = D.head[i];
-        __syncthreads();
+        const int dep_lo = D.cta_dep[2 * rank], dep_hi = D.cta_dep[2 * rank + 1];
         SpmvSrc L;
         L.slabs = D.slabs;
         L.head = &S.head[0][0][0];
-        L.ns = D.ns;
+        L.ns = s_rng[0];
         L.kind = D.kind;
         L.site = 40;
         L.gt = D.gt;
+        const int vlo = s_rng[1] * 16, vhi = s_rng[2] * 16;
+        __syncthreads();  // s_rng read by all before the next system overwrites it
         double *x = D.x, *r = D.r, *d = D.d, *q = D.q;
         const double *b = D.b;
-        const int vhi = D.n16;
+        // r = b - A x0, d = r (x0 is written before the launch: no halo wait)
         EpiResidual er{b, r, 0.0, vpol};
-        if (!cta_spmv_src<false>(L, C, x, S, dyn, pp, er)) return;
+        if (!cta_spmv_src<false, EpiResidual, 8>(L, C, x, S, dyn, pp, er)) return;
         double bbp = 0.0;
-        MF_PAIRS(4, 0, vhi, {
+        MF_PAIRS(4, vlo, vhi, {
             double2 rv[_vb], bv[_vb];
 #pragma unroll
             MF_FOR_VB if (MF_LIVE(u, vhi)) {
@@ -1265,17 +1319,19 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_batch_cg(BatchParams B) {
             }
         })
         double v2[2] = {er.rr, bbp}, o2[2];
-        block_sum<2>(S, v2, o2);
+        if (!group_sum<2>(X, S, v2, o2, phase)) return;
+        publish_x(X, ++ep);
         double rr = o2[0];
         const double bb = o2[1];
         const double bnorm = sqrt(bb);
         double rel = bnorm > 0 ? sqrt(rr) / bnorm : 0.0;
         int it = 0, status = MF_OK;
         while (it < maxit && (fixed || rel > B.tol)) {
+            if (!wait_deps_x(X, S, dep_lo, dep_hi, ep)) return;
             EpiQ eq{d, q, 0.0, vpol};
-            if (!cta_spmv_src<false>(L, C, d, S, dyn, pp, eq)) return;
+            if (!cta_spmv_src<false, EpiQ, 8>(L, C, d, S, dyn, pp, eq)) return;
             double v1[1] = {eq.dq}, o1[1];
-            block_sum<1>(S, v1, o1);
+            if (!group_sum<1>(X, S, v1, o1, phase)) return;
             const double dq = o1[0];
             if (!(dq != 0.0) || !isfinite(dq)) {
                 status = MF_ERR_BREAKDOWN;
@@ -1283,7 +1339,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_batch_cg(BatchParams B) {
             }
             const double alpha = rr / dq;
             double rrp = 0.0;
-            MF_PAIRS(4, 0, vhi, {
+            MF_PAIRS(4, vlo, vhi, {
                 double2 rv[_vb], qv[_vb];
 #pragma unroll
                 MF_FOR_VB if (MF_LIVE(u, vhi)) {
@@ -1300,13 +1356,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_batch_cg(BatchParams B) {
                 }
             })
             double w1[1] = {rrp}, u1[1];
-            block_sum<1>(S, w1, u1);
+            if (!group_sum<1>(X, S, w1, u1, phase)) return;
             const double rrn = u1[0];
             ++it;
             rel = bnorm > 0 ? sqrt(rrn) / bnorm : 0.0;
             const double beta = rrn / rr;
             const bool done = !fixed && rel <= B.tol;
-            MF_PAIRS(4, 0, vhi, {
+            MF_PAIRS(4, vlo, vhi, {
                 double2 dv[_vb], xv[_vb], rv[_vb];
 #pragma unroll
                 MF_FOR_VB if (MF_LIVE(u, vhi)) {
@@ -1328,13 +1384,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_batch_cg(BatchParams B) {
                 }
             })
             rr = rrn;
-            __syncthreads();  // d complete before the next SpMV stages it
+            publish_x(X, ++ep);  // d complete before any rank's next SpMV stages it
             if (!isfinite(rrn)) {
                 status = MF_ERR_BREAKDOWN;
                 break;
             }
         }
-        if (tid == 0) {
+        if (rank == 0 && tid == 0) {
             if (status == MF_OK && !fixed && rel > B.tol) status = MF_ERR_NOT_CONVERGED;
             BatchResult R;
             R.iterations = it;
@@ -1441,9 +1497,19 @@ int launch_solver(mf_tiles *t, int kind, KParams &P, cudaStream_t s) {
 }
 
 int launch_batch(const BatchParams &B, int grid, cudaStream_t s) {
-    const int dyn = STAGES * (B.stage_stride);
-    k_batch_cg<<<grid, NTHREADS, dyn, s>>>(B);
-    MF_CUDA_TRY(cudaGetLastError());
+    // cooperative: the CTAs of a group wait on each other, so all must be
+    // resident at once (the launch fails instead of deadlocking)
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(NTHREADS);
+    cfg.dynamicSmemBytes = STAGES * (size_t)B.stage_stride;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    MF_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_batch_cg, B));
     return MF_OK;
 }
 

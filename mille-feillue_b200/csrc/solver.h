@@ -59,7 +59,7 @@ struct KParams {
     DevResult *res;
 };
 
-// ---- batched solve: one CTA per system, systems taken from a device queue
+// ---- batched solve: groups of CTAs, one system per group at a time, from a device queue
 struct GTiles {
     const int *tile_ptr, *tile_col, *tile_off, *csrptr_off;
     const uint8_t *ptr;
@@ -68,8 +68,9 @@ struct GTiles {
     int tilem, rowA;
 };
 struct SysDesc {
-    const uint8_t *slabs;  // single-CTA slab layout of the system
-    const uint8_t *head;   // its STAGES issue records
+    const uint8_t *slabs;  // slab layout of the system for one group of gs CTAs
+    const uint8_t *head;   // STAGES issue records per CTA of the group
+    const int *cta_slab, *cta_rb, *cta_dep;  // per-rank slab / row-block ranges, halo ranks
     int ns, kind;
     GTiles gt;             // tile arrays (oversize row blocks)
     double *b, *x, *r, *d, *q;  // 16*tilem entries each
@@ -87,7 +88,9 @@ struct BatchParams {
     double tol;
     int stage_stride, slab_area;
     uint64_t limit_ns;
-    uint32_t *sync;
+    int gs, gsync_words;  // CTAs per group; sync words per group
+    uint32_t *gsync;      // per group: arrive counter, error word, rank flags
+    double *gpartial;     // per group: 2 slots x gs x 4 partial sums
     BatchResult *res;
 };
 int launch_batch(const BatchParams &B, int grid, cudaStream_t s);

@@ -1,18 +1,23 @@
-"""Batched persistent launch: every system solved by one CTA from a queue,
-compared with the single-system solver and the CPU oracle."""
+"""Batched persistent launch: groups of CTAs take systems from a queue and
+solve each with group-local reductions; compared with the single-system
+solver and the CPU oracle for several group sizes."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
 
-def test_batch_matches_single_system_solver(mf, O):
+@pytest.mark.parametrize("gs", [1, 4, 8, 16])
+def test_batch_matches_single_system_solver(mf, O, gs):
     import torch
 
     sizes = [1000, 1500, 2333, 4000, 777, 16, 5000, 12000, 3000, 9000]
     mats = [mf.Matrix.spd_random(n, 100 + i) for i, n in enumerate(sizes)]
     mats.append(mf.Matrix.poisson2d(40))
-    B = mf.Batch(mats, with_baseline=True)
+    o = mf.options()
+    o.reserved[4] = gs
+    B = mf.Batch(mats, o, with_baseline=True)
+    assert B.info()["grid"] == (148 // gs) * gs or B.info()["grid"] % gs == 0
     b = np.concatenate([m.b() for m in mats])
     bd = torch.tensor(b, device="cuda")
     xd = torch.zeros_like(bd)
