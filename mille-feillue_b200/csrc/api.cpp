@@ -231,17 +231,25 @@ int mf_tiles_set_precisions(mf_tiles *t, const unsigned char *prec) {
 }
 
 // ------------------------------------------------------------------ SpMV
-static int prepare_x(mf_tiles *t, const double *x, const double **xs) {
+static int prepare_x(mf_tiles *t, int level, const double *x, const void **xs, cudaStream_t st = 0) {
     // the x stage reads whole 16-entry segments: use x directly when it is
     // 16-byte aligned and covers every segment, else a padded copy
     const size_t need = (size_t)t->tilen * 16;
+    if (level >= 0 && level < MF_NLEVELS && t->mixed_ready && t->Lmix[level].x32) {
+        // the layout stages x in FP32: a rounded, zero-padded copy
+        if (t->x32buf.n < need && t->x32buf.alloc(need)) return MF_ERR_NOMEM;
+        int rc = launch_to_f32(t->colA, x, t->x32buf.p, need, st);
+        if (rc) return rc;
+        *xs = t->x32buf.p;
+        return MF_OK;
+    }
     if (((uintptr_t)x & 15u) == 0 && (size_t)t->colA == need) {
         *xs = x;
         return MF_OK;
     }
     if (t->xpad.n < need && t->xpad.alloc(need)) return MF_ERR_NOMEM;
-    MF_CUDA_TRY(cudaMemsetAsync(t->xpad.p, 0, need * sizeof(double)));
-    MF_CUDA_TRY(cudaMemcpyAsync(t->xpad.p, x, (size_t)t->colA * sizeof(double), cudaMemcpyDeviceToDevice));
+    MF_CUDA_TRY(cudaMemsetAsync(t->xpad.p, 0, need * sizeof(double), st));
+    MF_CUDA_TRY(cudaMemcpyAsync(t->xpad.p, x, (size_t)t->colA * sizeof(double), cudaMemcpyDeviceToDevice, st));
     *xs = t->xpad.p;
     return MF_OK;
 }
@@ -249,8 +257,8 @@ static int prepare_x(mf_tiles *t, const double *x, const double **xs) {
 int mf_spmv(const mf_tiles *tc, const double *x, double *y, void *stream) {
     mf_tiles *t = const_cast<mf_tiles *>(tc);
     if (!t || !x || !y) return MF_ERR_ARG;
-    const double *xs;
-    int rc = prepare_x(t, x, &xs);
+    const void *xs;
+    int rc = prepare_x(t, -1, x, &xs, (cudaStream_t)stream);
     if (rc) return rc;
     rc = launch_spmv(t, -1, xs, y, 1, (cudaStream_t)stream);
     if (rc) return rc;
@@ -261,8 +269,8 @@ int mf_spmv(const mf_tiles *tc, const double *x, double *y, void *stream) {
 int mf_spmv_level(const mf_tiles *tc, int level, const double *x, double *y) {
     mf_tiles *t = const_cast<mf_tiles *>(tc);
     if (!t || !x || !y) return MF_ERR_ARG;
-    const double *xs;
-    int rc = prepare_x(t, x, &xs);
+    const void *xs;
+    int rc = prepare_x(t, level, x, &xs);
     if (rc) return rc;
     rc = launch_spmv(t, level, xs, y, 1, 0);
     if (rc) return rc;
@@ -286,8 +294,8 @@ int mf_spmv_bench_level(const mf_tiles *tc, int level, const double *x, double *
                         double *alg_bytes) {
     mf_tiles *t = const_cast<mf_tiles *>(tc);
     if (!t || !x || !y || reps <= 0) return MF_ERR_ARG;
-    const double *xs;
-    int rc = prepare_x(t, x, &xs);
+    const void *xs;
+    int rc = prepare_x(t, level, x, &xs);  // outside the timed launches
     if (rc) return rc;
     // warm-up
     if ((rc = launch_spmv(t, level, xs, y, 1, 0))) return rc;
@@ -419,6 +427,7 @@ static int solve_dev(mf_tiles *t, int kind, const double *b_dev, double *x_dev, 
             a.cta_rb = t->Lmix[l].cta_rb.p;
             a.cta_dep = t->Lmix[l].cta_dep.p;
             a.kind = t->Lmix[l].kind;
+            a.x32 = t->Lmix[l].x32 ? 1 : 0;
             P.level_rel[nl] = t->level_switch[l];
             ++nl;
         }

@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_slabs(const SlabPlan *__r
                                                              const XRun *__restrict__ runs, TileArgs A,
                                                              const int *__restrict__ rbW,
                                                              const unsigned *__restrict__ rbvb, bool mixed,
-                                                             uint8_t *slabs) {
+                                                             uint32_t segbytes, uint8_t *slabs) {
     __shared__ uint32_t s_off[RB_PER_SLAB_MAX + 1];
     const int s = blockIdx.x;
     const SlabPlan P = plans[s];
@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_slabs(const SlabPlan *__r
             const SlabPlan Q = plans[nx];
             h.next_off16 = Q.off16;
             h.next_bytes = Q.bytes;
-            h.next_xbytes = Q.mode == SLAB_STAGED ? (uint32_t)Q.nseg * 128u : 0u;
+            h.next_xbytes = Q.mode == SLAB_STAGED ? (uint32_t)Q.nseg * segbytes : 0u;
             h.next_nruns = Q.mode == SLAB_STAGED ? (uint16_t)Q.nruns : 0;
             XRun *dst = reinterpret_cast<XRun *>(base + SLAB_HDR);
             for (int k = 0; k < h.next_nruns; ++k) dst[k] = runs[Q.run_off + k];
@@ -347,7 +347,6 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
     const int tilem = t->tilem, tilenum = t->tilenum;
     const int G = t->G;
     const int slab_max = t->opt.slab_bytes > 0 ? t->opt.slab_bytes : SLAB_MAX_DEFAULT;
-    const int rbps = t->opt.rb_per_slab > 0 ? std::min(t->opt.rb_per_slab, RB_PER_SLAB_MAX) : RB_PER_SLAB_MAX;
     const auto &tp = t->h_tile_ptr;
     const auto &tc = t->h_tile_col;
     const auto &tn = t->h_tile_nnz;
@@ -399,6 +398,12 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
         t->h_cta_rb.swap(part);
     }
     const std::vector<int> &cta_rb = t->h_cta_rb;
+    // Layouts whose tiles are all below FP64 stage x in FP32 (64-byte
+    // segments): twice the x window per stage, so slabs may hold twice the
+    // row blocks. An oversize row block turns its tiles FP64, and then the
+    // layout is planned again with FP64 x.
+    bool x32 = mixed;
+    for (size_t k = 0; k < prec.size() && x32; ++k) x32 = prec[k] != MF_PREC_FP64;
     // slabs
     std::vector<SlabPlan> plans;
     std::vector<int> seg_all;
@@ -412,68 +417,88 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
             if (i == 0 || v[i] != v[i - 1] + 1) ++r;
         return r;
     };
-    int n_gather = 0, n_over = 0;
-    for (int g = 0; g < G; ++g) {
-        cta_slab[g] = (int)plans.size();
-        int rb = cta_rb[g];
-        while (rb < cta_rb[g + 1]) {
-            SlabPlan P{};
-            P.rb0 = rb;
-            rbsegs.assign(tc.begin() + tp[rb], tc.begin() + tp[rb + 1]);  // ascending already
-            const bool staged0 = (int)rbsegs.size() <= XSEG_MAX && count_runs(rbsegs) <= MAXRUNS;
-            const uint32_t tot0 = slab_blocks_off(1) + rb_bytes(rb, !staged0);
-            if (tot0 > (uint32_t)slab_max || rbW[rb] > maxw) {
-                P.mode = SLAB_OVERSIZE;
-                P.nrb = 1;
-                P.ntiles = tp[rb + 1] - tp[rb];
-                P.bytes = slab_blocks_off(0);
-                for (int k = tp[rb]; k < tp[rb + 1]; ++k) prec[k] = MF_PREC_FP64;
-                ++n_over;
-                rb += 1;
-            } else {
-                const bool staged = staged0;
-                P.mode = staged ? SLAB_STAGED : SLAB_GATHER;
-                if (staged) cur = rbsegs;
-                P.nrb = 1;
-                P.ntiles = tp[rb + 1] - tp[rb];
-                uint32_t body = rb_bytes(rb, !staged);
-                int nx = rb + 1;
-                while (nx < cta_rb[g + 1] && P.nrb < rbps) {
-                    if (rbW[nx] > maxw) break;
-                    const uint32_t bx = rb_bytes(nx, !staged);
-                    if (slab_blocks_off(P.nrb + 1) + body + bx > (uint32_t)slab_max) break;
-                    if (staged) {
-                        merged.clear();
-                        std::set_union(cur.begin(), cur.end(), tc.begin() + tp[nx], tc.begin() + tp[nx + 1],
-                                       std::back_inserter(merged));
-                        if ((int)merged.size() > XSEG_MAX || count_runs(merged) > MAXRUNS) break;
-                        cur.swap(merged);
+    int n_gather = 0, n_over = 0, xseg_max = XSEG_MAX, rbps = RB_PER_SLAB_X64;
+    uint32_t segbytes = 128u;
+    for (;;) {
+        xseg_max = x32 ? XSEG_MAX32 : XSEG_MAX;
+        segbytes = x32 ? 64u : 128u;
+        rbps = t->opt.rb_per_slab > 0 ? std::min(t->opt.rb_per_slab, RB_PER_SLAB_MAX)
+                                      : (x32 ? RB_PER_SLAB_MAX : RB_PER_SLAB_X64);
+        plans.clear();
+        seg_all.clear();
+        run_all.clear();
+        slab_cta.clear();
+        cta_slab.assign(G + 1, 0);
+        n_gather = n_over = 0;
+        for (int g = 0; g < G; ++g) {
+            cta_slab[g] = (int)plans.size();
+            int rb = cta_rb[g];
+            while (rb < cta_rb[g + 1]) {
+                SlabPlan P{};
+                P.rb0 = rb;
+                rbsegs.assign(tc.begin() + tp[rb], tc.begin() + tp[rb + 1]);  // ascending already
+                const bool staged0 = (int)rbsegs.size() <= xseg_max && count_runs(rbsegs) <= MAXRUNS;
+                const uint32_t tot0 = slab_blocks_off(1) + rb_bytes(rb, !staged0);
+                if (tot0 > (uint32_t)slab_max || rbW[rb] > maxw) {
+                    P.mode = SLAB_OVERSIZE;
+                    P.nrb = 1;
+                    P.ntiles = tp[rb + 1] - tp[rb];
+                    P.bytes = slab_blocks_off(0);
+                    for (int k = tp[rb]; k < tp[rb + 1]; ++k) prec[k] = MF_PREC_FP64;
+                    ++n_over;
+                    rb += 1;
+                } else {
+                    const bool staged = staged0;
+                    P.mode = staged ? SLAB_STAGED : SLAB_GATHER;
+                    if (staged) cur = rbsegs;
+                    P.nrb = 1;
+                    P.ntiles = tp[rb + 1] - tp[rb];
+                    uint32_t body = rb_bytes(rb, !staged);
+                    int nx = rb + 1;
+                    while (nx < cta_rb[g + 1] && P.nrb < rbps) {
+                        if (rbW[nx] > maxw) break;
+                        const uint32_t bx = rb_bytes(nx, !staged);
+                        if (slab_blocks_off(P.nrb + 1) + body + bx > (uint32_t)slab_max) break;
+                        if (staged) {
+                            merged.clear();
+                            std::set_union(cur.begin(), cur.end(), tc.begin() + tp[nx], tc.begin() + tp[nx + 1],
+                                           std::back_inserter(merged));
+                            if ((int)merged.size() > xseg_max || count_runs(merged) > MAXRUNS) break;
+                            cur.swap(merged);
+                        }
+                        P.nrb += 1;
+                        P.ntiles += tp[nx + 1] - tp[nx];
+                        body += bx;
+                        ++nx;
                     }
-                    P.nrb += 1;
-                    P.ntiles += tp[nx + 1] - tp[nx];
-                    body += bx;
-                    ++nx;
+                    P.bytes = slab_blocks_off(P.nrb) + body;
+                    if (!staged) ++n_gather;
+                    rb = nx;
                 }
-                P.bytes = slab_blocks_off(P.nrb) + body;
-                if (!staged) ++n_gather;
-                rb = nx;
-            }
-            if (P.mode == SLAB_STAGED) {
-                P.seg_off = (int)seg_all.size();
-                P.nseg = (int)cur.size();
-                seg_all.insert(seg_all.end(), cur.begin(), cur.end());
-                P.run_off = (int)run_all.size();
-                for (size_t i = 0; i < cur.size(); ++i) {
-                    if (i == 0 || cur[i] != cur[i - 1] + 1) run_all.push_back(XRun{cur[i], 0, (uint16_t)i});
-                    run_all.back().nseg++;
+                if (P.mode == SLAB_STAGED) {
+                    P.seg_off = (int)seg_all.size();
+                    P.nseg = (int)cur.size();
+                    seg_all.insert(seg_all.end(), cur.begin(), cur.end());
+                    P.run_off = (int)run_all.size();
+                    for (size_t i = 0; i < cur.size(); ++i) {
+                        if (i == 0 || cur[i] != cur[i - 1] + 1) run_all.push_back(XRun{cur[i], 0, (uint16_t)i});
+                        run_all.back().nseg++;
+                    }
+                    P.nruns = (int)run_all.size() - P.run_off;
                 }
-                P.nruns = (int)run_all.size() - P.run_off;
+                plans.push_back(P);
+                slab_cta.push_back(g);
             }
-            plans.push_back(P);
-            slab_cta.push_back(g);
         }
+        cta_slab[G] = (int)plans.size();
+        if (x32 && n_over > 0) {
+            x32 = false;
+            prec = prec_in;
+            if ((int)prec.size() != tilenum) prec.assign(tilenum, MF_PREC_FP64);
+            continue;
+        }
+        break;
     }
-    cta_slab[G] = (int)plans.size();
     const int ns = (int)plans.size();
     uint64_t off = 0;
     for (auto &P : plans) {
@@ -500,7 +525,7 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
             const SlabPlan &P = plans[s];
             rec[0] = P.off16;
             rec[1] = P.bytes;
-            rec[2] = P.mode == SLAB_STAGED ? (uint32_t)P.nseg * 128u : 0u;
+            rec[2] = P.mode == SLAB_STAGED ? (uint32_t)P.nseg * segbytes : 0u;
             rec[3] = P.mode == SLAB_STAGED ? (uint32_t)P.nruns : 0u;
             if (P.mode == SLAB_STAGED) std::memcpy(&rec[4], &run_all[P.run_off], sizeof(XRun) * P.nruns);
         }
@@ -534,6 +559,10 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
             if (P.mode != SLAB_OVERSIZE)
                 for (int k = tp[P.rb0]; k < tp[P.rb0 + P.nrb] && !any64; ++k) any64 = prec[k] == MF_PREC_FP64;
         kind = any64 ? LAYOUT_ANY : LAYOUT_LOW;
+        // the LOW row path reads FP32 x: a layout planned with FP64 x (after
+        // an oversize row block) takes the general path, which rounds x per
+        // entry to the same FP32 value
+        if (kind == LAYOUT_LOW && !x32) kind = LAYOUT_ANY;
     }
     // algorithmic bytes and precision fractions
     double alg = 16.0 * (double)t->rowA;
@@ -564,7 +593,7 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
         MF_CUDA_TRY(cudaMemcpyAsync(d_runs.p, run_all.data(), sizeof(XRun) * run_all.size(), cudaMemcpyHostToDevice, st));
     if (ns > 0)
         k_fill_slabs<<<ns, FILL_THREADS, 0, st>>>(d_plans.p, d_slab_cta.p, L.cta_slab.p, d_segs.p, d_runs.p, A,
-                                                 d_rbW.p, d_rbvb.p, mixed, L.slabs.p);
+                                                 d_rbW.p, d_rbvb.p, mixed, segbytes, L.slabs.p);
     MF_CUDA_TRY(cudaGetLastError());
     MF_CUDA_TRY(cudaStreamSynchronize(st));
     L.prec.swap(prec);
@@ -576,6 +605,7 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
     L.rb_per_slab = rbps;
     L.mixed = mixed;
     L.kind = kind;
+    L.x32 = x32;
     L.bytes = off;
     L.alg_bytes = alg;
     for (int p = 0; p < 4; ++p) L.tile_frac[p] = tilenum > 0 ? cnt[p] / tilenum : 0.0;

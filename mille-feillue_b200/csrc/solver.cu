@@ -58,14 +58,16 @@ __device__ void set_error(const KParams &P, uint32_t code, uint32_t site) { set_
 
 // Thread 0: issue the bulk copies of one slab (x runs first, slab last: the
 // issue record may live inside the stage the slab overwrites).
+// An x segment is 16 entries: 128 bytes of FP64 x, 64 bytes of FP32 x.
 __device__ void issue_slab(Smem &S, uint8_t *stage, int slab_area, int k, uint32_t off16, uint32_t bytes,
                            uint32_t xbytes, int nruns, const XRun *runs, const uint8_t *slabs,
-                           const double *xv, uint64_t pol_m, uint64_t pol_v) {
+                           const uint8_t *xv, uint32_t segb, uint64_t pol_m, uint64_t pol_v) {
     mbar_arrive_expect_tx(&S.full[k], bytes + xbytes);
     uint8_t *xarea = stage + slab_area;
     for (int q = 0; q < nruns; ++q) {
         const XRun r = runs[q];
-        bulk_g2s(xarea + (size_t)r.slot0 * 128, xv + (size_t)r.seg0 * 16, (uint32_t)r.nseg * 128u, &S.full[k], pol_v);
+        bulk_g2s(xarea + (size_t)r.slot0 * segb, xv + (size_t)r.seg0 * segb, (uint32_t)r.nseg * segb, &S.full[k],
+                 pol_v);
     }
     bulk_g2s(stage, slabs + (size_t)off16 * 16, bytes, &S.full[k], pol_m);
 }
@@ -86,6 +88,9 @@ __device__ bool wait_bar(uint64_t *bar, uint32_t parity, uint64_t limit_ns) {
     }
 }
 
+__device__ __forceinline__ float to_f32(double v) { return __double2float_rn(v); }
+__device__ __forceinline__ float to_f32(float v) { return v; }
+
 // Sum of row r of row block j of a staged / gather slab (row-sliced planes).
 // FP64 tiles: sum = 0, sum += x*v in order, acc += sum at each tile start,
 // exactly blockspmv_cpu's order. Tiles below FP64 (mixed layouts): the
@@ -93,9 +98,9 @@ __device__ bool wait_bar(uint64_t *bar, uint32_t parity, uint64_t limit_ns) {
 // GB > 1: FP64 gather rows issue GB x loads from L2 before using the first
 // (more gathers in flight, more registers: for kernels with registers to
 // spare; the solver kernels with 128 live registers take GB = 1).
-template <int KIND, int GB>
-__device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &h, int j, int r, const double *xstage,
-                                           const double *__restrict__ xg) {
+template <int KIND, int GB, typename XT>
+__device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &h, int j, int r, const XT *xstage,
+                                           const XT *__restrict__ xg) {
     const RbDir d = reinterpret_cast<const RbDir *>(st + slab_rbdir_off())[j];
     const uint8_t *blk = st + d.off;
     const int W = (int)d.W;
@@ -110,7 +115,7 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
             for (int k = 0; k < len; ++k) {
                 const uint32_t id = idx[k * 16 + r];
                 const double v = vals[k * 16 + r];
-                const double x = xstage[id & IDX16_POS];
+                const XT x = xstage[id & IDX16_POS];
                 if (id & IDX16_START) {
                     acc = dadd(acc, sum);
                     sum = 0.0;
@@ -123,7 +128,7 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
             for (int k = 0; k < len; ++k) {
                 const uint32_t id = idx[k * 16 + r];
                 const double v = vals[k * 16 + r];
-                const double x = __ldcg(xg + (id & IDX32_POS));
+                const XT x = __ldcg(xg + (id & IDX32_POS));
                 if (id & IDX32_START) {
                     acc = dadd(acc, sum);
                     sum = 0.0;
@@ -136,7 +141,8 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
             const uint32_t *idx = reinterpret_cast<const uint32_t *>(blk + rb_idx_off(W, false));
             for (int k0 = 0; k0 < len; k0 += GB) {
                 uint32_t id[GB];
-                double v[GB], x[GB];
+                double v[GB];
+                XT x[GB];
 #pragma unroll
                 for (int u = 0; u < GB; ++u) {
                     const bool on = k0 + u < len;
@@ -144,7 +150,7 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
                     v[u] = on ? vals[(k0 + u) * 16 + r] : 0.0;
                 }
 #pragma unroll
-                for (int u = 0; u < GB; ++u) x[u] = k0 + u < len ? __ldcg(xg + (id[u] & IDX32_POS)) : 0.0;
+                for (int u = 0; u < GB; ++u) x[u] = k0 + u < len ? __ldcg(xg + (id[u] & IDX32_POS)) : XT(0);
 #pragma unroll
                 for (int u = 0; u < GB; ++u) {
                     if (k0 + u < len) {
@@ -175,12 +181,12 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
             for (int k = 0; k < len; ++k) {
                 const uint32_t id = idx[k * 16 + r];
                 const float v = v32[k * 16 + r];
-                const double x = xstage[id & IDX16_POS];
+                const XT x = xstage[id & IDX16_POS];
                 if (id & IDX16_START) {
                     acc = dadd(acc, (double)sumf);
                     sumf = 0.0f;
                 }
-                sumf = __fmaf_rn(__double2float_rn(x), v, sumf);
+                sumf = __fmaf_rn(to_f32(x), v, sumf);
             }
         } else {
             const uint32_t *idx = reinterpret_cast<const uint32_t *>(idxb);
@@ -188,12 +194,12 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
             for (int k = 0; k < len; ++k) {
                 const uint32_t id = idx[k * 16 + r];
                 const float v = v32[k * 16 + r];
-                const double x = __ldcg(xg + (id & IDX32_POS));
+                const XT x = __ldcg(xg + (id & IDX32_POS));
                 if (id & IDX32_START) {
                     acc = dadd(acc, (double)sumf);
                     sumf = 0.0f;
                 }
-                sumf = __fmaf_rn(__double2float_rn(x), v, sumf);
+                sumf = __fmaf_rn(to_f32(x), v, sumf);
             }
         }
         return dadd(acc, (double)sumf);
@@ -209,7 +215,7 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
                 const uint32_t pr = (uint32_t)(pbits >> (2 * k)) & 3u;
                 const uint32_t wlog = 3u - pr;
                 const uint32_t id = idx[k * 16 + r];
-                const double x = xstage[id & IDX16_POS];
+                const XT x = xstage[id & IDX16_POS];
                 const uint32_t boff = voff + ((uint32_t)r << wlog);
                 const uint32_t wrd = *reinterpret_cast<const uint32_t *>(vals + (boff & ~3u));
                 const uint32_t sh = (boff & 3u) * 8u;
@@ -222,7 +228,7 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
                     acc = dadd(acc, (double)sumf);
                     sumf = 0.0f;
                 }
-                sumf = __fmaf_rn(__double2float_rn(x), v, sumf);
+                sumf = __fmaf_rn(to_f32(x), v, sumf);
                 voff += 16u << wlog;
             }
         } else {
@@ -232,7 +238,7 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
                 const uint32_t pr = (uint32_t)(pbits >> (2 * k)) & 3u;
                 const uint32_t wlog = 3u - pr;
                 const uint32_t id = idx[k * 16 + r];
-                const double x = __ldcg(xg + (id & IDX32_POS));
+                const XT x = __ldcg(xg + (id & IDX32_POS));
                 const uint32_t boff = voff + ((uint32_t)r << wlog);
                 const uint32_t wrd = *reinterpret_cast<const uint32_t *>(vals + (boff & ~3u));
                 const uint32_t sh = (boff & 3u) * 8u;
@@ -245,7 +251,7 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
                     acc = dadd(acc, (double)sumf);
                     sumf = 0.0f;
                 }
-                sumf = __fmaf_rn(__double2float_rn(x), v, sumf);
+                sumf = __fmaf_rn(to_f32(x), v, sumf);
                 voff += 16u << wlog;
             }
         }
@@ -284,7 +290,7 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
                 if (pr == MF_PREC_FP16) vf = __half2float(reinterpret_cast<const __half *>(pv)[r]) * sc;
                 else vf = __half2float(__half(__nv_cvt_fp8_to_halfraw((__nv_fp8_storage_t)pv[r], __NV_E4M3))) * sc;
             }
-            sumf = __fmaf_rn(__double2float_rn(x), vf, sumf);
+            sumf = __fmaf_rn(to_f32(x), vf, sumf);
         } else {
             sum = dadd(sum, dmul(x, reinterpret_cast<const double *>(pv)[r]));
         }
@@ -298,6 +304,7 @@ struct SpmvSrc {
     const uint8_t *slabs;
     const uint8_t *head;  // STAGES issue records (shared memory)
     int ns, kind, site;
+    int x32;              // x staged in FP32 (the input vector is FP32)
     GTiles gt;
 };
 struct PipeCfg {
@@ -339,7 +346,7 @@ __device__ double global_row(const GTiles &P, int rb, int r, const double *__res
 // entries, then epi(row, acc, v) runs with the row sum. Returns false on
 // abort.
 template <bool MIXED, class Epi, int GB = 1>
-__device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const double *xv, Smem &S, uint8_t *dyn,
+__device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const void *xv, Smem &S, uint8_t *dyn,
                              Pipe &pp, Epi &epi) {
     const int ns = L.ns;
     const int stride = C.stage_stride;
@@ -384,7 +391,8 @@ __device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const double *x
                     if (C.prefetch && h->pf_bytes) bulk_prefetch_l2(L.slabs + (size_t)h->pf_off16 * 16, h->pf_bytes);
                 }
                 fence_proxy_async_smem();
-                issue_slab(S, st, slab_area, k, off16, bytes, xbytes, nruns, runs, L.slabs, xv, pm, pv);
+                issue_slab(S, st, slab_area, k, off16, bytes, xbytes, nruns, runs, L.slabs,
+                           static_cast<const uint8_t *>(xv), L.x32 ? 64u : 128u, pm, pv);
             }
         }
         __syncwarp();
@@ -408,7 +416,7 @@ __device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const double *x
                 if (w == 0 && half == 0) {
                     const int row = h.rb0 * 16 + r;
                     const double pv = row < L.gt.rowA ? epi.pre(row) : 0.0;
-                    const double acc = global_row(L.gt, h.rb0, r, xv);
+                    const double acc = global_row(L.gt, h.rb0, r, static_cast<const double *>(xv));
                     if (row < L.gt.rowA) epi(row, acc, pv);
                 }
             } else {
@@ -420,10 +428,13 @@ __device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const double *x
                     const bool live = row < L.gt.rowA;
                     const double pv = live ? epi.pre(row) : 0.0;
                     const double *xsg = reinterpret_cast<const double *>(st + slab_area);
+                    const double *xg = static_cast<const double *>(xv);
                     double acc;
-                    if (!MIXED || L.kind == LAYOUT_FP64) acc = slab_row<LAYOUT_FP64, GB>(st, h, j, r, xsg, xv);
-                    else if (L.kind == LAYOUT_LOW) acc = slab_row<LAYOUT_LOW, GB>(st, h, j, r, xsg, xv);
-                    else acc = slab_row<LAYOUT_ANY, GB>(st, h, j, r, xsg, xv);
+                    if (!MIXED || L.kind == LAYOUT_FP64) acc = slab_row<LAYOUT_FP64, GB>(st, h, j, r, xsg, xg);
+                    else if (L.kind == LAYOUT_LOW)  // always FP32 x
+                        acc = slab_row<LAYOUT_LOW, GB>(st, h, j, r, reinterpret_cast<const float *>(xsg),
+                                                       static_cast<const float *>(xv));
+                    else acc = slab_row<LAYOUT_ANY, GB>(st, h, j, r, xsg, xg);
                     if (live) epi(row, acc, pv);
                 }
             }
@@ -437,13 +448,15 @@ __device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const double *x
 
 
 // Grid-kernel form: layout `lay` of the kernel parameters, this CTA's slabs.
+// xv: FP64 vector, or FP32 when the layout stages x in FP32.
 template <bool MIXED, class Epi, int GB = 1>
-__device__ bool cta_spmv(const KParams &P, int lay, const double *xv, Smem &S, uint8_t *dyn, Pipe &pp, Epi &epi) {
+__device__ bool cta_spmv(const KParams &P, int lay, const void *xv, Smem &S, uint8_t *dyn, Pipe &pp, Epi &epi) {
     SpmvSrc L;
     L.slabs = P.lay[lay].slabs;
     L.head = &S.head[lay][0][0];
     L.ns = S.slab1[lay] - S.slab0[lay];
     L.kind = P.lay[lay].kind;
+    L.x32 = P.lay[lay].x32;
     L.site = lay;
     L.gt = gtiles_of(P);
     const PipeCfg C{P.stage_stride, P.slab_area, P.limit_ns, P.sync, P.prefetch};
@@ -620,7 +633,7 @@ struct EpiStore {
 };
 
 template <bool MIXED>
-__global__ void __launch_bounds__(NTHREADS, 1) k_spmv(KParams P, const double *x, double *y, int lay, int reps) {
+__global__ void __launch_bounds__(NTHREADS, 1) k_spmv(KParams P, const void *x, double *y, int lay, int reps) {
     extern __shared__ __align__(128) uint8_t dyn[];
     __shared__ Smem S;
     kernel_setup(P, S, lay + 1);
@@ -643,6 +656,20 @@ struct EpiResidual {  // r = b - A x, rr += r*r
     __device__ void operator()(int row, double acc, double bv) {
         const double v = bv - acc;
         st_hint(r + row, v, pol);
+        rr += v * v;
+    }
+};
+struct EpiResidual32 {  // r = b - A x and its FP32 copy, rr += r*r
+    const double *b;
+    double *r;
+    float *r32;
+    double rr;
+    uint64_t pol;
+    __device__ double pre(int row) const { return ld_hint(b + row, pol); }
+    __device__ void operator()(int row, double acc, double bv) {
+        const double v = bv - acc;
+        st_hint(r + row, v, pol);
+        stf_hint(r32 + row, __double2float_rn(v), pol);
         rr += v * v;
     }
 };
@@ -679,6 +706,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cg(KParams P) {
     const int rb_lo = P.lay[0].cta_rb[g], rb_hi = P.lay[0].cta_rb[g + 1];
     const int vlo = rb_lo * 16, vhi = rb_hi * 16;  // own rows, zero padded past rowA
     double *x = P.x, *r = P.r, *d = P.d, *q = P.q;
+    float *d32 = MIXED ? reinterpret_cast<float *>(P.t) : nullptr;  // FP32 d for FP32-x layouts
     const double *b = P.b;
     if (P.inject_wait) {
         // test hook: a dependency epoch no CTA ever publishes; the bounded
@@ -700,6 +728,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cg(KParams P) {
 #pragma unroll
         MF_FOR_VB if (MF_LIVE(u, vhi)) {
             st2_hint(d + 2 * MF_PI(u), rv[u], vpol);
+            if (MIXED)
+                stf2_hint(d32 + 2 * MF_PI(u), make_float2(__double2float_rn(rv[u].x), __double2float_rn(rv[u].y)),
+                          vpol);
             bbp += bv[u].x * bv[u].x + bv[u].y * bv[u].y;
         }
     })
@@ -761,7 +792,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cg(KParams P) {
         ++it_lay[lay];
         EpiQ eq{d, q, 0.0, vpol};
         bool ok;
-        if (MIXED && lay != lay64) ok = cta_spmv<true>(P, lay, d, S, dyn, pp, eq);
+        if (MIXED && lay != lay64) ok = cta_spmv<true>(P, lay, P.lay[lay].x32 ? (const void *)d32 : d, S, dyn, pp, eq);
         else ok = cta_spmv<false>(P, lay64, d, S, dyn, pp, eq);
         if (!ok) return;
         MF_TRACE(it, 2);
@@ -819,6 +850,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cg(KParams P) {
                     dn.x = rv[u].x + beta * dv[u].x;
                     dn.y = rv[u].y + beta * dv[u].y;
                     st2_hint(d + 2 * MF_PI(u), dn, vpol);
+                    if (MIXED)
+                        stf2_hint(d32 + 2 * MF_PI(u), make_float2(__double2float_rn(dn.x), __double2float_rn(dn.y)),
+                                  vpol);
                 }
             }
         })
@@ -885,9 +919,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cgcg(KParams P) {
     double *x = P.x, *r = P.r;
     float *pv32 = reinterpret_cast<float *>(P.d), *sv32 = reinterpret_cast<float *>(P.q),
           *wv32 = reinterpret_cast<float *>(P.s);
+    float *r32 = reinterpret_cast<float *>(P.t);  // FP32 r: the input of FP32-x layouts
     const double *b = P.b;
     // r = b - A x0; p = s = 0
-    EpiResidual er{b, r, 0.0, vpol};
+    EpiResidual32 er{b, r, r32, 0.0, vpol};
     if (!cta_spmv<false>(P, lay64, x, S, dyn, pp, er)) return;
     double bbp = 0.0;
     MF_PAIRS(4, vlo, vhi, {
@@ -918,7 +953,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cgcg(KParams P) {
         const bool repl_now = pending || (P.replace_every > 0 && it > 0 && it % P.replace_every == 0);
         if (repl_now) {
             if (!wait_deps(P, S, lay64, ep)) return;
-            EpiResidual e2{b, r, 0.0, vpol};
+            EpiResidual32 e2{b, r, r32, 0.0, vpol};
             if (!cta_spmv<false>(P, lay64, x, S, dyn, pp, e2)) return;
             double a1[1] = {e2.rr}, c1[1];
             if (!grid_sum<1>(P, S, a1, c1, phase)) return;
@@ -944,15 +979,19 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cgcg(KParams P) {
             }
         }
         if (it >= maxit) break;
+        MF_TRACE(it, 0);
         if (!wait_deps(P, S, lay, ep)) return;
+        MF_TRACE(it, 1);
         ++it_lay[lay];
         EpiW ew{r, wv32, 0.0, 0.0, vpol};
         bool ok;
-        if (lay != lay64) ok = cta_spmv<true>(P, lay, r, S, dyn, pp, ew);
+        if (lay != lay64) ok = cta_spmv<true>(P, lay, P.lay[lay].x32 ? (const void *)r32 : r, S, dyn, pp, ew);
         else ok = cta_spmv<false>(P, lay64, r, S, dyn, pp, ew);
         if (!ok) return;
+        MF_TRACE(it, 2);
         double a2[2] = {ew.g, ew.dl}, c2[2];
         if (!grid_sum<2>(P, S, a2, c2, phase)) return;
+        MF_TRACE(it, 3);
         gam = c2[0];
         const double delta = c2[1];
         rel = bnorm > 0 ? sqrt(gam) / bnorm : 0.0;
@@ -1000,13 +1039,17 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cgcg(KParams P) {
                 ro.y = rv[u].y - alpha * (double)sf.y;
                 st2_hint(x + 2 * MF_PI(u), xo, vpol);
                 st2_hint(r + 2 * MF_PI(u), ro, vpol);
+                stf2_hint(r32 + 2 * MF_PI(u), make_float2(__double2float_rn(ro.x), __double2float_rn(ro.y)), vpol);
             }
         })
         gamma_old = gam;
         alpha_old = alpha;
+        MF_TRACE(it, 4);
+        MF_TRACE(it, 5);
         ++it;
         ++ep;
         publish(P, ep);
+        MF_TRACE(it - 1, 6);
     }
     if (g == 0 && tid == 0) {
         if (status == MF_OK && !fixed && rel > tol) status = MF_ERR_NOT_CONVERGED;
@@ -1296,6 +1339,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_batch_cg(BatchParams B) {
         L.ns = s_rng[0];
         L.kind = D.kind;
         L.site = 40;
+        L.x32 = 0;  // FP64 layouts
         L.gt = D.gt;
         const int vlo = s_rng[1] * 16, vhi = s_rng[2] * 16;
         __syncthreads();  // s_rng read by all before the next system overwrites it
@@ -1437,6 +1481,7 @@ int kernel_config(mf_tiles *t, int *G_out) {
 
 static void fill_layout_args(LayoutArgs &a, const Layout &L) {
     a.kind = L.kind;
+    a.x32 = L.x32 ? 1 : 0;
     a.slabs = L.slabs.p;
     a.head = L.head.p;
     a.cta_slab = L.cta_slab.p;
@@ -1465,7 +1510,21 @@ void base_params(mf_tiles *t, KParams &P) {
     P.nlay = 1;
 }
 
-int launch_spmv(mf_tiles *t, int level, const double *x, double *y, int reps, cudaStream_t s) {
+__global__ void k_to_f32(int n, const double *__restrict__ src, float *__restrict__ dst, size_t npad) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < npad; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = i < (size_t)n ? __double2float_rn(src[i]) : 0.0f;
+}
+
+int launch_to_f32(int n, const double *src, float *dst, size_t npad, cudaStream_t s) {
+    size_t blocks = (npad + 255) / 256;
+    if (blocks > 1184) blocks = 1184;
+    if (blocks < 1) blocks = 1;
+    k_to_f32<<<(unsigned)blocks, 256, 0, s>>>(n, src, dst, npad);
+    MF_CUDA_TRY(cudaGetLastError());
+    return MF_OK;
+}
+
+int launch_spmv(mf_tiles *t, int level, const void *x, double *y, int reps, cudaStream_t s) {
     KParams P;
     base_params(t, P);
     int lay = 0;

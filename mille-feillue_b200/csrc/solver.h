@@ -25,7 +25,7 @@ struct LayoutArgs {
     const uint8_t *head;
     const int *cta_slab, *cta_rb, *cta_dep;
     int kind;  // LAYOUT_*
-    int pad;
+    int x32;   // x staged in FP32: the SpMV input is an FP32 vector
 };
 
 struct DevResult {
@@ -97,7 +97,10 @@ int launch_batch(const BatchParams &B, int grid, cudaStream_t s);
 
 int kernel_config(mf_tiles *t, int *G_out);
 void base_params(mf_tiles *t, KParams &P);
-int launch_spmv(mf_tiles *t, int level, const double *x, double *y, int reps, cudaStream_t s);
+// x: FP64, or FP32 (16*tilen entries) when the level's layout stages FP32 x.
+int launch_spmv(mf_tiles *t, int level, const void *x, double *y, int reps, cudaStream_t s);
+// dst[0..n) = (float)src[0..n), dst[n..npad) = 0.
+int launch_to_f32(int n, const double *src, float *dst, size_t npad, cudaStream_t s);
 int launch_solver(mf_tiles *t, int kind, KParams &P, cudaStream_t s);
 int launch_residual_norms(int n, const double *b, const double *ax, double *out, cudaStream_t s);
 

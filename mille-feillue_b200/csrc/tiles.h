@@ -71,11 +71,13 @@ struct DevArray {
 // tiles in ascending column, entries of the row inside a tile in CSR order.
 constexpr int STAGES = 4;
 constexpr int MAXRUNS = 24;
-constexpr int XSEG_MAX = 112;      // staged x segments per slab (14 KB)
+constexpr int XSEG_MAX = 112;      // staged x segments per slab (14 KB of FP64 x)
+constexpr int XSEG_MAX32 = 224;    // the same 14 KB holding FP32 x
 constexpr int MAXW = 255;          // planes per row block (rowlen is u8)
 constexpr int MAXW_MIXED = 32;     // planes per row block in mixed layouts
 constexpr int SLAB_MAX_DEFAULT = 40960;
-constexpr int RB_PER_SLAB_MAX = 30;  // one per consumer half-warp
+constexpr int RB_PER_SLAB_MAX = 60;  // two per consumer half-warp
+constexpr int RB_PER_SLAB_X64 = 30;  // default for layouts staging FP64 x
 constexpr int ISSUE_REC = 16 + MAXRUNS * 8;
 constexpr uint32_t IDX16_START = 0x8000u, IDX16_LOW = 0x4000u, IDX16_POS = 0x3fffu;
 constexpr uint32_t IDX32_START = 0x80000000u, IDX32_LOW = 0x40000000u, IDX32_POS = 0x3fffffffu;
@@ -150,6 +152,8 @@ struct Layout {
     int slab_max = 0, rb_per_slab = 0;  // stage size / row blocks the planner used
     bool mixed = false;                  // plane precision info present
     int kind = 0;                        // LAYOUT_*
+    bool x32 = false;                    // x staged in FP32: the SpMV input is an FP32 vector
+                                         // (every LAYOUT_LOW layout)
     size_t bytes = 0;
     double alg_bytes = 0;        // algorithmic bytes of one SpMV
     double tile_frac[4] = {0, 0, 0, 0};
@@ -190,6 +194,7 @@ struct mf_tiles {
     mf::DevArray<double> ws;
     mf::DevArray<uint32_t> sync;
     mf::DevArray<double> xpad;  // padded copy of a user x for mf_spmv
+    mf::DevArray<float> x32buf;  // FP32 copy of x for layouts staging FP32 x
     mf::DevArray<uint64_t> trace;  // phase timestamps of the last traced solve
     int trace_iters = 0;
 };

@@ -83,6 +83,8 @@ def main():
             tr = t.trace(args.trace).astype(np.float64)
             tr = tr[(tr[:, 0] > 0) & (tr[:, 6] > 0)]
             names = ["halo wait", "SpMV", "dot d.q", "r update", "dot r.r", "x/d update+publish"]
+            if args.mode != "fp64":  # single-reduction CG
+                names = ["halo wait", "SpMV (w = A r)", "reduction (r.r, w.r)", "p,s,x,r update", "-", "publish"]
             d = np.diff(tr[:, :7], axis=1) / 1e3
             it_us = np.diff(tr[:, 0]) / 1e3
             print("trace over %d iterations (us, median):" % len(tr))
