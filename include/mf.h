@@ -87,7 +87,9 @@ typedef struct {
                                 2-10 us per SpMV; read at encode for
                                 mf_spmv, at solve for the solvers);
                                 reserved[4] = CTAs per system group of
-                                mf_batch_create (0 = 8)                       */
+                                mf_batch_create (0 = 8); reserved[5] = 1:
+                                the single-reduction CG keeps x and r in
+                                global memory instead of tensor memory       */
 } mf_options;
 void mf_options_default(mf_options *opt);
 

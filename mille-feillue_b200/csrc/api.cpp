@@ -444,7 +444,14 @@ static int solve_dev(mf_tiles *t, int kind, const double *b_dev, double *x_dev, 
     cudaEventRecord(e0, 0);
     // mixed layouts run the single-reduction CG unless the classic
     // recurrence is asked for (mf_options.reserved[2] == 1)
-    const int launch_kind = (mixed && opt.reserved[2] != 1) ? 2 : kind;
+    int launch_kind = (mixed && opt.reserved[2] != 1) ? 2 : kind;
+    if (launch_kind == 2 && opt.reserved[5] != 1) {
+        // x and r stay in tensor memory when every CTA's rows fit it
+        int rows_max = 0;
+        for (size_t g = 0; g + 1 < t->h_cta_rb.size(); ++g)
+            rows_max = std::max(rows_max, 16 * (t->h_cta_rb[g + 1] - t->h_cta_rb[g]));
+        if (rows_max <= TMEM_ROWS_MAX) launch_kind = 3;
+    }
     rc = launch_solver(t, launch_kind, P, 0);
     cudaEventRecord(e1, 0);
     cudaError_t ce = cudaEventSynchronize(e1);

@@ -256,7 +256,18 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_slabs(const SlabPlan *__r
                 s_off[j] = off;
                 const int W = rbW[P.rb0 + j];
                 dir[j].off = off;
-                dir[j].W = (uint32_t)W;
+                uint32_t dslot = 0;  // own column segment in the staged x window
+                if (P.mode == SLAB_STAGED) {
+                    const int *sg = segs + P.seg_off;
+                    int lo = 0, hi = P.nseg;
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (sg[mid] < P.rb0 + j) lo = mid + 1;
+                        else hi = mid;
+                    }
+                    if (lo < P.nseg && sg[lo] == P.rb0 + j) dslot = (uint32_t)lo + 1u;
+                }
+                dir[j].W = (uint32_t)W | (dslot << 16);
                 off += rb_block_bytes(W, mixed, gather, rbvb[P.rb0 + j]);
             }
             dir[P.nrb].off = off;

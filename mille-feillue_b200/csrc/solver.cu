@@ -103,7 +103,7 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
                                            const XT *__restrict__ xg) {
     const RbDir d = reinterpret_cast<const RbDir *>(st + slab_rbdir_off())[j];
     const uint8_t *blk = st + d.off;
-    const int W = (int)d.W;
+    const int W = (int)(d.W & 0xffffu);
     const int len = blk[r];
     const bool gather = h.mode == SLAB_GATHER;
     double acc = 0.0, sum = 0.0;
@@ -342,7 +342,7 @@ __device__ double global_row(const GTiles &P, int rb, int r, const double *__res
 // runs and the slab of the next slab with 1D bulk copies. The NWARPS
 // consumer warps wait for a stage's full barrier, compute their row blocks
 // (one half-warp per row block, one lane per row) and release the stage.
-// For every row < rowA: v = epi.pre(row) is loaded before the row's
+// For every row < rowA: v = epi.pre(row) (any type) is loaded before the row's
 // entries, then epi(row, acc, v) runs with the row sum. Returns false on
 // abort.
 template <bool MIXED, class Epi, int GB = 1>
@@ -415,7 +415,8 @@ __device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const void *xv,
             if (h.mode == SLAB_OVERSIZE) {
                 if (w == 0 && half == 0) {
                     const int row = h.rb0 * 16 + r;
-                    const double pv = row < L.gt.rowA ? epi.pre(row) : 0.0;
+                    using PV = decltype(epi.pre(0));
+                    const PV pv = row < L.gt.rowA ? epi.pre(row) : PV(0);
                     const double acc = global_row(L.gt, h.rb0, r, static_cast<const double *>(xv));
                     if (row < L.gt.rowA) epi(row, acc, pv);
                 }
@@ -426,8 +427,23 @@ __device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const void *xv,
                 for (int j = j0; j < h.nrb; j += 2 * NWARPS) {
                     const int row = (h.rb0 + j) * 16 + r;
                     const bool live = row < L.gt.rowA;
-                    const double pv = live ? epi.pre(row) : 0.0;
+                    // the pre-loaded value keeps its own type until the epilogue:
+                    // a conversion here would wait for the load before the
+                    // row's arithmetic instead of overlapping it
                     const double *xsg = reinterpret_cast<const double *>(st + slab_area);
+                    using PV = decltype(epi.pre(0));
+                    PV pv;
+                    if constexpr (Epi::kUsesX) {
+                        // the row's own x value from the stage (rows this CTA
+                        // wrote just before load slowly from global memory);
+                        // an FP64 value is not taken from an FP32 stage
+                        const uint32_t ds = reinterpret_cast<const RbDir *>(st + slab_rbdir_off())[j].W >> 16;
+                        if (ds == 0u || !live || (L.x32 && sizeof(PV) == 8)) pv = live ? epi.pre(row) : PV(0);
+                        else if (L.x32) pv = PV(reinterpret_cast<const float *>(xsg)[(ds - 1u) * 16u + r]);
+                        else pv = PV(xsg[(ds - 1u) * 16u + r]);
+                    } else {
+                        pv = live ? epi.pre(row) : PV(0);
+                    }
                     const double *xg = static_cast<const double *>(xv);
                     double acc;
                     if (!MIXED || L.kind == LAYOUT_FP64) acc = slab_row<LAYOUT_FP64, GB>(st, h, j, r, xsg, xg);
@@ -627,6 +643,7 @@ __device__ void kernel_setup(const KParams &P, Smem &S, int nlay) {
 
 // ------------------------------------------------------------------ SpMV
 struct EpiStore {
+    static constexpr bool kUsesX = false;
     double *y;
     __device__ double pre(int) const { return 0.0; }
     __device__ void operator()(int row, double acc, double) const { y[row] = acc; }
@@ -648,6 +665,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_spmv(KParams P, const void *x, 
 // The solver's vectors are read and written with an L2 evict_last policy
 // so they stay resident in L2 while the matrix streams with evict_first.
 struct EpiResidual {  // r = b - A x, rr += r*r
+    static constexpr bool kUsesX = false;
     const double *b;
     double *r;
     double rr;
@@ -660,6 +678,7 @@ struct EpiResidual {  // r = b - A x, rr += r*r
     }
 };
 struct EpiResidual32 {  // r = b - A x and its FP32 copy, rr += r*r
+    static constexpr bool kUsesX = false;
     const double *b;
     double *r;
     float *r32;
@@ -674,6 +693,7 @@ struct EpiResidual32 {  // r = b - A x and its FP32 copy, rr += r*r
     }
 };
 struct EpiQ {  // q = A d, dq += d*q
+    static constexpr bool kUsesX = true;  // d is the SpMV input
     const double *d;
     double *q;
     double dq;
@@ -891,6 +911,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cg(KParams P) {
 //   w = A r;  gamma = r.r;  delta = w.r;
 //   beta = gamma / gamma_old;  alpha = gamma / (delta - beta gamma / alpha_old)
 struct EpiW {  // w = A r (FP32), gamma += r*r, delta += w*r
+    static constexpr bool kUsesX = false;
     const double *r;
     float *w;
     double g, dl;
@@ -925,7 +946,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cgcg(KParams P) {
     EpiResidual32 er{b, r, r32, 0.0, vpol};
     if (!cta_spmv<false>(P, lay64, x, S, dyn, pp, er)) return;
     double bbp = 0.0;
-    MF_PAIRS(4, vlo, vhi, {
+    MF_PAIRS(2, vlo, vhi, {
         double2 bv[_vb];
 #pragma unroll
         MF_FOR_VB if (MF_LIVE(u, vhi)) bv[u] = ld2_hint(b + 2 * MF_PI(u), vpol);
@@ -1012,7 +1033,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cgcg(KParams P) {
             status = MF_ERR_BREAKDOWN;
             break;
         }
-        MF_PAIRS(2, vlo, vhi, {
+        MF_PAIRS(4, vlo, vhi, {
             double2 rv[_vb], xv[_vb];
             float2 pw[_vb], sw[_vb], ww[_vb];
 #pragma unroll
@@ -1065,8 +1086,358 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cgcg(KParams P) {
     }
 }
 
+// ------------------------------------- CG, single reduction, x and r in TMEM
+// The recurrence of k_cgcg with x and r of the CTA's own rows resident in
+// tensor memory across iterations (16 bytes a row, at most 16384 rows a CTA),
+// so the fused vector pass reads and writes only the FP32 vectors p, s, w and
+// the FP32 copy r32 of r (the SpMV input and the halo) in global memory.
+// Own rows come in blocks of 512: in block k, rows 4L .. 4L+3 belong to TMEM
+// lane L (thread L % 32 of warp L / 32 of a warpgroup), columns 16k + 4j ..
+// +3 holding (x low, x high, r low, r high) of row 4L + j; warp w serves the
+// blocks k = w/4, w/4 + 4, ... One 16-column TMEM load and 16-byte loads of
+// p, s, w cover a thread's four rows. gamma = r.r is summed where r is
+// produced, delta = w.r32 in the SpMV epilogue (w itself comes from the FP32
+// operator applied to r32). x goes to global memory for the FP64
+// true-residual replacement and at the end; r also while the FP64 layout is
+// active.
+struct EpiW32 {  // w = A r (FP32), delta += w * r (r in FP32)
+    // r(row) is the SpMV input: taken from the x stage when the row block's
+    // own segment is staged there, else loaded
+    static constexpr bool kUsesX = true;
+    const float *r32;
+    float *w;
+    double dl;
+    uint64_t pol;
+    __device__ float pre(int row) const { return ldf_hint(r32 + row, pol); }
+    __device__ void operator()(int row, double acc, float rv) {
+        const float wf = __double2float_rn(acc);
+        stf_hint(w + row, wf, pol);
+        dl += (double)wf * (double)rv;
+    }
+};
+
+constexpr int TM_CB = 2;  // 512-row blocks in flight per warp
+
+struct TmemRows {
+    uint32_t base;  // TMEM address of lane 32*q, column 0
+    int q, k0, nblk, nrows, vlo;
+    __device__ uint32_t addr(int k) const { return base + 16u * (uint32_t)k; }
+    // first of the thread's four rows in block k (own-row index)
+    __device__ int row_of(int k) const { return k * 512 + 4 * (32 * q + (int)(threadIdx.x & 31)); }
+};
+// Built inside each pass from the TMEM base (shared memory) and the CTA's
+// row range, so that none of it stays live across the SpMV, which needs
+// every register it can get.
+__device__ __forceinline__ TmemRows tm_rows(const KParams &P, const volatile uint32_t *s_tmem) {
+    const int g = blockIdx.x, w = threadIdx.x >> 5;
+    TmemRows T;
+    T.vlo = P.lay[0].cta_rb[g] * 16;
+    T.nrows = P.lay[0].cta_rb[g + 1] * 16 - T.vlo;
+    T.q = w & 3;
+    T.k0 = w >> 2;
+    T.nblk = (T.nrows + 511) / 512;
+    T.base = *s_tmem + ((uint32_t)(32 * T.q) << 16);
+    return T;
+}
+
+__device__ __forceinline__ double tm_x(const uint32_t (&t)[16], int j) {
+    return __hiloint2double((int)t[4 * j + 1], (int)t[4 * j]);
+}
+__device__ __forceinline__ double tm_r(const uint32_t (&t)[16], int j) {
+    return __hiloint2double((int)t[4 * j + 3], (int)t[4 * j + 2]);
+}
+__device__ __forceinline__ void tm_set(uint32_t (&t)[16], int j, double x, double r) {
+    t[4 * j] = (uint32_t)__double2loint(x);
+    t[4 * j + 1] = (uint32_t)__double2hiint(x);
+    t[4 * j + 2] = (uint32_t)__double2loint(r);
+    t[4 * j + 3] = (uint32_t)__double2hiint(r);
+}
+
+// x (when xg) and r of the own rows from global memory into TMEM; returns the
+// thread's share of r.r. xg == nullptr keeps x in TMEM. Own rows are a
+// multiple of 16, so a thread's four rows are all live or all past the end.
+__device__ double tm_load(const TmemRows &T, const double *xg, const double *rg, uint64_t pol) {
+    double rr = 0.0;
+    for (int k = T.k0; k < T.nblk; k += 4) {
+        const int i = T.row_of(k);
+        const bool live = i < T.nrows;
+        uint32_t t[16];
+        __syncwarp();  // tcgen05 ops are warp-collective
+        if (!xg) tmem_ld16(T.addr(k), t);
+        double2 r01 = make_double2(0.0, 0.0), r23 = r01, x01 = r01, x23 = r01;
+        if (live) {
+            r01 = ld2_hint(rg + T.vlo + i, pol);
+            r23 = ld2_hint(rg + T.vlo + i + 2, pol);
+            if (xg) {
+                x01 = ld2_hint(xg + T.vlo + i, pol);
+                x23 = ld2_hint(xg + T.vlo + i + 2, pol);
+            }
+        }
+        if (!xg) {
+            tmem_wait_ld16(t);
+            x01 = make_double2(tm_x(t, 0), tm_x(t, 1));
+            x23 = make_double2(tm_x(t, 2), tm_x(t, 3));
+        }
+        tm_set(t, 0, x01.x, r01.x);
+        tm_set(t, 1, x01.y, r01.y);
+        tm_set(t, 2, x23.x, r23.x);
+        tm_set(t, 3, x23.y, r23.y);
+        tmem_st16_wait(T.addr(k), t);
+        rr += r01.x * r01.x + r01.y * r01.y + r23.x * r23.x + r23.y * r23.y;
+    }
+    return rr;
+}
+
+// x (and r when rg) of the own rows from TMEM to global memory.
+__device__ void tm_store(const TmemRows &T, double *xg, double *rg, uint64_t pol) {
+    for (int k = T.k0; k < T.nblk; k += 4) {
+        uint32_t t[16];
+        __syncwarp();
+        tmem_ld16(T.addr(k), t);
+        tmem_wait_ld16(t);
+        const int i = T.row_of(k);
+        if (i < T.nrows) {
+            st2_hint(xg + T.vlo + i, make_double2(tm_x(t, 0), tm_x(t, 1)), pol);
+            st2_hint(xg + T.vlo + i + 2, make_double2(tm_x(t, 2), tm_x(t, 3)), pol);
+            if (rg) {
+                st2_hint(rg + T.vlo + i, make_double2(tm_r(t, 0), tm_r(t, 1)), pol);
+                st2_hint(rg + T.vlo + i + 2, make_double2(tm_r(t, 2), tm_r(t, 3)), pol);
+            }
+        }
+    }
+}
+
+// The fused vector pass of k_cgcg on TMEM-resident x, r:
+//   p = r + beta p;  s = w + beta s;  x += alpha p;  r -= alpha s;  r32 = r
+// (p, s rounded to FP32 before use, as in k_cgcg). r also goes to global
+// memory when rg. Returns the thread's share of the new r.r.
+__device__ double tm_update(const TmemRows &T, double alpha, double beta, float *pv, float *sv, const float *wv,
+                            float *r32, double *rg, uint64_t pol) {
+    double rr = 0.0;
+    for (int k = T.k0; k < T.nblk; k += 4 * TM_CB) {
+        uint32_t t[TM_CB][16];
+        float4 pf[TM_CB], sf[TM_CB], wf[TM_CB];
+        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < TM_CB; ++u) {
+            const int kk = k + 4 * u;
+            if (kk < T.nblk) {
+                tmem_ld16(T.addr(kk), t[u]);
+                const int i = T.row_of(kk);
+                if (i < T.nrows) {
+                    pf[u] = ldf4_hint(pv + T.vlo + i, pol);
+                    sf[u] = ldf4_hint(sv + T.vlo + i, pol);
+                    wf[u] = ldf4_hint(wv + T.vlo + i, pol);
+                } else {
+                    pf[u] = sf[u] = wf[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < TM_CB; ++u) {
+            const int kk = k + 4 * u;
+            __syncwarp();
+            if (kk < T.nblk) {
+                tmem_wait_ld16(t[u]);
+                const float pin[4] = {pf[u].x, pf[u].y, pf[u].z, pf[u].w};
+                const float sin_[4] = {sf[u].x, sf[u].y, sf[u].z, sf[u].w};
+                const float win[4] = {wf[u].x, wf[u].y, wf[u].z, wf[u].w};
+                float pn[4], sn[4], rn[4];
+                double rsq = 0.0;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    double xv = tm_x(t[u], j), rv = tm_r(t[u], j);
+                    pn[j] = __double2float_rn(rv + beta * (double)pin[j]);
+                    sn[j] = __double2float_rn((double)win[j] + beta * (double)sin_[j]);
+                    xv = xv + alpha * (double)pn[j];
+                    rv = rv - alpha * (double)sn[j];
+                    tm_set(t[u], j, xv, rv);
+                    rn[j] = __double2float_rn(rv);
+                    rsq += rv * rv;
+                }
+                tmem_st16_wait(T.addr(kk), t[u]);
+                const int i = T.row_of(kk);
+                if (i < T.nrows) {
+                    const int row = T.vlo + i;
+                    stf4_hint(pv + row, make_float4(pn[0], pn[1], pn[2], pn[3]), pol);
+                    stf4_hint(sv + row, make_float4(sn[0], sn[1], sn[2], sn[3]), pol);
+                    stf4_hint(r32 + row, make_float4(rn[0], rn[1], rn[2], rn[3]), pol);
+                    if (rg) {
+                        st2_hint(rg + row, make_double2(tm_r(t[u], 0), tm_r(t[u], 1)), pol);
+                        st2_hint(rg + row + 2, make_double2(tm_r(t[u], 2), tm_r(t[u], 3)), pol);
+                    }
+                    rr += rsq;
+                }
+            }
+        }
+    }
+    return rr;
+}
+
+__device__ __forceinline__ void cgcg_tm_body(const KParams &P, Smem &S, uint8_t *dyn, const volatile uint32_t *s_tmem,
+                                             volatile double *s_gpart) {
+    const int g = blockIdx.x, tid = threadIdx.x;
+    Pipe pp;
+    uint32_t phase = 0;
+    const uint64_t vpol = policy_evict_last();
+    const int lay64 = 0;
+    int lay = P.start_layout;
+    const int rb_lo = P.lay[0].cta_rb[g], rb_hi = P.lay[0].cta_rb[g + 1];
+    const int vlo = rb_lo * 16, vhi = rb_hi * 16;
+    double *x = P.x, *r = P.r;
+    float *pv32 = reinterpret_cast<float *>(P.d), *sv32 = reinterpret_cast<float *>(P.q),
+          *wv32 = reinterpret_cast<float *>(P.s);
+    float *r32 = reinterpret_cast<float *>(P.t);
+    const double *b = P.b;
+    // r = b - A x0 (global r and r32); p = s = 0; x, r into TMEM
+    EpiResidual32 er{b, r, r32, 0.0, vpol};
+    if (!cta_spmv<false>(P, lay64, x, S, dyn, pp, er)) return;
+    double bbp = 0.0;
+    MF_PAIRS(2, vlo, vhi, {
+        double2 bv[_vb];
+#pragma unroll
+        MF_FOR_VB if (MF_LIVE(u, vhi)) bv[u] = ld2_hint(b + 2 * MF_PI(u), vpol);
+#pragma unroll
+        MF_FOR_VB if (MF_LIVE(u, vhi)) {
+            bbp += bv[u].x * bv[u].x + bv[u].y * bv[u].y;
+            stf2_hint(pv32 + 2 * MF_PI(u), make_float2(0.f, 0.f), vpol);
+            stf2_hint(sv32 + 2 * MF_PI(u), make_float2(0.f, 0.f), vpol);
+        }
+    })
+    // this thread's share of r.r, carried to the next reduction in shared
+    // memory (not in a register across the SpMV)
+    s_gpart[tid] = tm_load(tm_rows(P, s_tmem), x, r, vpol);
+    double v1[1] = {bbp}, o1[1];
+    if (!grid_sum<1>(P, S, v1, o1, phase)) return;
+    const double bb = o1[0];
+    const double bnorm = sqrt(bb);
+    const double tol = P.tol;
+    uint32_t ep = 1;
+    publish(P, ep);
+    int it = 0, status = MF_OK, repl = 0, switches = 0, fellback = 0;
+    int it_lay[KMAX_LAYOUTS] = {0, 0, 0, 0};
+    double gamma_old = 0.0, alpha_old = 1.0, rel = 1.0, rr_best = 1e300, gam = 0.0;
+    bool first = true, pending = false;
+    const bool fixed = P.fixed_iterations > 0;
+    const int maxit = fixed ? P.fixed_iterations : P.maxiter;
+    while (true) {
+        const bool repl_now = pending || (P.replace_every > 0 && it > 0 && it % P.replace_every == 0);
+        if (repl_now) {
+            // x to global memory for the FP64 SpMV, then r = b - A x into TMEM
+            tm_store(tm_rows(P, s_tmem), x, nullptr, vpol);
+            ++ep;
+            publish(P, ep);
+            if (!wait_deps(P, S, lay64, ep)) return;
+            EpiResidual32 e2{b, r, r32, 0.0, vpol};
+            if (!cta_spmv<false>(P, lay64, x, S, dyn, pp, e2)) return;
+            const double gl = tm_load(tm_rows(P, s_tmem), nullptr, r, vpol);
+            s_gpart[tid] = gl;
+            double a1[1] = {gl}, c1[1];
+            if (!grid_sum<1>(P, S, a1, c1, phase)) return;
+            ++repl;
+            ++ep;
+            publish(P, ep);
+            const double relt = bnorm > 0 ? sqrt(c1[0]) / bnorm : 0.0;
+            if (pending) {
+                pending = false;
+                rel = relt;
+                if (rel <= tol) break;
+            }
+            if (lay != lay64) {
+                if (c1[0] < rr_best) rr_best = c1[0];
+                if (!(c1[0] <= 1e4 * rr_best)) {
+                    lay = lay64;
+                    fellback = 1;
+                }
+                while (lay != lay64 && lay < P.nlay - 1 && relt < P.level_rel[lay]) {
+                    ++lay;
+                    ++switches;
+                }
+            }
+        }
+        if (it >= maxit) break;
+        MF_TRACE(it, 0);
+        if (!wait_deps(P, S, lay, ep)) return;
+        MF_TRACE(it, 1);
+        ++it_lay[lay];
+        EpiW32 ew{r32, wv32, 0.0, vpol};
+        bool ok;
+        if (lay != lay64) ok = cta_spmv<true>(P, lay, P.lay[lay].x32 ? (const void *)r32 : r, S, dyn, pp, ew);
+        else ok = cta_spmv<false>(P, lay64, r, S, dyn, pp, ew);
+        if (!ok) return;
+        MF_TRACE(it, 2);
+        double a2[2] = {s_gpart[tid], ew.dl}, c2[2];
+        if (!grid_sum<2>(P, S, a2, c2, phase)) return;
+        MF_TRACE(it, 3);
+        gam = c2[0];
+        const double delta = c2[1];
+        rel = bnorm > 0 ? sqrt(gam) / bnorm : 0.0;
+        if (!fixed && rel <= tol) {
+            pending = true;  // confirm with the FP64 true residual
+            continue;
+        }
+        double alpha, beta;
+        if (first) {
+            beta = 0.0;
+            alpha = gam / delta;
+            first = false;
+        } else {
+            beta = gam / gamma_old;
+            alpha = gam / (delta - beta * gam / alpha_old);
+        }
+        if (!isfinite(alpha) || !isfinite(beta) || alpha == 0.0) {
+            status = MF_ERR_BREAKDOWN;
+            break;
+        }
+        s_gpart[tid] = tm_update(tm_rows(P, s_tmem), alpha, beta, pv32, sv32, wv32, r32, lay == lay64 ? r : nullptr,
+                                 vpol);
+        gamma_old = gam;
+        alpha_old = alpha;
+        MF_TRACE(it, 4);
+        MF_TRACE(it, 5);
+        ++it;
+        ++ep;
+        publish(P, ep);
+        MF_TRACE(it - 1, 6);
+    }
+    tm_store(tm_rows(P, s_tmem), x, r, vpol);
+    if (g == 0 && tid == 0) {
+        if (status == MF_OK && !fixed && rel > tol) status = MF_ERR_NOT_CONVERGED;
+        P.res->iterations = it;
+        P.res->status = status;
+        P.res->replacements = repl;
+        P.res->level_switches = switches;
+        P.res->rr = bnorm > 0 ? rel * rel * bb : gam;
+        P.res->bb = bb;
+        P.res->final_layout = lay;
+        for (int l = 0; l < KMAX_LAYOUTS; ++l) P.res->it_layout[l] = it_lay[l];
+        P.res->pad = fellback;
+    }
+}
+
+// One CTA per SM holds all 512 TMEM columns for the whole solve; every exit
+// of the body (including aborts) comes back here to release them.
+__global__ void __launch_bounds__(NTHREADS, 1) k_cgcg_tm(KParams P) {
+    extern __shared__ __align__(128) uint8_t dyn[];
+    __shared__ Smem S;
+    __shared__ uint32_t s_tmem;
+    __shared__ double s_gpart[NTHREADS];
+    kernel_setup(P, S, P.nlay);
+    const int w = threadIdx.x >> 5;
+    if (w == 0) tmem_alloc512(&s_tmem);
+    tcgen05_fence_before_sync();
+    __syncthreads();
+    tcgen05_fence_after_sync();
+    cgcg_tm_body(P, S, dyn, &s_tmem, s_gpart);
+    tcgen05_fence_before_sync();
+    __syncthreads();
+    tcgen05_fence_after_sync();
+    if (w == 0) tmem_dealloc512(s_tmem);
+}
+
 // -------------------------------------------------------------- BiCGSTAB
 struct EpiDot {  // y = A p, dot += z*y
+    static constexpr bool kUsesX = false;
     const double *z;
     double *y;
     double dot;
@@ -1078,6 +1449,7 @@ struct EpiDot {  // y = A p, dot += z*y
     }
 };
 struct EpiDot2 {  // t = A s, ts += t*s, tt += t*t
+    static constexpr bool kUsesX = true;  // s is the SpMV input
     const double *s;
     double *t;
     double ts, tt;
@@ -1461,7 +1833,7 @@ int kernel_config(mf_tiles *t, int *G_out) {
     }
     const void *kerns[] = {(const void *)k_cg<false>, (const void *)k_cg<true>, (const void *)k_bicgstab,
                            (const void *)k_spmv<false>, (const void *)k_spmv<true>, (const void *)k_cgcg,
-                           (const void *)k_batch_cg};
+                           (const void *)k_batch_cg, (const void *)k_cgcg_tm};
     int occ_min = 1 << 30;
     for (const void *k : kerns) {
         MF_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
@@ -1550,6 +1922,7 @@ int launch_solver(mf_tiles *t, int kind, KParams &P, cudaStream_t s) {
     void *args[] = {&P};
     const void *k = kind == 0   ? (P.nlay > 1 ? (const void *)k_cg<true> : (const void *)k_cg<false>)
                     : kind == 2 ? (const void *)k_cgcg
+                    : kind == 3 ? (const void *)k_cgcg_tm
                                 : (const void *)k_bicgstab;
     MF_CUDA_TRY(cudaLaunchCooperativeKernel(k, dim3(t->G), dim3(NTHREADS), args, dyn, s));
     return MF_OK;

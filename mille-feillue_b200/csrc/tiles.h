@@ -107,7 +107,8 @@ struct XRun {
 
 struct RbDir {
     uint32_t off;  // byte offset of the row-block block from the slab start
-    uint32_t W;    // planes
+    uint32_t W;    // planes (low 16 bits); high 16 bits: 1 + the x-stage slot of
+                   // the row block's own column segment (0: not staged)
 };
 
 // Layout kinds: every tile FP64 / every tile below FP64 / both.

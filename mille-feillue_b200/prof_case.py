@@ -32,6 +32,7 @@ def main():
     ap.add_argument("--time", action="store_true", help="print the CUDA-event time of the launches")
     ap.add_argument("--trace", type=int, default=0, help="trace the phases of the first N CG iterations")
     ap.add_argument("--prefetch", action="store_true", help="L2 prefetch of slabs ahead of the copy ring")
+    ap.add_argument("--no-tmem", action="store_true", help="single-reduction CG with x, r in global memory")
     args = ap.parse_args()
     import torch
 
@@ -77,6 +78,8 @@ def main():
         o.reserved[1] = args.trace
     if args.prefetch:
         o.reserved[3] = 1
+    if args.no_tmem:
+        o.reserved[5] = 1
     if args.kernel == "cg":
         res = t.solve_cg_dev(b.data_ptr(), x.data_ptr(), 1e-10, 40000, o)
         if args.trace > 0:
