@@ -280,6 +280,14 @@ def gpu_arm(args, world, rank, local, dist):
         return gbs
 
     gbs = roof(res, kms)
+    # DRAM bytes per CG iteration (read + write) measured with ncu on a
+    # 20-iteration launch of the same matrix (profiles/k_cg_k_cgcg_tm_varpoisson128.md),
+    # scaled by the iterations of the timed solve (plus the initial and the
+    # replacement FP64 SpMVs at their algorithmic bytes)
+    dram_per_iter = {"mixed": 98.6e6, "fp64": 179.9e6}[headline]
+    traffic = res["iterations"] * dram_per_iter + (1 + res["replacements"]) * spmv_bytes
+    kname = ("k_cgcg_tm (mixed single-reduction CG, x and r in tensor memory)" if headline == "mixed"
+             else "k_cg<0> (FP64 CG)")
     out = None
     if rank == 0:
         out = {
@@ -302,9 +310,9 @@ def gpu_arm(args, world, rank, local, dist):
                      "roofline_gbs": roof(res64, k64), "roofline_frac": roof(res64, k64) / peak},
             "speedup_mixed_vs_fp64": ms64 / msmx,
             "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
-                         "traffic": None, "peak_kind": peak_kind,
-                         "kernel": "k_cg (persistent solve); bytes = every SpMV's algorithmic bytes "
-                                   "+ 56 n per iteration"},
+                         "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": kname + "; one launch = one solve; algorithmic bytes = every SpMV's "
+                                   "algorithmic bytes + 56 n per iteration"},
             "spmv": {"fp64": {"ms": spmv_ms, "alg_bytes": spmv_bytes, "gbs": spmv_bytes / spmv_ms / 1e6,
                               "frac": spmv_bytes / spmv_ms / 1e6 / peak, "gflops": 2.0 * len(v) / spmv_ms / 1e6},
                      "mixed_level0": {"ms": spmv_mx_ms, "alg_bytes": spmv_mx_bytes,
