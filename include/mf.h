@@ -89,7 +89,9 @@ typedef struct {
                                 reserved[4] = CTAs per system group of
                                 mf_batch_create (0 = 8); reserved[5] = 1:
                                 the single-reduction CG keeps x and r in
-                                global memory instead of tensor memory       */
+                                global memory instead of tensor memory;
+                                reserved[6] = N > 0: reference iteration
+                                count for the learned selector's fallback   */
 } mf_options;
 void mf_options_default(mf_options *opt);
 
@@ -115,7 +117,10 @@ typedef struct {
     int fell_back_fp64;      /* 1 if a low-precision level let the true
                                 residual grow and the solve finished on the
                                 FP64 layout                                   */
-    int reserved2;
+    int selector_fallback;   /* MF_MODE_MIXED_MLP: 1 if the learned selector's
+                                solve missed the tolerance, fell back to FP64
+                                or ran > 10% over mf_options.reserved[6]
+                                iterations, and the magnitude rule solved it  */
 } mf_result;
 
 /* ---- opaque handles --------------------------------------------------- */
@@ -262,6 +267,33 @@ int mf_trace(const mf_tiles *t, unsigned long long *out, int max_iters);
 /* ||b - A x|| / ||b|| with the FP64 tiled SpMV (device vectors).             */
 int mf_true_residual(mf_tiles *t, const double *b_dev, const double *x_dev,
                      double *rel);
+
+/* ---- learned precision selector (MF_MODE_MIXED_MLP) --------------------- */
+/* An MLP 6 -> 64 -> 64 -> 4 (ReLU) over per-tile features; its classes are
+ * the tile precisions MF_PREC_*. Features: f0 = log10 max|a_ij|/sqrt(a_ii
+ * a_jj) over the tile, f1 = log10 max|a|/min|a| over the tile, f2 = log10
+ * of the matrix nnz, f3 = diagonal tile, f4 = log10 max|a|/min|a| over the
+ * matrix, f5 = log10 of the relative residual at which the precision is
+ * used. Weights (MF_MLP_WEIGHTS floats): W1[64][6], b1[64], W2[64][64],
+ * b2[64], W3[4][64], b3[4]. Inference rounds them to BF16 and accumulates in
+ * FP32. The reference has no counterpart (it stores every tile in FP64).   */
+#define MF_MLP_WEIGHTS 4868
+int mf_mlp_set_weights(const float *w_host);  /* process-wide; NULL clears   */
+int mf_mlp_get_weights(float *w_host);        /* MF_ERR_ARG when none set    */
+/* Features f0..f4 of every tile, feat[6*t + k] (f5 = 0).                     */
+int mf_tiles_features(const mf_tiles *t, float *feat_host);
+/* Selector classes at nlev residual levels: prec[l*tilenum + t].            */
+int mf_tiles_select_mlp(const mf_tiles *t, int nlev, const double *rel_res,
+                        unsigned char *prec_host);
+/* The training kernels (device pointers): logits[4n] of n samples x[6n];
+ * gradient g of the mean softmax cross-entropy (*loss on the host); `steps`
+ * Adam steps, step i on the samples [i*batch mod n, +batch).                */
+int mf_mlp_forward_dev(const float *w, const float *x, int n, int bf16,
+                       float *logits);
+int mf_mlp_grad_dev(const float *w, const float *x, const int *labels, int n,
+                    float *g, float *loss);
+int mf_mlp_train_dev(float *w, const float *x, const int *labels, int n,
+                     int steps, int batch, float lr, float *loss);
 
 /* ---- batched solve of many independent systems ------------------------- */
 /* Encodes `count` square systems (host CSR) for one persistent launch. The

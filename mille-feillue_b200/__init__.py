@@ -60,7 +60,7 @@ class MfResult(C.Structure):
         ("rel_residual_true", _d), ("rel_residual_rec", _d), ("time_ms", _d), ("spmv_bytes", _d),
         ("spmv_bytes_fp64", _d), ("tile_frac", _d * 4), ("error_site", _i), ("iters_fp64", _i),
         ("iters_level", _i * 3), ("spmv_bytes_level", _d * 3), ("total_bytes", _d),
-        ("fell_back_fp64", _i), ("reserved2", _i),
+        ("fell_back_fp64", _i), ("selector_fallback", _i),
     ]
 
     def as_dict(self):
@@ -72,6 +72,7 @@ class MfResult(C.Structure):
             "tile_frac": list(self.tile_frac), "error_site": self.error_site, "iters_fp64": self.iters_fp64,
             "iters_level": list(self.iters_level), "spmv_bytes_level": list(self.spmv_bytes_level),
             "total_bytes": self.total_bytes, "fell_back_fp64": self.fell_back_fp64,
+            "selector_fallback": self.selector_fallback,
         }
 
 
@@ -110,8 +111,11 @@ EXPORTED = [
     "mf_solve_bicgstab_dev", "mf_true_residual", "cg_solve_inc", "bicgstab", "mf_version", "mf_last_error",
     "mf_spmv_level", "mf_spmv_bench_level", "mf_trace", "mf_batch_create", "mf_batch_solve_cg_dev",
     "mf_batch_solve_cg_each_dev", "mf_batch_results", "mf_batch_info", "mf_batch_free",
-    "mf_solve_cg_dev_noalloc",
+    "mf_solve_cg_dev_noalloc", "mf_mlp_set_weights", "mf_mlp_get_weights", "mf_tiles_features",
+    "mf_tiles_select_mlp", "mf_mlp_forward_dev", "mf_mlp_grad_dev", "mf_mlp_train_dev",
 ]
+MLP_WEIGHTS = 4868
+MLP_WEIGHTS_PATH = os.path.join(_HERE, "mlp_weights.bin")
 
 _lib = None
 
@@ -163,6 +167,13 @@ def lib():
               "mf_solve_cg_dev_noalloc"):
         getattr(L, f).argtypes = [_p, _p, _p, _d, _i, C.POINTER(MfOptions), C.POINTER(MfResult)]
     L.mf_true_residual.argtypes = [_p, _p, _p, C.POINTER(_d)]
+    L.mf_mlp_set_weights.argtypes = [_p]
+    L.mf_mlp_get_weights.argtypes = [_p]
+    L.mf_tiles_features.argtypes = [_p, _p]
+    L.mf_tiles_select_mlp.argtypes = [_p, _i, _p, _p]
+    L.mf_mlp_forward_dev.argtypes = [_p, _p, _i, _i, _p]
+    L.mf_mlp_grad_dev.argtypes = [_p, _p, _p, _i, _p, C.POINTER(C.c_float)]
+    L.mf_mlp_train_dev.argtypes = [_p, _p, _p, _i, _i, _i, C.c_float, C.POINTER(C.c_float)]
     L.mf_trace.argtypes = [_p, _p, _i]
     L.mf_batch_create.argtypes = [_i, _p, C.POINTER(MfOptions), _i, C.POINTER(_p)]
     L.mf_batch_solve_cg_dev.argtypes = [_p, _p, _p, _d, _i, C.POINTER(_d)]
@@ -192,6 +203,24 @@ def _check(rc, what):
 
 def _ptr(a):
     return a.ctypes.data_as(_p)
+
+
+def set_mlp_weights(w):
+    """Process-wide selector weights (MLP_WEIGHTS floats); None clears them."""
+    if w is None:
+        _check(lib().mf_mlp_set_weights(None), "mf_mlp_set_weights")
+        return
+    a = np.ascontiguousarray(w, np.float32)
+    if a.size != MLP_WEIGHTS:
+        raise ValueError(f"selector weights need {MLP_WEIGHTS} floats, got {a.size}")
+    _check(lib().mf_mlp_set_weights(_ptr(a)), "mf_mlp_set_weights")
+
+
+def load_mlp_weights(path=None):
+    """Loads selector weights (raw little-endian float32) and sets them."""
+    w = np.fromfile(path or MLP_WEIGHTS_PATH, dtype="<f4")
+    set_mlp_weights(w)
+    return w
 
 
 def options(**kw):
@@ -321,8 +350,25 @@ class Tiles:
             self._keep = (np.ascontiguousarray(rp, np.int32), np.ascontiguousarray(ci, np.int32),
                           np.ascontiguousarray(v, np.float64))
             c = MfCsr(n, ncols, int(self._keep[0][n]), _ptr(self._keep[0]), _ptr(self._keep[1]), _ptr(self._keep[2]))
+        if o.precision_mode == MODE_MIXED_MLP and lib().mf_mlp_get_weights(None) != MF_OK:
+            load_mlp_weights()  # the packaged selector, unless the caller set one
         _check(lib().mf_encode(C.byref(c), C.byref(o), C.byref(self.h)), "mf_encode")
         self.opts = o
+
+    def features(self):
+        """Selector features f0..f5 of every tile, shape (tilenum, 6)."""
+        n = self.info()["tilenum"]
+        f = np.zeros((max(n, 1), 6), np.float32)
+        _check(lib().mf_tiles_features(self.h, _ptr(f)), "mf_tiles_features")
+        return f[:n]
+
+    def select_mlp(self, rel_res):
+        """Learned selector classes at the given residual levels, (levels, tilenum)."""
+        n = self.info()["tilenum"]
+        r = np.ascontiguousarray(rel_res, np.float64)
+        p = np.zeros((len(r), max(n, 1)), np.uint8)
+        _check(lib().mf_tiles_select_mlp(self.h, len(r), _ptr(r), _ptr(p)), "mf_tiles_select_mlp")
+        return p[:, :n]
 
     def info(self):
         i = MfTileInfo()

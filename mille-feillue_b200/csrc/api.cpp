@@ -370,8 +370,8 @@ static int true_residual_ws(mf_tiles *t, const double *b, const double *x, doubl
 }
 
 // kind 0 = CG, 1 = BiCGSTAB. b_dev / x_dev: n entries (device). x in: x0.
-static int solve_dev(mf_tiles *t, int kind, const double *b_dev, double *x_dev, double tol, int maxiter,
-                     const mf_options *opt_in, mf_result *res) {
+static int solve_dev_once(mf_tiles *t, int kind, const double *b_dev, double *x_dev, double tol, int maxiter,
+                          const mf_options *opt_in, mf_result *res) {
     if (!t || !b_dev || !x_dev) return MF_ERR_ARG;
     if (t->rowA != t->colA) {
         set_last_error("the solvers need a square matrix");
@@ -506,6 +506,43 @@ static int solve_dev(mf_tiles *t, int kind, const double *b_dev, double *x_dev, 
     }
     if (res) *res = R;
     return status;
+}
+
+// With the learned selector's layouts, a CG solve that misses the tolerance,
+// falls back to the FP64 layout, or runs more than 10% over the reference
+// iteration count (mf_options.reserved[6]) is solved again from the same x0
+// with layouts from the magnitude rule, which this handle keeps afterwards.
+static int solve_dev(mf_tiles *t, int kind, const double *b_dev, double *x_dev, double tol, int maxiter,
+                     const mf_options *opt_in, mf_result *res) {
+    if (!t || !b_dev || !x_dev) return MF_ERR_ARG;
+    const mf_options opt = opt_in ? *opt_in : t->opt;
+    const bool mlp = kind == 0 && t->mixed_ready && t->opt.precision_mode == MF_MODE_MIXED_MLP &&
+                     opt.precision_mode != MF_MODE_FP64;
+    if (!mlp) return solve_dev_once(t, kind, b_dev, x_dev, tol, maxiter, opt_in, res);
+    DevArray<double> x0;
+    if (x0.alloc((size_t)t->rowA)) return MF_ERR_NOMEM;
+    MF_CUDA_TRY(cudaMemcpy(x0.p, x_dev, sizeof(double) * t->rowA, cudaMemcpyDeviceToDevice));
+    mf_result R;
+    std::memset(&R, 0, sizeof R);
+    int rc = solve_dev_once(t, kind, b_dev, x_dev, tol, maxiter, opt_in, &R);
+    const int ref = opt.reserved[6];
+    const bool solved = rc == MF_OK || rc == MF_ERR_NOT_CONVERGED || rc == MF_ERR_BREAKDOWN;
+    const bool bad = rc == MF_ERR_NOT_CONVERGED || rc == MF_ERR_BREAKDOWN || R.fell_back_fp64 ||
+                     (ref > 0 && R.iterations > 1.1 * ref);
+    if (solved && bad) {
+        t->opt.precision_mode = MF_MODE_MIXED_RULE;
+        if ((rc = build_mixed_levels(t, 0)) != MF_OK) return rc;
+        MF_CUDA_TRY(cudaMemcpy(x_dev, x0.p, sizeof(double) * t->rowA, cudaMemcpyDeviceToDevice));
+        mf_options o2 = opt;
+        o2.precision_mode = MF_MODE_MIXED_RULE;
+        const double first_ms = R.time_ms;
+        std::memset(&R, 0, sizeof R);
+        rc = solve_dev_once(t, kind, b_dev, x_dev, tol, maxiter, &o2, &R);
+        R.selector_fallback = 1;
+        R.time_ms += first_ms;  // both solves
+    }
+    if (res) *res = R;
+    return rc;
 }
 
 int mf_solve_cg_dev(mf_tiles *t, const double *b, double *x, double tol, int maxiter, const mf_options *opt,

@@ -1,11 +1,5 @@
-// Per-tile precision selection for the mixed-precision layouts.
-//
-// Features (one warp per tile, from the encoder's tile arrays and the
-// diagonal): f0 = log10 of the tile's scaled magnitude
-// m_t = max |a_ij| / sqrt(|a_ii a_jj|), f1 = log10 of the tile's dynamic
-// range max|a| / min|a|, f2 = nnz / 256, f3 = 1 for a diagonal tile,
-// f4 = log10 max|a| relative to the matrix maximum, f5 = log10 of the
-// relative residual at which the precision is used (filled per level).
+// Per-tile precision selection for the mixed-precision layouts (features:
+// features.cuh).
 //
 // Magnitude rule: at level l with tolerance tau_l a tile takes the lowest of
 // FP8, FP16, FP32 whose unit roundoff u_p satisfies u_p * m_t <= tau_l and
@@ -16,62 +10,91 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
+#include "features.cuh"
 #include "tiles.h"
 
 namespace mf {
 
+int mlp_select(mf_tiles *t, int nlev, const double *rel_res, std::vector<uint8_t> &prec, cudaStream_t s);  // mlp.cu
+
+TileFeatArgs tile_feat_args(const mf_tiles *t) {
+    TileFeatArgs A;
+    A.tilenum = t->tilenum;
+    A.tilem = t->tilem;
+    A.rowA = t->rowA;
+    A.lognnz = 0.0f;
+    A.logrange = 0.0f;
+    A.tile_ptr = t->tile_ptr.p;
+    A.tile_col = t->tile_col.p;
+    A.tile_off = t->tile_off.p;
+    A.csrptr_off = t->csrptr_off.p;
+    A.bptr = t->ptr.p;
+    A.col = t->col.p;
+    A.val = t->val.p;
+    A.diag = t->diag.p;
+    return A;
+}
+
 namespace {
 
-__global__ void k_tile_features(int tilenum, int tilem, const int *tile_ptr, const int *tile_col,
-                                const int *tile_off, const int *csrptr_off, const unsigned char *bptr,
-                                const unsigned char *col, const double *val, const double *diag, int rowA,
-                                float *feat) {
-    const int lane = threadIdx.x & 31;
+__global__ void k_tile_features(TileFeatArgs A, float *feat) {
     const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (t >= tilenum) return;
-    int lo = 0, hi = tilem - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (tile_ptr[mid] <= t) lo = mid; else hi = mid - 1;
+    if (t >= A.tilenum) return;
+    float f[5];
+    warp_tile_features(A, t, f);
+    if ((threadIdx.x & 31) == 0) {
+        float *o = feat + (size_t)t * 6;
+        for (int k = 0; k < 5; ++k) o[k] = f[k];
+        o[5] = 0.0f;
     }
-    const int rb = lo;
-    const int rl = rb == tilem - 1 ? rowA - (tilem - 1) * 16 : 16;
-    const int vo = tile_off[t], nk = tile_off[t + 1] - vo;
-    const int cc = csrptr_off[t];
-    const int c0 = tile_col[t] * 16;
-    double smax = 0.0, amax = 0.0, amin = INFINITY;
-    for (int k = lane; k < nk; k += 32) {
-        // row of entry k: last r with ptr[r] <= k
-        int r = 0;
-        for (int q = 1; q < rl; ++q)
-            if (bptr[cc + q] <= k) r = q;
-        const int i = rb * 16 + r, j = c0 + col[vo + k];
-        const double a = fabs(val[vo + k]);
-        const double di = fabs(diag[i]), dj = j < rowA ? fabs(diag[j]) : 0.0;
-        const double s = (di > 0 && dj > 0) ? a / sqrt(di * dj) : INFINITY;
-        smax = fmax(smax, s);
-        amax = fmax(amax, a);
-        if (a > 0) amin = fmin(amin, a);
+}
+
+// Positive doubles order like their bit patterns: the min / max of |a| over
+// the nonzeros by integer atomics (the caller sets mn to ~0 and mx to 0).
+__global__ void k_absminmax(const double *v, long long n, unsigned long long *mn, unsigned long long *mx) {
+    unsigned long long lo = ~0ull, hi = 0ull;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(v[i]));
+        if (b != 0ull) lo = b < lo ? b : lo;
+        hi = b > hi ? b : hi;
     }
     for (int d = 16; d > 0; d >>= 1) {
-        smax = fmax(smax, __shfl_xor_sync(0xffffffffu, smax, d));
-        amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, d));
-        amin = fmin(amin, __shfl_xor_sync(0xffffffffu, amin, d));
+        const unsigned long long l2 = __shfl_xor_sync(0xffffffffu, lo, d), h2 = __shfl_xor_sync(0xffffffffu, hi, d);
+        lo = l2 < lo ? l2 : lo;
+        hi = h2 > hi ? h2 : hi;
     }
-    if (lane == 0) {
-        float *f = feat + (size_t)t * 6;
-        f[0] = (float)log10(fmax(smax, 1e-300));
-        f[1] = amax > 0 && amin < INFINITY ? (float)log10(amax / amin) : 0.0f;
-        f[2] = nk / 256.0f;
-        f[3] = tile_col[t] == rb ? 1.0f : 0.0f;
-        f[4] = (float)log10(fmax(amax, 1e-300));  // made relative on the host
-        f[5] = 0.0f;
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(mn, lo);
+        atomicMax(mx, hi);
     }
 }
 
 }  // namespace
+
+// The whole-matrix features f2 and f4 (a device reduction over the values).
+int matrix_features(const mf_tiles *t, float *lognnz, float *logrange, cudaStream_t s) {
+    *lognnz = (float)std::log10(std::max(1.0, (double)t->csrsize));
+    *logrange = 0.0f;
+    if (t->csrsize == 0) return MF_OK;
+    DevArray<unsigned long long> d;
+    if (d.alloc(2)) return MF_ERR_NOMEM;
+    const unsigned long long init[2] = {~0ull, 0ull};
+    MF_CUDA_TRY(cudaMemcpyAsync(d.p, init, sizeof init, cudaMemcpyHostToDevice, s));
+    k_absminmax<<<592, 256, 0, s>>>(t->val.p, (long long)t->csrsize, d.p, d.p + 1);
+    MF_CUDA_TRY(cudaGetLastError());
+    unsigned long long h[2];
+    MF_CUDA_TRY(cudaMemcpyAsync(h, d.p, sizeof h, cudaMemcpyDeviceToHost, s));
+    MF_CUDA_TRY(cudaStreamSynchronize(s));
+    if (h[0] == ~0ull || h[1] == 0ull) return MF_OK;
+    double lo, hi;
+    std::memcpy(&lo, &h[0], sizeof lo);
+    std::memcpy(&hi, &h[1], sizeof hi);
+    *logrange = (float)std::log10(hi / lo);
+    return MF_OK;
+}
 
 int tile_features(mf_tiles *t, std::vector<float> &feat, cudaStream_t s) {
     const int tn = t->tilenum;
@@ -79,15 +102,13 @@ int tile_features(mf_tiles *t, std::vector<float> &feat, cudaStream_t s) {
     if (tn == 0) return MF_OK;
     DevArray<float> d;
     if (d.alloc((size_t)tn * 6)) return MF_ERR_NOMEM;
-    k_tile_features<<<(tn + 7) / 8, 256, 0, s>>>(tn, t->tilem, t->tile_ptr.p, t->tile_col.p, t->tile_off.p,
-                                                 t->csrptr_off.p, t->ptr.p, t->col.p, t->val.p, t->diag.p, t->rowA,
-                                                 d.p);
+    TileFeatArgs A = tile_feat_args(t);
+    int rc = matrix_features(t, &A.lognnz, &A.logrange, s);
+    if (rc) return rc;
+    k_tile_features<<<(tn + 7) / 8, 256, 0, s>>>(A, d.p);
     MF_CUDA_TRY(cudaGetLastError());
     MF_CUDA_TRY(cudaMemcpyAsync(feat.data(), d.p, sizeof(float) * feat.size(), cudaMemcpyDeviceToHost, s));
     MF_CUDA_TRY(cudaStreamSynchronize(s));
-    float gmax = -1e30f;
-    for (int k = 0; k < tn; ++k) gmax = std::max(gmax, feat[(size_t)k * 6 + 4]);
-    for (int k = 0; k < tn; ++k) feat[(size_t)k * 6 + 4] -= gmax;
     return MF_OK;
 }
 
@@ -140,6 +161,35 @@ int build_mixed_levels(mf_tiles *t, cudaStream_t s) {
         int rc = build_layout(t, t->Lmix[0], p, s);
         if (rc) return rc;
         t->nlevels = 1;
+        t->mixed_ready = true;
+        return MF_OK;
+    }
+    if (mode == MF_MODE_MIXED_MLP) {
+        // the learned selector: one class per tile and level, with the
+        // level's starting relative residual as the sixth feature
+        double res[MF_NLEVELS];
+        int nlev = 0;
+        for (int l = 0; l < MF_NLEVELS; ++l) {
+            res[l] = l == 0 ? 1.0 : kLevelSwitch[l - 1];
+            ++nlev;
+            if (kLevelSwitch[l] <= 0.0) break;  // the last level used
+        }
+        std::vector<uint8_t> pm;
+        int rc = mlp_select(t, nlev, res, pm, s);
+        if (rc) return rc;
+        int nl = 0;
+        std::vector<uint8_t> prev;
+        for (int l = 0; l < nlev; ++l) {
+            std::vector<uint8_t> p(pm.begin() + (size_t)l * t->tilenum, pm.begin() + (size_t)(l + 1) * t->tilenum);
+            promote_minority(t, p);
+            if (l > 0 && p == prev) break;
+            rc = build_layout(t, t->Lmix[l], p, s);
+            if (rc) return rc;
+            t->level_switch[l] = kLevelSwitch[l];
+            prev.swap(p);
+            ++nl;
+        }
+        t->nlevels = nl;
         t->mixed_ready = true;
         return MF_OK;
     }

@@ -75,6 +75,34 @@ def lib():
     return _lib
 
 
+# MLP weight blocks inside the packed weight vector: W1[64][6], b1[64],
+# W2[64][64], b2[64], W3[4][64], b3[4]
+_MLP_BLOCKS = [(0, 384), (384, 448), (448, 4544), (4544, 4608), (4608, 4864), (4864, 4868)]
+
+
+def mlp_forward(w, x):
+    """Logits (n, 4) of the oracle's FP32 MLP for packed weights w."""
+    w = np.ascontiguousarray(w, np.float32)
+    x = np.ascontiguousarray(x, np.float32)
+    n = x.shape[0]
+    out = np.zeros((n, 4), np.float32)
+    parts = [w[a:b] for a, b in _MLP_BLOCKS]
+    lib().mfo_mlp_forward(*[_ptr(q) for q in parts], _ptr(x), n, _ptr(out))
+    return out
+
+
+def mlp_grad(w, x, labels):
+    """(packed gradient, loss) of the mean softmax cross-entropy."""
+    w = np.ascontiguousarray(w, np.float32)
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(labels, np.int32)
+    parts = [w[a:b] for a, b in _MLP_BLOCKS]
+    g = np.zeros_like(w)
+    gparts = [g[a:b] for a, b in _MLP_BLOCKS]
+    loss = lib().mfo_mlp_grad(*[_ptr(q) for q in parts], _ptr(x), _ptr(y), x.shape[0], *[_ptr(q) for q in gparts])
+    return g, float(loss)
+
+
 def ref_available():
     return os.path.exists(REF_SO)
 

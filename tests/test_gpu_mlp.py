@@ -1,0 +1,160 @@
+"""Learned precision selector: the GPU forward and backward kernels against
+the CPU oracle's MLP, training, the selector fused into the feature pass,
+and the magnitude-rule fallback of the solve."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+NW = 4868
+
+
+def _weights(seed, scale=0.2):
+    return (np.random.default_rng(seed).standard_normal(NW) * scale).astype(np.float32)
+
+
+def _dev(a):
+    import torch
+
+    return torch.tensor(a, device="cuda")
+
+
+def test_forward_matches_oracle(mf, O):
+    import ctypes as C
+    import torch
+
+    w = _weights(1)
+    x = np.random.default_rng(2).standard_normal((1500, 6)).astype(np.float32)
+    wd, xd = _dev(w), _dev(x)
+    out = torch.zeros((1500, 4), dtype=torch.float32, device="cuda")
+    assert mf.lib().mf_mlp_forward_dev(C.c_void_p(wd.data_ptr()), C.c_void_p(xd.data_ptr()), 1500, 0,
+                                       C.c_void_p(out.data_ptr())) == 0
+    ref = O.mlp_forward(w, x)
+    assert np.max(np.abs(out.cpu().numpy() - ref)) <= 1e-5 * max(1.0, np.max(np.abs(ref)))
+
+
+def test_gradient_matches_oracle(mf, O):
+    """Samples span several blocks of the kernel (512 each), so the fixed-order
+    sum of the per-block partial gradients is exercised too."""
+    import ctypes as C
+    import torch
+
+    rng = np.random.default_rng(3)
+    w = _weights(4)
+    n = 2600
+    x = rng.standard_normal((n, 6)).astype(np.float32)
+    y = rng.integers(0, 4, n).astype(np.int32)
+    g = torch.zeros(NW, dtype=torch.float32, device="cuda")
+    loss = C.c_float()
+    wd, xd, yd = _dev(w), _dev(x), torch.tensor(y, device="cuda")
+    assert mf.lib().mf_mlp_grad_dev(C.c_void_p(wd.data_ptr()), C.c_void_p(xd.data_ptr()), C.c_void_p(yd.data_ptr()),
+                                    n, C.c_void_p(g.data_ptr()), C.byref(loss)) == 0
+    g_ref, loss_ref = O.mlp_grad(w, x, y)
+    gg = g.cpu().numpy()
+    assert abs(loss.value - loss_ref) <= 1e-5 * abs(loss_ref)
+    # FP32 sums in different orders: tolerance relative to the gradient's size
+    assert np.linalg.norm(gg - g_ref) <= 1e-5 * np.linalg.norm(g_ref)
+    assert np.max(np.abs(gg - g_ref)) <= 1e-5 * np.max(np.abs(g_ref))
+    # the gradient is deterministic
+    g2 = torch.zeros_like(g)
+    mf.lib().mf_mlp_grad_dev(C.c_void_p(wd.data_ptr()), C.c_void_p(xd.data_ptr()), C.c_void_p(yd.data_ptr()), n,
+                             C.c_void_p(g2.data_ptr()), C.byref(loss))
+    assert torch.equal(g, g2)
+
+
+def test_training_learns_a_rule(mf):
+    """Labels from a threshold rule on two features: Adam on the GPU kernels
+    fits it to > 97 % training accuracy."""
+    import ctypes as C
+    import torch
+
+    rng = np.random.default_rng(5)
+    n = 20000
+    x = rng.uniform(-1, 1, (n, 6)).astype(np.float32)
+    y = np.where(x[:, 0] > 0.3, 0, np.where(x[:, 0] > -0.2, 1, np.where(x[:, 3] > 0, 1, 2))).astype(np.int32)
+    w = _weights(6, 0.1)
+    wd, xd, yd = _dev(w), _dev(x), torch.tensor(y, device="cuda")
+    loss = C.c_float()
+    assert mf.lib().mf_mlp_train_dev(C.c_void_p(wd.data_ptr()), C.c_void_p(xd.data_ptr()),
+                                     C.c_void_p(yd.data_ptr()), n, 1500, 512, C.c_float(3e-3), C.byref(loss)) == 0
+    out = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    mf.lib().mf_mlp_forward_dev(C.c_void_p(wd.data_ptr()), C.c_void_p(xd.data_ptr()), n, 0, C.c_void_p(out.data_ptr()))
+    acc = float(np.mean(out.cpu().numpy().argmax(1) == y))
+    assert acc > 0.97, (acc, loss.value)
+
+
+def _select_numpy(logits, f):
+    c = logits.argmax(1)
+    c = np.where((f[:, 3] > 0.5) & (c > 1), 1, c)
+    c = np.where((c == 3) & (f[:, 1] > 3.6124), 2, c)
+    c = np.where((c == 2) & (f[:, 1] > 8.0), 1, c)
+    c = np.where(~np.isfinite(f[:, 0]) | (f[:, 0] > 300), 0, c)
+    return c
+
+
+def test_fused_selector_equals_features_plus_forward(mf):
+    """The selector fused into the feature pass (BF16 weights) gives the class
+    of the separate feature export + BF16 forward."""
+    import ctypes as C
+    import torch
+
+    A = mf.Matrix.varpoisson3d(12, 1e-2, 1e2, 3)
+    t = mf.Tiles(A)
+    w = _weights(7, 0.5)
+    mf.set_mlp_weights(w)
+    try:
+        levels = np.array([1.0, 1e-6])
+        p = t.select_mlp(levels)
+        f = t.features()
+        assert np.allclose(f[:, 2], np.log10(A.nnz), atol=1e-5)  # whole-matrix nnz feature
+        for l, res in enumerate(levels):
+            fl = f.copy()
+            fl[:, 5] = np.log10(res)
+            out = torch.zeros((len(f), 4), dtype=torch.float32, device="cuda")
+            wd, fd = _dev(w), _dev(fl)
+            mf.lib().mf_mlp_forward_dev(C.c_void_p(wd.data_ptr()), C.c_void_p(fd.data_ptr()), len(f), 1,
+                                        C.c_void_p(out.data_ptr()))
+            logits = out.cpu().numpy()
+            srt = np.sort(logits, 1)
+            clear = (srt[:, 3] - srt[:, 2]) > 1e-4  # near-ties may break either way
+            assert np.array_equal(p[l][clear], _select_numpy(logits, fl)[clear])
+            assert clear.mean() > 0.99
+    finally:
+        mf.set_mlp_weights(None)
+
+
+def test_selector_fallback_to_rule(mf):
+    """Weights that put every off-diagonal tile as low as its range allows
+    (FP8 or FP16) make the solve miss; the rule then solves it from the same
+    x0 and the result says so."""
+    A = mf.Matrix.varpoisson3d(20)
+    b = A.b()
+    w = np.zeros(NW, np.float32)
+    w[4864:4868] = [0.0, 0.0, 0.0, 10.0]  # b3: class FP8 everywhere
+    mf.set_mlp_weights(w)
+    try:
+        t = mf.Tiles(A, mf.options(precision_mode=mf.MODE_MIXED_MLP))
+        p, _ = t.precisions()
+        assert (p >= mf.PREC_FP16).mean() > 0.5
+        x, res = t.solve_cg(b, tol=1e-10, maxiter=20000)
+        assert res["selector_fallback"] == 1, res
+        assert res["status"] == 0 and res["rel_residual_true"] <= 1e-10, res
+    finally:
+        mf.set_mlp_weights(None)
+
+
+def test_packaged_selector_solves(mf):
+    """The trained selector shipped with the package reaches the FP64 true
+    residual on a held-out matrix of the training family."""
+    import os
+
+    if not os.path.exists(mf.MLP_WEIGHTS_PATH):
+        pytest.skip("no trained selector weights packaged")
+    A = mf.Matrix.varpoisson3d(40, 10 ** -2.5, 10 ** 2.5, 901)
+    b = A.b()
+    try:
+        t = mf.Tiles(A, mf.options(precision_mode=mf.MODE_MIXED_MLP))
+        x, res = t.solve_cg(b, tol=1e-10, maxiter=40000)
+        assert res["status"] == 0 and res["rel_residual_true"] <= 1e-10, res
+    finally:
+        mf.set_mlp_weights(None)

@@ -139,3 +139,44 @@ def test_two_pointer_balance_small_case(O):
     assert idx == 2
     assert list(bp) == [0, 2, 6]
     assert list(a[:6]) == [0, 5, 1, 4, 2, 3]
+
+
+def _np_mlp_grad(w, x, y):
+    """FP64 numpy forward/backward of the 6-64-64-4 ReLU MLP (softmax
+    cross-entropy, mean over the batch): an independent check of the oracle."""
+    w = w.astype(np.float64)
+    W1, b1 = w[0:384].reshape(64, 6), w[384:448]
+    W2, b2 = w[448:4544].reshape(64, 64), w[4544:4608]
+    W3, b3 = w[4608:4864].reshape(4, 64), w[4864:4868]
+    x = x.astype(np.float64)
+    z1 = x @ W1.T + b1
+    h1 = np.maximum(z1, 0)
+    z2 = h1 @ W2.T + b2
+    h2 = np.maximum(z2, 0)
+    o = h2 @ W3.T + b3
+    o -= o.max(1, keepdims=True)
+    p = np.exp(o)
+    p /= p.sum(1, keepdims=True)
+    n = len(x)
+    loss = -np.mean(np.log(p[np.arange(n), y]))
+    d3 = p.copy()
+    d3[np.arange(n), y] -= 1
+    d3 /= n
+    d2 = (d3 @ W3) * (z2 > 0)
+    d1 = (d2 @ W2) * (z1 > 0)
+    g = np.concatenate([(d1.T @ x).ravel(), d1.sum(0), (d2.T @ h1).ravel(), d2.sum(0), (d3.T @ h2).ravel(),
+                        d3.sum(0)])
+    return g, loss
+
+
+def test_oracle_mlp_gradient_matches_numpy(O):
+    rng = np.random.default_rng(12)
+    w = (rng.standard_normal(4868) * 0.3).astype(np.float32)
+    x = rng.standard_normal((300, 6)).astype(np.float32)
+    y = rng.integers(0, 4, 300)
+    g, loss = O.mlp_grad(w, x, y)
+    g64, loss64 = _np_mlp_grad(w, x, y)
+    assert abs(loss - loss64) <= 1e-5 * loss64
+    assert np.linalg.norm(g - g64) <= 1e-4 * np.linalg.norm(g64)
+    logits = O.mlp_forward(w, x)
+    assert logits.shape == (300, 4)
