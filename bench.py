@@ -392,7 +392,7 @@ def batch_arm(args, world, rank, local, dist):
         "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "batch512_spd n~logU[1e3,2e5] seed 2, CG to 1e-10", "systems": len(mats),
                    "rows_rank0": inf["rows"], "nnz_rank0": inf["nnz"], "grid": inf["grid"],
-                   "ctas_per_group": args.batch_group or 8,
+                   "ctas_per_group": args.batch_group or 4,
                    "parallelism": f"systems split over {world} ranks (LPT)" if world > 1 else "single"},
         "iterations_min_max": [int(it.min()), int(it.max())], "all_converged": bool(np.all(st == 0)),
         "max_rel_residual": float(rel.max()),

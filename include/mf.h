@@ -87,7 +87,7 @@ typedef struct {
                                 2-10 us per SpMV; read at encode for
                                 mf_spmv, at solve for the solvers);
                                 reserved[4] = CTAs per system group of
-                                mf_batch_create (0 = 8); reserved[5] = 1:
+                                mf_batch_create (0 = 4); reserved[5] = 1:
                                 the single-reduction CG keeps x and r in
                                 global memory instead of tensor memory;
                                 reserved[6] = N > 0: reference iteration
@@ -297,7 +297,7 @@ int mf_mlp_train_dev(float *w, const float *x, const int *labels, int n,
 
 /* ---- batched solve of many independent systems ------------------------- */
 /* Encodes `count` square systems (host CSR) for one persistent launch. The
- * grid is split into groups of opt->reserved[4] CTAs (0 = 8); each group
+ * grid is split into groups of opt->reserved[4] CTAs (0 = 4); each group
  * solves whole systems taken from a device queue, largest first, with
  * reductions local to the group. with_baseline != 0 also builds whole-GPU
  * layouts for mf_batch_solve_cg_each_dev (one launch per system).          */
