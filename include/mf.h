@@ -239,6 +239,15 @@ int mf_solve_cg(mf_tiles *t, const double *b_host, double *x_host, double tol,
 /* Same with device vectors (n entries each).                                */
 int mf_solve_cg_dev(mf_tiles *t, const double *b_dev, double *x_dev, double tol,
                     int maxiter, const mf_options *opt, mf_result *res);
+/* Jacobi-preconditioned CG (M = diag(A), the "jpcg" runs of the reference's
+ * PETSc comparison: KSPCG + PCJACOBI, PC/PETSc/src/ksp/ksp/impls/cg/cg.c),
+ * FP64 layout, one persistent kernel; stops on the unpreconditioned
+ * ||b - A x|| / ||b|| <= tol like mf_solve_cg. precision_mode is ignored.   */
+int mf_solve_pcg(mf_tiles *t, const double *b_host, double *x_host, double tol,
+                 int maxiter, const mf_options *opt, mf_result *res);
+int mf_solve_pcg_dev(mf_tiles *t, const double *b_dev, double *x_dev,
+                     double tol, int maxiter, const mf_options *opt,
+                     mf_result *res);
 /* Single persistent-kernel BiCGSTAB.                                         */
 int mf_solve_bicgstab(mf_tiles *t, const double *b_host, double *x_host,
                       double tol, int maxiter, const mf_options *opt,

@@ -112,7 +112,8 @@ EXPORTED = [
     "mf_spmv_level", "mf_spmv_bench_level", "mf_trace", "mf_batch_create", "mf_batch_solve_cg_dev",
     "mf_batch_solve_cg_each_dev", "mf_batch_results", "mf_batch_info", "mf_batch_free",
     "mf_solve_cg_dev_noalloc", "mf_mlp_set_weights", "mf_mlp_get_weights", "mf_tiles_features",
-    "mf_tiles_select_mlp", "mf_mlp_forward_dev", "mf_mlp_grad_dev", "mf_mlp_train_dev",
+    "mf_tiles_select_mlp", "mf_mlp_forward_dev", "mf_mlp_grad_dev", "mf_mlp_train_dev", "mf_solve_pcg",
+    "mf_solve_pcg_dev",
 ]
 MLP_WEIGHTS = 4868
 MLP_WEIGHTS_PATH = os.path.join(_HERE, "mlp_weights.bin")
@@ -163,7 +164,8 @@ def lib():
     L.mf_spmv_host.argtypes = [_p, _p, _p]
     L.mf_spmv_bench.argtypes = [_p, _p, _p, _i, C.POINTER(_d), C.POINTER(_d)]
     L.mf_spmv_bench_level.argtypes = [_p, _i, _p, _p, _i, C.POINTER(_d), C.POINTER(_d)]
-    for f in ("mf_solve_cg", "mf_solve_cg_dev", "mf_solve_bicgstab", "mf_solve_bicgstab_dev",
+    for f in ("mf_solve_cg", "mf_solve_cg_dev", "mf_solve_bicgstab", "mf_solve_bicgstab_dev", "mf_solve_pcg",
+              "mf_solve_pcg_dev",
               "mf_solve_cg_dev_noalloc"):
         getattr(L, f).argtypes = [_p, _p, _p, _d, _i, C.POINTER(MfOptions), C.POINTER(MfResult)]
     L.mf_true_residual.argtypes = [_p, _p, _p, C.POINTER(_d)]
@@ -448,6 +450,13 @@ class Tiles:
 
     def solve_bicgstab(self, b, x0=None, tol=1e-10, maxiter=10000, opts=None):
         return self._solve(lib().mf_solve_bicgstab, b, x0, tol, maxiter, opts)
+
+    def solve_pcg(self, b, x0=None, tol=1e-10, maxiter=10000, opts=None):
+        """Jacobi-preconditioned CG (FP64)."""
+        return self._solve(lib().mf_solve_pcg, b, x0, tol, maxiter, opts)
+
+    def solve_pcg_dev(self, b_ptr, x_ptr, tol=1e-10, maxiter=10000, opts=None):
+        return self._solve_dev(lib().mf_solve_pcg_dev, b_ptr, x_ptr, tol, maxiter, opts)
 
     def _solve_dev(self, fn, b_ptr, x_ptr, tol, maxiter, opts):
         res = MfResult()

@@ -369,7 +369,8 @@ static int true_residual_ws(mf_tiles *t, const double *b, const double *x, doubl
     return MF_OK;
 }
 
-// kind 0 = CG, 1 = BiCGSTAB. b_dev / x_dev: n entries (device). x in: x0.
+// kind 0 = CG, 1 = BiCGSTAB, 2 = Jacobi-preconditioned CG (FP64 layout).
+// b_dev / x_dev: n entries (device). x in: x0.
 static int solve_dev_once(mf_tiles *t, int kind, const double *b_dev, double *x_dev, double tol, int maxiter,
                           const mf_options *opt_in, mf_result *res) {
     if (!t || !b_dev || !x_dev) return MF_ERR_ARG;
@@ -444,7 +445,11 @@ static int solve_dev_once(mf_tiles *t, int kind, const double *b_dev, double *x_
     cudaEventRecord(e0, 0);
     // mixed layouts run the single-reduction CG unless the classic
     // recurrence is asked for (mf_options.reserved[2] == 1)
-    int launch_kind = (mixed && opt.reserved[2] != 1) ? 2 : kind;
+    if (kind == 2) {
+        int rj = launch_jacobi_inv(n, (int)n16, t->diag.p, v.s, 0);
+        if (rj) return rj;
+    }
+    int launch_kind = kind == 2 ? 4 : (mixed && opt.reserved[2] != 1) ? 2 : kind;
     if (launch_kind == 2 && opt.reserved[5] != 1) {
         // x and r stay in tensor memory when every CTA's rows fit it
         int rows_max = 0;
@@ -491,7 +496,7 @@ static int solve_dev_once(mf_tiles *t, int kind, const double *b_dev, double *x_
         R.spmv_bytes_level[l] = (mixed && t->Lmix[l].built) ? t->Lmix[l].alg_bytes : 0.0;
     }
     {
-        const double vec = 56.0 * (double)n;
+        const double vec = (kind == 2 ? 72.0 : 56.0) * (double)n;  // PCG also reads 1/a_ii twice
         double tb = (double)(1 + dr.replacements) * (t->L64.alg_bytes + 16.0 * n);  // initial + replacements
         tb += (double)dr.it_layout[0] * (t->L64.alg_bytes + vec);
         for (int l = 0; l < 3; ++l) tb += (double)dr.it_layout[l + 1] * (R.spmv_bytes_level[l] + vec);
@@ -549,6 +554,10 @@ int mf_solve_cg_dev(mf_tiles *t, const double *b, double *x, double tol, int max
                     mf_result *res) {
     return solve_dev(t, 0, b, x, tol, maxiter, opt, res);
 }
+int mf_solve_pcg_dev(mf_tiles *t, const double *b, double *x, double tol, int maxiter, const mf_options *opt,
+                     mf_result *res) {
+    return solve_dev(t, 2, b, x, tol, maxiter, opt, res);
+}
 int mf_solve_bicgstab_dev(mf_tiles *t, const double *b, double *x, double tol, int maxiter,
                           const mf_options *opt, mf_result *res) {
     return solve_dev(t, 1, b, x, tol, maxiter, opt, res);
@@ -570,6 +579,10 @@ static int solve_host(mf_tiles *t, int kind, const double *b, double *x, double 
 int mf_solve_cg(mf_tiles *t, const double *b, double *x, double tol, int maxiter, const mf_options *opt,
                 mf_result *res) {
     return solve_host(t, 0, b, x, tol, maxiter, opt, res);
+}
+int mf_solve_pcg(mf_tiles *t, const double *b, double *x, double tol, int maxiter, const mf_options *opt,
+                 mf_result *res) {
+    return solve_host(t, 2, b, x, tol, maxiter, opt, res);
 }
 int mf_solve_bicgstab(mf_tiles *t, const double *b, double *x, double tol, int maxiter, const mf_options *opt,
                       mf_result *res) {

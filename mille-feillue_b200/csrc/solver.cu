@@ -900,6 +900,166 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cg(KParams P) {
     (void)G;
 }
 
+// ----------------------------------------------- Jacobi-preconditioned CG
+// PCG with M = diag(A) (KSPCG + PCJACOBI, the "jpcg" runs of the reference's
+// PETSc comparison) on the FP64 layout, in one persistent kernel like k_cg:
+//   z = M^-1 r;  d = z;  rz = r.z
+//   q = A d;  alpha = rz / d.q;  x += alpha d;  r -= alpha q;  z = M^-1 r
+//   beta = (r.z)_new / rz;  d = z + beta d
+// M^-1 is applied on the fly from 1/a_ii (P.s, filled by the host); z is
+// never stored. The stop test is the unpreconditioned ||r|| / ||b||, as for
+// CG; r.z and r.r share one grid reduction.
+__global__ void __launch_bounds__(NTHREADS, 1) k_pcg(KParams P) {
+    extern __shared__ __align__(128) uint8_t dyn[];
+    __shared__ Smem S;
+    kernel_setup(P, S, 1);
+    const int g = blockIdx.x, tid = threadIdx.x;
+    Pipe pp;
+    uint32_t phase = 0;
+    const uint64_t vpol = policy_evict_last();
+    const int vlo = P.lay[0].cta_rb[g] * 16, vhi = P.lay[0].cta_rb[g + 1] * 16;
+    double *x = P.x, *r = P.r, *d = P.d, *q = P.q;
+    const double *minv = P.s, *b = P.b;
+    // r = b - A x0;  d = z = M^-1 r
+    EpiResidual er{b, r, 0.0, vpol};
+    if (!cta_spmv<false>(P, 0, x, S, dyn, pp, er)) return;
+    double rzp = 0.0, bbp = 0.0;
+    MF_PAIRS(2, vlo, vhi, {
+        double2 rv[_vb], bv[_vb], mv[_vb];
+#pragma unroll
+        MF_FOR_VB if (MF_LIVE(u, vhi)) {
+            rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+            bv[u] = ld2_hint(b + 2 * MF_PI(u), vpol);
+            mv[u] = ld2_hint(minv + 2 * MF_PI(u), vpol);
+        }
+#pragma unroll
+        MF_FOR_VB if (MF_LIVE(u, vhi)) {
+            double2 z;
+            z.x = mv[u].x * rv[u].x;
+            z.y = mv[u].y * rv[u].y;
+            st2_hint(d + 2 * MF_PI(u), z, vpol);
+            rzp += rv[u].x * z.x + rv[u].y * z.y;
+            bbp += bv[u].x * bv[u].x + bv[u].y * bv[u].y;
+        }
+    })
+    double v3[3] = {er.rr, rzp, bbp}, o3[3];
+    if (!grid_sum<3>(P, S, v3, o3, phase)) return;
+    double rr = o3[0], rz = o3[1];
+    const double bb = o3[2];
+    const double bnorm = sqrt(bb);
+    const double tol = P.tol;
+    uint32_t ep = 1;
+    publish(P, ep);
+    int it = 0, status = MF_OK;
+    double rel = bnorm > 0 ? sqrt(rr) / bnorm : 0.0;
+    const bool fixed = P.fixed_iterations > 0;
+    const int maxit = fixed ? P.fixed_iterations : P.maxiter;
+    while (it < maxit && (fixed || rel > tol)) {
+        MF_TRACE(it, 0);
+        if (!wait_deps(P, S, 0, ep)) return;
+        MF_TRACE(it, 1);
+        EpiQ eq{d, q, 0.0, vpol};
+        if (!cta_spmv<false>(P, 0, d, S, dyn, pp, eq)) return;
+        MF_TRACE(it, 2);
+        double v1[1] = {eq.dq}, o1[1];
+        if (!grid_sum<1>(P, S, v1, o1, phase)) return;
+        MF_TRACE(it, 3);
+        const double dq = o1[0];
+        if (!(dq != 0.0) || !isfinite(dq)) {
+            status = MF_ERR_BREAKDOWN;
+            break;
+        }
+        const double alpha = rz / dq;
+        double rzn = 0.0, rrn = 0.0;
+        MF_PAIRS(2, vlo, vhi, {
+            double2 rv[_vb], qv[_vb], mv[_vb];
+#pragma unroll
+            MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+                qv[u] = ld2_hint(q + 2 * MF_PI(u), vpol);
+                mv[u] = ld2_hint(minv + 2 * MF_PI(u), vpol);
+            }
+#pragma unroll
+            MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                double2 o;
+                o.x = rv[u].x - alpha * qv[u].x;
+                o.y = rv[u].y - alpha * qv[u].y;
+                st2_hint(r + 2 * MF_PI(u), o, vpol);
+                rzn += o.x * (mv[u].x * o.x) + o.y * (mv[u].y * o.y);
+                rrn += o.x * o.x + o.y * o.y;
+            }
+        })
+        MF_TRACE(it, 4);
+        double w2[2] = {rzn, rrn}, u2[2];
+        if (!grid_sum<2>(P, S, w2, u2, phase)) return;
+        MF_TRACE(it, 5);
+        rr = u2[1];
+        ++it;
+        rel = bnorm > 0 ? sqrt(rr) / bnorm : 0.0;
+        const double beta = u2[0] / rz;
+        rz = u2[0];
+        const bool done = !fixed && rel <= tol;
+        MF_PAIRS(2, vlo, vhi, {
+            double2 dv[_vb], xv[_vb], rv[_vb], mv[_vb];
+#pragma unroll
+            MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                dv[u] = ld2_hint(d + 2 * MF_PI(u), vpol);
+                xv[u] = ld2_hint(x + 2 * MF_PI(u), vpol);
+                if (!done) {
+                    rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+                    mv[u] = ld2_hint(minv + 2 * MF_PI(u), vpol);
+                }
+            }
+#pragma unroll
+            MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                double2 xo, dn;
+                xo.x = xv[u].x + alpha * dv[u].x;
+                xo.y = xv[u].y + alpha * dv[u].y;
+                st2_hint(x + 2 * MF_PI(u), xo, vpol);
+                if (!done) {
+                    dn.x = mv[u].x * rv[u].x + beta * dv[u].x;
+                    dn.y = mv[u].y * rv[u].y + beta * dv[u].y;
+                    st2_hint(d + 2 * MF_PI(u), dn, vpol);
+                }
+            }
+        })
+        ++ep;
+        publish(P, ep);
+        MF_TRACE(it - 1, 6);
+        if (!isfinite(rr)) {
+            status = MF_ERR_BREAKDOWN;
+            break;
+        }
+    }
+    if (g == 0 && tid == 0) {
+        if (status == MF_OK && !fixed && rel > tol) status = MF_ERR_NOT_CONVERGED;
+        P.res->iterations = it;
+        P.res->status = status;
+        P.res->replacements = 0;
+        P.res->level_switches = 0;
+        P.res->rr = rr;
+        P.res->bb = bb;
+        P.res->final_layout = 0;
+        for (int l = 0; l < KMAX_LAYOUTS; ++l) P.res->it_layout[l] = l == 0 ? it : 0;
+        P.res->pad = 0;
+    }
+}
+
+// 1/a_ii for the Jacobi preconditioner (rows with a zero diagonal and the
+// padding rows keep 1 / 0 so that they pass r through / stay zero).
+__global__ void k_jacobi_inv(int n, int npad, const double *diag, double *minv) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npad; i += gridDim.x * blockDim.x)
+        minv[i] = i < n ? (diag[i] != 0.0 ? 1.0 / diag[i] : 1.0) : 0.0;
+}
+
+int launch_jacobi_inv(int n, int npad, const double *diag, double *minv, cudaStream_t s) {
+    int blocks = (npad + 255) / 256;
+    blocks = blocks < 1 ? 1 : (blocks > 1184 ? 1184 : blocks);
+    k_jacobi_inv<<<blocks, 256, 0, s>>>(n, npad, diag, minv);
+    MF_CUDA_TRY(cudaGetLastError());
+    return MF_OK;
+}
+
 // ------------------------------------------------- CG, single reduction
 // Chronopoulos-Gear form of CG for the mixed-precision layouts: one grid
 // reduction and one fused vector pass per iteration. w = A r comes from the
@@ -1833,7 +1993,7 @@ int kernel_config(mf_tiles *t, int *G_out) {
     }
     const void *kerns[] = {(const void *)k_cg<false>, (const void *)k_cg<true>, (const void *)k_bicgstab,
                            (const void *)k_spmv<false>, (const void *)k_spmv<true>, (const void *)k_cgcg,
-                           (const void *)k_batch_cg, (const void *)k_cgcg_tm};
+                           (const void *)k_batch_cg, (const void *)k_cgcg_tm, (const void *)k_pcg};
     int occ_min = 1 << 30;
     for (const void *k : kerns) {
         MF_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
@@ -1923,6 +2083,7 @@ int launch_solver(mf_tiles *t, int kind, KParams &P, cudaStream_t s) {
     const void *k = kind == 0   ? (P.nlay > 1 ? (const void *)k_cg<true> : (const void *)k_cg<false>)
                     : kind == 2 ? (const void *)k_cgcg
                     : kind == 3 ? (const void *)k_cgcg_tm
+                    : kind == 4 ? (const void *)k_pcg
                                 : (const void *)k_bicgstab;
     MF_CUDA_TRY(cudaLaunchCooperativeKernel(k, dim3(t->G), dim3(NTHREADS), args, dyn, s));
     return MF_OK;

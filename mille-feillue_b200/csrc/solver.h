@@ -102,9 +102,11 @@ int launch_spmv(mf_tiles *t, int level, const void *x, double *y, int reps, cuda
 // dst[0..n) = (float)src[0..n), dst[n..npad) = 0.
 int launch_to_f32(int n, const double *src, float *dst, size_t npad, cudaStream_t s);
 // kind 0 CG, 1 BiCGSTAB, 2 single-reduction CG, 3 the same with x and r in
-// TMEM (every CTA's rows <= TMEM_ROWS_MAX).
+// TMEM (every CTA's rows <= TMEM_ROWS_MAX), 4 Jacobi-preconditioned CG.
 constexpr int TMEM_ROWS_MAX = 128 * 128;
 int launch_solver(mf_tiles *t, int kind, KParams &P, cudaStream_t s);
 int launch_residual_norms(int n, const double *b, const double *ax, double *out, cudaStream_t s);
+// minv[i] = 1 / diag[i] for i < n (1 where diag is 0), 0 up to npad.
+int launch_jacobi_inv(int n, int npad, const double *diag, double *minv, cudaStream_t s);
 
 }  // namespace mf

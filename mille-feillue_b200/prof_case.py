@@ -21,7 +21,7 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel", default="spmv", choices=["spmv", "cg", "bicgstab"])
+    ap.add_argument("--kernel", default="spmv", choices=["spmv", "cg", "pcg", "bicgstab"])
     ap.add_argument("--grid", type=int, default=128)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--iters", type=int, default=50)
@@ -80,8 +80,9 @@ def main():
         o.reserved[3] = 1
     if args.no_tmem:
         o.reserved[5] = 1
-    if args.kernel == "cg":
-        res = t.solve_cg_dev(b.data_ptr(), x.data_ptr(), 1e-10, 40000, o)
+    if args.kernel in ("cg", "pcg"):
+        fn = t.solve_cg_dev if args.kernel == "cg" else t.solve_pcg_dev
+        res = fn(b.data_ptr(), x.data_ptr(), 1e-10, 40000, o)
         if args.trace > 0:
             tr = t.trace(args.trace).astype(np.float64)
             tr = tr[(tr[:, 0] > 0) & (tr[:, 6] > 0)]

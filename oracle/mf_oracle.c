@@ -411,6 +411,45 @@ int mfo_cg(const mfo_tiles *t, const double *b, double *x, double tol, int maxit
     return it;
 }
 
+/* Jacobi-preconditioned CG: KSPCG with PCJACOBI as in the "jpcg" runs of the
+ * reference's PETSc comparison (PC/PETSc/src/ksp/ksp/impls/cg/cg.c:112-380,
+ * unpreconditioned-norm stop test as test_a100.sh asks): z = r / a_ii,
+ * alpha = (r.z) / (d.q), beta = (r.z)_new / (r.z)_old, d = z + beta d, stop on
+ * ||r|| / ||b|| <= tol. diag[i] = a_ii (0 leaves the row unscaled). */
+int mfo_pcg_jacobi(const mfo_tiles *t, const double *diag, const double *b, double *x, double tol,
+                   int maxiter, double *rel_res) {
+    const int n = t->rowA;
+    double *r = (double *)malloc(sizeof(double) * (size_t)n);
+    double *z = (double *)malloc(sizeof(double) * (size_t)n);
+    double *d = (double *)malloc(sizeof(double) * (size_t)n);
+    double *q = (double *)malloc(sizeof(double) * (size_t)n);
+    double *minv = (double *)malloc(sizeof(double) * (size_t)n);
+    for (int i = 0; i < n; ++i) minv[i] = diag[i] != 0.0 ? 1.0 / diag[i] : 1.0;
+    mfo_blockspmv(t, x, q, NULL, NULL, NULL);
+    for (int i = 0; i < n; ++i) { r[i] = b[i] - q[i]; z[i] = minv[i] * r[i]; d[i] = z[i]; }
+    const double bn = sqrt(mfo_dot(n, b, b));
+    double rz = mfo_dot(n, r, z);
+    double rel = bn > 0 ? sqrt(mfo_dot(n, r, r)) / bn : 0.0;
+    int it = 0;
+    while (it < maxiter && rel > tol) {
+        mfo_blockspmv(t, d, q, NULL, NULL, NULL);
+        const double alpha = rz / mfo_dot(n, d, q);
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < n; ++i) { x[i] += alpha * d[i]; r[i] -= alpha * q[i]; z[i] = minv[i] * r[i]; }
+        const double rzold = rz;
+        rz = mfo_dot(n, r, z);
+        ++it;
+        rel = sqrt(mfo_dot(n, r, r)) / bn;
+        if (rel <= tol) break;
+        const double beta = rz / rzold;
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < n; ++i) d[i] = z[i] + beta * d[i];
+    }
+    if (rel_res) *rel_res = rel;
+    free(r); free(z); free(d); free(q); free(minv);
+    return it;
+}
+
 int mfo_bicgstab(const mfo_tiles *t, const double *b, double *x, double tol, int maxiter,
                  double *rel_res) {
     const int n = t->rowA;

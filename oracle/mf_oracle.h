@@ -66,6 +66,11 @@ double mfo_dot(int n, const double *a, const double *b);
 int mfo_cg(const mfo_tiles *t, const double *b, double *x, double tol, int maxiter,
            double *rel_res);
 
+/* Jacobi-preconditioned CG (KSPCG + PCJACOBI, PETSc/src/ksp/ksp/impls/cg/cg.c:112-380);
+ * diag[i] = a_ii. Stops on the unpreconditioned ||r|| / ||b|| <= tol. */
+int mfo_pcg_jacobi(const mfo_tiles *t, const double *diag, const double *b, double *x, double tol,
+                   int maxiter, double *rel_res);
+
 /* BiCGSTAB of Mille-feuille_BiCGSTAB_NVIDIA.cu:787-1061 / cuSPARSE_BiCGSTAB.cu:579-666. */
 int mfo_bicgstab(const mfo_tiles *t, const double *b, double *x, double tol, int maxiter,
                  double *rel_res);

@@ -55,6 +55,8 @@ def lib():
         L.mfo_dot.restype = C.c_double
         L.mfo_cg.argtypes = [C.POINTER(MfoTiles), _p, _p, C.c_double, _i, C.POINTER(C.c_double)]
         L.mfo_cg.restype = _i
+        L.mfo_pcg_jacobi.argtypes = [C.POINTER(MfoTiles), _p, _p, _p, C.c_double, _i, C.POINTER(C.c_double)]
+        L.mfo_pcg_jacobi.restype = _i
         L.mfo_bicgstab.argtypes = [C.POINTER(MfoTiles), _p, _p, C.c_double, _i, C.POINTER(C.c_double)]
         L.mfo_bicgstab.restype = _i
         L.mfo_fp8_e4m3_encode.argtypes = [C.c_double]
@@ -231,6 +233,14 @@ class OracleTiles:
         x = np.zeros(self.sizes["rowA"]) if x0 is None else np.array(x0, np.float64)
         rel = C.c_double()
         it = lib().mfo_cg(C.byref(self.t), _ptr(b), _ptr(x), tol, maxiter, C.byref(rel))
+        return it, x, rel.value
+
+    def pcg_jacobi(self, diag, b, tol, maxiter, x0=None):
+        diag = np.ascontiguousarray(diag, np.float64)
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(self.sizes["rowA"]) if x0 is None else np.array(x0, np.float64)
+        rel = C.c_double()
+        it = lib().mfo_pcg_jacobi(C.byref(self.t), _ptr(diag), _ptr(b), _ptr(x), tol, maxiter, C.byref(rel))
         return it, x, rel.value
 
     def bicgstab(self, b, tol, maxiter, x0=None):

@@ -124,3 +124,27 @@ def test_bounded_wait_times_out_and_context_survives(mf):
     # the context is still usable
     x, res = t.solve_cg(A.b(), tol=1e-10)
     assert res["status"] == 0
+
+
+@pytest.mark.parametrize("maker", ["varpoisson3d_16", "varpoisson3d_24", "poisson2d_96"])
+def test_jacobi_pcg_iterations_match_oracle(mf, O, maker):
+    """The fused Jacobi PCG against the oracle's KSPCG + PCJACOBI restatement:
+    iterations within +-2 % and the true residual at the tolerance."""
+    kind, size = maker.rsplit("_", 1)
+    size = int(size)
+    A = mf.Matrix.varpoisson3d(size) if kind == "varpoisson3d" else mf.Matrix.poisson2d(size)
+    n = A.n
+    rp, ci, v = A.csr()
+    diag = np.zeros(n)
+    for i in range(n):
+        cols = ci[rp[i]:rp[i + 1]]
+        diag[i] = v[rp[i]:rp[i + 1]][cols == i].sum()
+    b = A.b()
+    t = mf.Tiles(A)
+    x, res = t.solve_pcg(b, tol=1e-10, maxiter=20000)
+    o = O.OracleTiles(n, n, rp, ci, v)
+    it_o, _, _ = o.pcg_jacobi(diag, b, 1e-10, 20000)
+    assert res["status"] == 0, res
+    assert abs(res["iterations"] - it_o) <= max(2, 0.02 * it_o), (res["iterations"], it_o)
+    M = _csr_mat(rp, ci, v, n)
+    assert np.linalg.norm(b - M @ x) / np.linalg.norm(b) <= 2e-10
