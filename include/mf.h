@@ -277,6 +277,24 @@ int mf_trace(const mf_tiles *t, unsigned long long *out, int max_iters);
 int mf_true_residual(mf_tiles *t, const double *b_dev, const double *x_dev,
                      double *rel);
 
+/* ---- memory-cost report (Memory-Cost/memory_Mille_feillue.cu:659-921) ---- */
+typedef struct {
+    double csr_bytes;            /* CSR as the cuSPARSE study counts it:
+                                    (n+1)*4 + nnz*(4 + 8)                      */
+    double tile_index_bytes;     /* the reference tally of the tile metadata,
+                                    row compression and column bytes          */
+    double tile_value_bytes[4];  /* value bytes per precision MF_PREC_* of the
+                                    level-0 mix (all FP64 without a mixed
+                                    layout)                                    */
+    double tile_total_bytes;     /* index + value bytes (the study's memory_MB
+                                    x 2^20)                                    */
+    double slab_bytes_fp64;      /* this library's FP64 slab layout           */
+    double slab_bytes_mixed;     /* its mixed layouts, all levels             */
+    double workspace_bytes;      /* solver workspace currently held           */
+    double device_bytes;         /* every device allocation of the handle     */
+} mf_memory_cost;
+int mf_memory_report(const mf_tiles *t, mf_memory_cost *out);
+
 /* ---- learned precision selector (MF_MODE_MIXED_MLP) --------------------- */
 /* An MLP 6 -> 64 -> 64 -> 4 (ReLU) over per-tile features; its classes are
  * the tile precisions MF_PREC_*. Features: f0 = log10 max|a_ij|/sqrt(a_ii

@@ -76,6 +76,12 @@ class MfResult(C.Structure):
         }
 
 
+class MfMemoryReport(C.Structure):
+    _fields_ = [("csr_bytes", _d), ("tile_index_bytes", _d), ("tile_value_bytes", _d * 4),
+                ("tile_total_bytes", _d), ("slab_bytes_fp64", _d), ("slab_bytes_mixed", _d),
+                ("workspace_bytes", _d), ("device_bytes", _d)]
+
+
 class MfTileInfo(C.Structure):
     _fields_ = [(n, _i) for n in ("rowA", "colA", "tilem", "tilen", "tilenum", "csrsize", "csrptrlen",
                                   "cnt_non_new", "nslabs", "nctas")] + [
@@ -113,7 +119,7 @@ EXPORTED = [
     "mf_batch_solve_cg_each_dev", "mf_batch_results", "mf_batch_info", "mf_batch_free",
     "mf_solve_cg_dev_noalloc", "mf_mlp_set_weights", "mf_mlp_get_weights", "mf_tiles_features",
     "mf_tiles_select_mlp", "mf_mlp_forward_dev", "mf_mlp_grad_dev", "mf_mlp_train_dev", "mf_solve_pcg",
-    "mf_solve_pcg_dev",
+    "mf_solve_pcg_dev", "mf_memory_report",
 ]
 MLP_WEIGHTS = 4868
 MLP_WEIGHTS_PATH = os.path.join(_HERE, "mlp_weights.bin")
@@ -169,6 +175,7 @@ def lib():
               "mf_solve_cg_dev_noalloc"):
         getattr(L, f).argtypes = [_p, _p, _p, _d, _i, C.POINTER(MfOptions), C.POINTER(MfResult)]
     L.mf_true_residual.argtypes = [_p, _p, _p, C.POINTER(_d)]
+    L.mf_memory_report.argtypes = [_p, C.POINTER(MfMemoryReport)]
     L.mf_mlp_set_weights.argtypes = [_p]
     L.mf_mlp_get_weights.argtypes = [_p]
     L.mf_tiles_features.argtypes = [_p, _p]
@@ -356,6 +363,14 @@ class Tiles:
             load_mlp_weights()  # the packaged selector, unless the caller set one
         _check(lib().mf_encode(C.byref(c), C.byref(o), C.byref(self.h)), "mf_encode")
         self.opts = o
+
+    def memory_report(self):
+        """Memory cost of the tile format vs CSR (the reference's study) and the device bytes held."""
+        r = MfMemoryReport()
+        _check(lib().mf_memory_report(self.h, C.byref(r)), "mf_memory_report")
+        d = {f: getattr(r, f) for f, _ in r._fields_}
+        d["tile_value_bytes"] = list(r.tile_value_bytes)
+        return d
 
     def features(self):
         """Selector features f0..f5 of every tile, shape (tilenum, 6)."""

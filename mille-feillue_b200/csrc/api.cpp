@@ -153,6 +153,54 @@ int mf_tiles_info(const mf_tiles *t, mf_tile_info *info) {
     return MF_OK;
 }
 
+extern "C++" {
+namespace {
+template <class T>
+double dev_bytes(const DevArray<T> &a) {
+    return (double)a.n * sizeof(T);
+}
+double layout_dev_bytes(const Layout &L) {
+    return dev_bytes(L.slabs) + dev_bytes(L.head) + dev_bytes(L.cta_slab) + dev_bytes(L.cta_rb) +
+           dev_bytes(L.cta_dep) + dev_bytes(L.prec_dev) + dev_bytes(L.scale_dev);
+}
+}  // namespace
+}  // extern "C++"
+
+// The reference's memory-cost study (Memory-Cost/memory_Mille_feillue.cu)
+// counts the tile metadata (:659-668), the row-compression and per-entry
+// column bytes (:859-863) and the value bytes of the precision mix (:916);
+// its cuSPARSE counterpart counts CSR as (n+1) + nnz int32 and nnz FP64
+// values (memory_cuSPARSE.cu:189-191). The same tallies here, for the
+// level-0 precision mix, beside what this handle actually holds on the GPU.
+int mf_memory_report(const mf_tiles *t, mf_memory_cost *r) {
+    if (!t || !r) return MF_ERR_ARG;
+    std::memset(r, 0, sizeof *r);
+    const double tn = t->tilenum, tm = t->tilem;
+    r->csr_bytes = (double)(t->rowA + 1) * 4 + (double)t->csrsize * (4 + 8);
+    r->tile_index_bytes = (tm + 1) * 4 + tn * 4 + (tn + 1) * 1 + (tn + 1) * 4 + (tn + 1) * 4 + (tn + 3) * 4 +
+                          2.0 * (t->cnt_non_new + 1) + tn + (double)t->csrsize + tn * 4;
+    const std::vector<uint8_t> *prec = (t->mixed_ready && t->Lmix[0].built) ? &t->Lmix[0].prec : nullptr;
+    for (int k = 0; k < t->tilenum; ++k) {
+        const int p = prec ? (*prec)[k] : MF_PREC_FP64;
+        r->tile_value_bytes[p] += (double)t->h_tile_nnz[k] * prec_width(p);
+    }
+    r->tile_total_bytes = r->tile_index_bytes;
+    for (int p = 0; p < 4; ++p) r->tile_total_bytes += r->tile_value_bytes[p];
+    r->slab_bytes_fp64 = (double)t->L64.bytes;
+    for (int l = 0; l < MF_NLEVELS; ++l)
+        if (t->Lmix[l].built) r->slab_bytes_mixed += (double)t->Lmix[l].bytes;
+    double d = dev_bytes(t->tile_ptr) + dev_bytes(t->tile_col) + dev_bytes(t->tile_off) + dev_bytes(t->csrptr_off) +
+               dev_bytes(t->val) + dev_bytes(t->val_low) + dev_bytes(t->col) + dev_bytes(t->ptr) +
+               dev_bytes(t->blknnznnz) + dev_bytes(t->nonzero_row_new) + dev_bytes(t->tile_rowidx) +
+               dev_bytes(t->block_signal) + dev_bytes(t->blockrowid_new) + dev_bytes(t->blockcsr_ptr_new) +
+               dev_bytes(t->diag) + layout_dev_bytes(t->L64);
+    for (int l = 0; l < MF_NLEVELS; ++l) d += layout_dev_bytes(t->Lmix[l]);
+    r->workspace_bytes = dev_bytes(t->ws) + dev_bytes(t->sync) + dev_bytes(t->xpad) + dev_bytes(t->x32buf) +
+                         dev_bytes(t->trace);
+    r->device_bytes = d + r->workspace_bytes;
+    return MF_OK;
+}
+
 int mf_tiles_export(const mf_tiles *t, mf_tile_arrays *h) {
     if (!t || !h) return MF_ERR_ARG;
     const size_t tn = (size_t)t->tilenum;

@@ -151,3 +151,26 @@ def test_spmv_full_size_varpoisson_128(mf, O):
     assert np.allclose(y, A.b(), rtol=1e-12, atol=1e-9)
     o = O.OracleTiles(n, n, rp, ci, v)
     assert np.array_equal(y, o.spmv(x))
+
+
+def test_memory_report_tallies(mf):
+    """The reference's memory-cost tallies for an FP64 and a mixed encoding,
+    and the device bytes held by the handle."""
+    A = mf.Matrix.varpoisson3d(20)
+    n, nnz = A.n, A.nnz
+    t64 = mf.Tiles(A)
+    r = t64.memory_report()
+    inf = t64.info()
+    assert r["csr_bytes"] == (n + 1) * 4 + nnz * 12
+    assert r["tile_value_bytes"] == [8.0 * nnz, 0.0, 0.0, 0.0]
+    tn, tm = inf["tilenum"], inf["tilem"]
+    idx = ((tm + 1) * 4 + tn * 4 + (tn + 1) + 2 * (tn + 1) * 4 + (tn + 3) * 4 + 2 * (inf["cnt_non_new"] + 1) + tn
+           + nnz + tn * 4)
+    assert r["tile_index_bytes"] == idx
+    assert r["tile_total_bytes"] == idx + 8.0 * nnz
+    assert r["slab_bytes_fp64"] == inf["layout_bytes"] and r["slab_bytes_mixed"] == 0
+    assert r["device_bytes"] > r["slab_bytes_fp64"] + 8 * nnz
+    tm_ = mf.Tiles(A, mf.options(precision_mode=mf.MODE_FIXED, fixed_precision=mf.PREC_FP16))
+    rm = tm_.memory_report()
+    assert rm["tile_value_bytes"] == [0.0, 0.0, 2.0 * nnz, 0.0]
+    assert rm["slab_bytes_mixed"] > 0
