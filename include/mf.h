@@ -277,6 +277,23 @@ int mf_trace(const mf_tiles *t, unsigned long long *out, int max_iters);
 int mf_true_residual(mf_tiles *t, const double *b_dev, const double *x_dev,
                      double *rel);
 
+/* ---- autotuner (no reference counterpart) ------------------------------- */
+/* The tile shape is the reference's 16x16 (the bit-exact contract); what is
+ * tuned is the slab geometry of the solver layouts: bytes per slab (24, 32,
+ * 40 KB: the copy-ring stage) x row blocks per slab (16, 30, 60). Every
+ * candidate re-plans the handle's FP64 and mixed layouts (no re-encode) and
+ * times the SpMV the solvers run (the mixed level 0 when present, else
+ * FP64) over `reps` launches; the handle keeps the fastest. Results do not
+ * depend on the choice (the SpMV is bit-exact for every geometry).           */
+typedef struct {
+    int slab_bytes, rb_per_slab;   /* the choice (now in the handle)           */
+    double ms_best, ms_default;    /* SpMV time of the choice / of the default */
+    int candidates;
+    int cand_slab_bytes[16], cand_rb_per_slab[16];
+    double cand_ms[16];
+} mf_tune_result;
+int mf_tiles_autotune(mf_tiles *t, int reps, mf_tune_result *out);
+
 /* ---- memory-cost report (Memory-Cost/memory_Mille_feillue.cu:659-921) ---- */
 typedef struct {
     double csr_bytes;            /* CSR as the cuSPARSE study counts it:

@@ -76,6 +76,11 @@ class MfResult(C.Structure):
         }
 
 
+class MfTuneResult(C.Structure):
+    _fields_ = [("slab_bytes", _i), ("rb_per_slab", _i), ("ms_best", _d), ("ms_default", _d), ("candidates", _i),
+                ("cand_slab_bytes", _i * 16), ("cand_rb_per_slab", _i * 16), ("cand_ms", _d * 16)]
+
+
 class MfMemoryReport(C.Structure):
     _fields_ = [("csr_bytes", _d), ("tile_index_bytes", _d), ("tile_value_bytes", _d * 4),
                 ("tile_total_bytes", _d), ("slab_bytes_fp64", _d), ("slab_bytes_mixed", _d),
@@ -119,7 +124,7 @@ EXPORTED = [
     "mf_batch_solve_cg_each_dev", "mf_batch_results", "mf_batch_info", "mf_batch_free",
     "mf_solve_cg_dev_noalloc", "mf_mlp_set_weights", "mf_mlp_get_weights", "mf_tiles_features",
     "mf_tiles_select_mlp", "mf_mlp_forward_dev", "mf_mlp_grad_dev", "mf_mlp_train_dev", "mf_solve_pcg",
-    "mf_solve_pcg_dev", "mf_memory_report",
+    "mf_solve_pcg_dev", "mf_memory_report", "mf_tiles_autotune",
 ]
 MLP_WEIGHTS = 4868
 MLP_WEIGHTS_PATH = os.path.join(_HERE, "mlp_weights.bin")
@@ -176,6 +181,7 @@ def lib():
         getattr(L, f).argtypes = [_p, _p, _p, _d, _i, C.POINTER(MfOptions), C.POINTER(MfResult)]
     L.mf_true_residual.argtypes = [_p, _p, _p, C.POINTER(_d)]
     L.mf_memory_report.argtypes = [_p, C.POINTER(MfMemoryReport)]
+    L.mf_tiles_autotune.argtypes = [_p, _i, C.POINTER(MfTuneResult)]
     L.mf_mlp_set_weights.argtypes = [_p]
     L.mf_mlp_get_weights.argtypes = [_p]
     L.mf_tiles_features.argtypes = [_p, _p]
@@ -363,6 +369,15 @@ class Tiles:
             load_mlp_weights()  # the packaged selector, unless the caller set one
         _check(lib().mf_encode(C.byref(c), C.byref(o), C.byref(self.h)), "mf_encode")
         self.opts = o
+
+    def autotune(self, reps=20):
+        """Picks the slab geometry with the fastest solver SpMV; the handle keeps it."""
+        r = MfTuneResult()
+        _check(lib().mf_tiles_autotune(self.h, reps, C.byref(r)), "mf_tiles_autotune")
+        k = r.candidates
+        return {"slab_bytes": r.slab_bytes, "rb_per_slab": r.rb_per_slab, "ms_best": r.ms_best,
+                "ms_default": r.ms_default,
+                "candidates": [(r.cand_slab_bytes[i], r.cand_rb_per_slab[i], r.cand_ms[i]) for i in range(k)]}
 
     def memory_report(self):
         """Memory cost of the tile format vs CSR (the reference's study) and the device bytes held."""

@@ -598,6 +598,85 @@ static int solve_dev(mf_tiles *t, int kind, const double *b_dev, double *x_dev, 
     return rc;
 }
 
+// Re-plans the handle's layouts (FP64 and, when present, the mixed levels)
+// with the candidate slab geometry and returns the time of the SpMV the
+// solvers run (the mixed level 0 when present, else FP64), averaged over
+// reps launches.
+static int tune_candidate(mf_tiles *t, int slab_bytes, int rbps, int reps, double *ms) {
+    t->opt.slab_bytes = slab_bytes;
+    t->opt.rb_per_slab = rbps;
+    int G = 0, rc;
+    if ((rc = kernel_config(t, &G)) != MF_OK) return rc;
+    std::vector<uint8_t> prec(t->tilenum, MF_PREC_FP64);
+    if ((rc = build_layout(t, t->L64, prec, 0)) != MF_OK) return rc;
+    const bool mixed = t->opt.precision_mode != MF_MODE_FP64;
+    if (mixed && (rc = build_mixed_levels(t, 0)) != MF_OK) return rc;
+    const int level = (mixed && t->mixed_ready) ? 0 : -1;
+    if ((rc = ensure_workspace(t)) != MF_OK) return rc;
+    WsView v = ws_view(t);
+    const size_t n16 = (size_t)t->tilen * 16;
+    MF_CUDA_TRY(cudaMemsetAsync(v.x, 0, sizeof(double) * n16));
+    const void *xs;
+    if ((rc = prepare_x(t, level, v.x, &xs)) != MF_OK) return rc;
+    if ((rc = launch_spmv(t, level, xs, v.q, 1, 0)) != MF_OK) return rc;  // warm-up
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, 0);
+    for (int i = 0; i < reps && rc == MF_OK; ++i) rc = launch_spmv(t, level, xs, v.q, 1, 0);
+    cudaEventRecord(e1, 0);
+    cudaError_t ce = cudaEventSynchronize(e1);
+    float f = 0.f;
+    cudaEventElapsedTime(&f, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    if (ce != cudaSuccess) {
+        set_last_error(cudaGetErrorString(ce));
+        return MF_ERR_CUDA;
+    }
+    *ms = f / reps;
+    return MF_OK;
+}
+
+int mf_tiles_autotune(mf_tiles *t, int reps, mf_tune_result *out) {
+    if (!t || !out) return MF_ERR_ARG;
+    if (reps <= 0) reps = 20;
+    MF_CUDA_TRY(cudaSetDevice(t->opt.device));
+    std::memset(out, 0, sizeof *out);
+    static const int kSlab[] = {24576, 32768, 40960};
+    static const int kRb[] = {16, 30, 60};
+    double best = 1e30;
+    int bsb = 0, brb = 0;
+    for (int sb : kSlab)
+        for (int rb : kRb) {
+            double ms = 0;
+            const int rc = tune_candidate(t, sb, rb, reps, &ms);
+            if (rc == MF_ERR_ARG) continue;  // does not fit shared memory
+            if (rc) return rc;
+            const int k = out->candidates++;
+            out->cand_slab_bytes[k] = sb;
+            out->cand_rb_per_slab[k] = rb;
+            out->cand_ms[k] = ms;
+            if (sb == SLAB_MAX_DEFAULT && rb == (t->opt.precision_mode != MF_MODE_FP64 ? RB_PER_SLAB_MAX
+                                                                                        : RB_PER_SLAB_X64))
+                out->ms_default = ms;
+            if (ms < best) {
+                best = ms;
+                bsb = sb;
+                brb = rb;
+            }
+        }
+    if (out->candidates == 0) return MF_ERR_RESIDENCY;
+    double ms = 0;
+    int rc = tune_candidate(t, bsb, brb, reps, &ms);  // leave the handle on the choice
+    if (rc) return rc;
+    out->slab_bytes = bsb;
+    out->rb_per_slab = brb;
+    out->ms_best = best;
+    return MF_OK;
+}
+
 int mf_solve_cg_dev(mf_tiles *t, const double *b, double *x, double tol, int maxiter, const mf_options *opt,
                     mf_result *res) {
     return solve_dev(t, 0, b, x, tol, maxiter, opt, res);

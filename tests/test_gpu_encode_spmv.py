@@ -174,3 +174,38 @@ def test_memory_report_tallies(mf):
     rm = tm_.memory_report()
     assert rm["tile_value_bytes"] == [0.0, 0.0, 2.0 * nnz, 0.0]
     assert rm["slab_bytes_mixed"] > 0
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_autotune_keeps_results_and_picks_the_fastest(mf, mode):
+    """The tuner times every slab geometry, leaves the handle on the fastest,
+    and the SpMV and the solve give the same results afterwards."""
+    import torch
+
+    A = mf.Matrix.varpoisson3d(40)
+    o = mf.options() if mode == "fp64" else mf.options(precision_mode=mf.MODE_MIXED_RULE)
+    t = mf.Tiles(A, o)
+    x = np.random.default_rng(8).standard_normal(A.n)
+    xd = torch.tensor(x, device="cuda")
+    y0 = torch.zeros_like(xd)
+    y1 = torch.zeros_like(xd)
+    level = -1 if mode == "fp64" else 0
+    if level < 0:
+        t.spmv_dev(xd.data_ptr(), y0.data_ptr())
+    else:
+        t.spmv_level_dev(0, xd.data_ptr(), y0.data_ptr())
+    _, r0 = t.solve_cg(A.b(), tol=1e-10, maxiter=20000)
+    tr = t.autotune(reps=10)
+    assert len(tr["candidates"]) == 9
+    assert tr["ms_best"] == min(c[2] for c in tr["candidates"]) and tr["ms_default"] > 0
+    assert (tr["slab_bytes"], tr["rb_per_slab"]) in [(c[0], c[1]) for c in tr["candidates"]]
+    if level < 0:
+        t.spmv_dev(xd.data_ptr(), y1.data_ptr())
+    else:
+        t.spmv_level_dev(0, xd.data_ptr(), y1.data_ptr())
+    assert torch.equal(y0, y1)  # bit-exact for every geometry
+    _, r1 = t.solve_cg(A.b(), tol=1e-10, maxiter=20000)
+    assert r1["status"] == 0 and r1["rel_residual_true"] <= 1e-10
+    # the dot products' rounding follows the row-to-thread mapping, which the
+    # slab grouping changes: iteration counts may move by a little
+    assert abs(r1["iterations"] - r0["iterations"]) <= max(2, 0.02 * r0["iterations"])
