@@ -277,6 +277,24 @@ int mf_trace(const mf_tiles *t, unsigned long long *out, int max_iters);
 int mf_true_residual(mf_tiles *t, const double *b_dev, const double *x_dev,
                      double *rel);
 
+/* ---- CG on up to 16 right-hand sides at once (no reference counterpart) -- */
+/* k <= 16 independent CG recurrences (each its own alpha, beta and stop
+ * test, the reference's CG) sharing every matrix-panel product, so the
+ * matrix streams once per iteration for all of them. B, X: n x k column-major
+ * (column j = right-hand side j; X holds x0 on entry). The SpMM keeps
+ * blockspmv_cpu's order per column (FP64); the CSR columns must ascend within
+ * each row. Per right-hand side: iterations and recursive relative residual;
+ * *time_ms = device time of the whole call. MF_ERR_NOT_CONVERGED if any
+ * column missed tol within maxiter.                                          */
+int mf_solve_cg_multi(const mf_csr *A, int k, const double *B_host,
+                      double *X_host, double tol, int maxiter,
+                      int *iterations, double *rel_residual, double *time_ms);
+int mf_solve_cg_multi_dev(int n, const int *row_ptr_dev, const int *col_idx_dev,
+                          const double *val_dev, int k, const double *B_dev,
+                          double *X_dev, double tol, int maxiter,
+                          int *iterations, double *rel_residual,
+                          double *time_ms);
+
 /* ---- autotuner (no reference counterpart) ------------------------------- */
 /* The tile shape is the reference's 16x16 (the bit-exact contract); what is
  * tuned is the slab geometry of the solver layouts: bytes per slab (24, 32,

@@ -124,7 +124,7 @@ EXPORTED = [
     "mf_batch_solve_cg_each_dev", "mf_batch_results", "mf_batch_info", "mf_batch_free",
     "mf_solve_cg_dev_noalloc", "mf_mlp_set_weights", "mf_mlp_get_weights", "mf_tiles_features",
     "mf_tiles_select_mlp", "mf_mlp_forward_dev", "mf_mlp_grad_dev", "mf_mlp_train_dev", "mf_solve_pcg",
-    "mf_solve_pcg_dev", "mf_memory_report", "mf_tiles_autotune",
+    "mf_solve_pcg_dev", "mf_memory_report", "mf_tiles_autotune", "mf_solve_cg_multi", "mf_solve_cg_multi_dev",
 ]
 MLP_WEIGHTS = 4868
 MLP_WEIGHTS_PATH = os.path.join(_HERE, "mlp_weights.bin")
@@ -182,6 +182,8 @@ def lib():
     L.mf_true_residual.argtypes = [_p, _p, _p, C.POINTER(_d)]
     L.mf_memory_report.argtypes = [_p, C.POINTER(MfMemoryReport)]
     L.mf_tiles_autotune.argtypes = [_p, _i, C.POINTER(MfTuneResult)]
+    L.mf_solve_cg_multi.argtypes = [C.POINTER(MfCsr), _i, _p, _p, _d, _i, _p, _p, C.POINTER(_d)]
+    L.mf_solve_cg_multi_dev.argtypes = [_i, _p, _p, _p, _i, _p, _p, _d, _i, _p, _p, C.POINTER(_d)]
     L.mf_mlp_set_weights.argtypes = [_p]
     L.mf_mlp_get_weights.argtypes = [_p]
     L.mf_tiles_features.argtypes = [_p, _p]
@@ -218,6 +220,22 @@ def _check(rc, what):
 
 def _ptr(a):
     return a.ctypes.data_as(_p)
+
+
+def solve_cg_multi(matrix, B, X0=None, tol=1e-10, maxiter=10000):
+    """CG on the k <= 16 columns of B (n x k) at once, sharing each SpMM.
+    Returns (X, iterations[k], rel_residual[k], device ms)."""
+    B = np.asfortranarray(B, dtype=np.float64)
+    n, k = B.shape
+    X = np.asfortranarray(np.zeros((n, k)) if X0 is None else X0, dtype=np.float64)
+    it = np.zeros(k, np.int32)
+    rel = np.zeros(k)
+    ms = _d()
+    rc = lib().mf_solve_cg_multi(C.byref(matrix.csr_struct()), k, _ptr(B), _ptr(X), tol, maxiter, _ptr(it),
+                                 _ptr(rel), C.byref(ms))
+    if rc not in (MF_OK, MF_ERR_NOT_CONVERGED):
+        _check(rc, "mf_solve_cg_multi")
+    return X, it, rel, ms.value
 
 
 def set_mlp_weights(w):
