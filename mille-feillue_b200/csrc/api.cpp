@@ -371,7 +371,7 @@ int mf_spmv_bench(const mf_tiles *t, const double *x, double *y, int reps, doubl
 // --------------------------------------------------------------- solvers
 static int ensure_workspace(mf_tiles *t) {
     const size_t n16 = (size_t)t->tilem * 16;
-    const size_t need = 8 * n16 + 2 * 4 * (size_t)t->G + 64;
+    const size_t need = 9 * n16 + 2 * 4 * (size_t)t->G + 64;  // 8 vectors + the FP32 pair
     if (t->ws.n < need) {
         if (t->ws.alloc(need)) return MF_ERR_NOMEM;
     }
@@ -384,6 +384,7 @@ static int ensure_workspace(mf_tiles *t) {
 
 struct WsView {
     double *b, *x, *r, *d, *q, *s, *t, *rh, *partial;
+    float *p32, *s32;  // FP32 SpMV inputs of the mixed BiCGSTAB
     DevResult *res;
 };
 
@@ -399,7 +400,9 @@ static WsView ws_view(mf_tiles *t) {
     v.s = w + 5 * n16;
     v.t = w + 6 * n16;
     v.rh = w + 7 * n16;
-    v.partial = w + 8 * n16;
+    v.p32 = reinterpret_cast<float *>(w + 8 * n16);
+    v.s32 = v.p32 + n16;
+    v.partial = w + 9 * n16;
     v.res = reinterpret_cast<DevResult *>(t->sync.p + sync_words(t->G));
     return v;
 }
@@ -432,7 +435,7 @@ static int solve_dev_once(mf_tiles *t, int kind, const double *b_dev, double *x_
     WsView v = ws_view(t);
     const size_t n16 = (size_t)t->tilem * 16;
     const int n = t->rowA;
-    MF_CUDA_TRY(cudaMemsetAsync(t->ws.p, 0, sizeof(double) * 8 * n16));
+    MF_CUDA_TRY(cudaMemsetAsync(t->ws.p, 0, sizeof(double) * 9 * n16));
     MF_CUDA_TRY(cudaMemcpyAsync(v.b, b_dev, sizeof(double) * n, cudaMemcpyDeviceToDevice));
     MF_CUDA_TRY(cudaMemcpyAsync(v.x, x_dev, sizeof(double) * n, cudaMemcpyDeviceToDevice));
     MF_CUDA_TRY(cudaMemsetAsync(t->sync.p, 0, sizeof(uint32_t) * t->sync.n));
@@ -449,6 +452,8 @@ static int solve_dev_once(mf_tiles *t, int kind, const double *b_dev, double *x_
     P.s = v.s;
     P.t = v.t;
     P.rh = v.rh;
+    P.p32 = v.p32;
+    P.s32 = v.s32;
     P.tol = tol;
     P.maxiter = maxiter;
     P.fixed_iterations = opt.fixed_iterations;
@@ -464,7 +469,7 @@ static int solve_dev_once(mf_tiles *t, int kind, const double *b_dev, double *x_
         P.trace_iters = ti;
         t->trace_iters = ti;
     }
-    const bool mixed = kind == 0 && opt.precision_mode != MF_MODE_FP64 && t->mixed_ready;
+    const bool mixed = (kind == 0 || kind == 1) && opt.precision_mode != MF_MODE_FP64 && t->mixed_ready;
     if (mixed) {
         int nl = 1;
         for (int l = 0; l < t->nlevels; ++l) {
@@ -497,7 +502,7 @@ static int solve_dev_once(mf_tiles *t, int kind, const double *b_dev, double *x_
         int rj = launch_jacobi_inv(n, (int)n16, t->diag.p, v.s, 0);
         if (rj) return rj;
     }
-    int launch_kind = kind == 2 ? 4 : (mixed && opt.reserved[2] != 1) ? 2 : kind;
+    int launch_kind = kind == 2 ? 4 : (mixed && kind == 0 && opt.reserved[2] != 1) ? 2 : kind;
     if (launch_kind == 2 && opt.reserved[5] != 1) {
         // x and r stay in tensor memory when every CTA's rows fit it
         int rows_max = 0;
@@ -538,16 +543,19 @@ static int solve_dev_once(mf_tiles *t, int kind, const double *b_dev, double *x_
     R.spmv_bytes = Lf->alg_bytes;
     for (int p = 0; p < 4; ++p) R.tile_frac[p] = Lf->tile_frac[p];
     R.iters_fp64 = dr.it_layout[0];
-    R.fell_back_fp64 = kind == 0 ? dr.pad : 0;
+    R.fell_back_fp64 = kind <= 1 ? dr.pad : 0;
     for (int l = 0; l < 3; ++l) {
         R.iters_level[l] = dr.it_layout[l + 1];
         R.spmv_bytes_level[l] = (mixed && t->Lmix[l].built) ? t->Lmix[l].alg_bytes : 0.0;
     }
     {
-        const double vec = (kind == 2 ? 72.0 : 56.0) * (double)n;  // PCG also reads 1/a_ii twice
+        // per iteration: CG one SpMV + 56 n, PCG + 16 n for 1/a_ii, BiCGSTAB
+        // two SpMVs + 88 n
+        const double vec = (kind == 1 ? 88.0 : kind == 2 ? 72.0 : 56.0) * (double)n;
+        const double nsp = kind == 1 ? 2.0 : 1.0;
         double tb = (double)(1 + dr.replacements) * (t->L64.alg_bytes + 16.0 * n);  // initial + replacements
-        tb += (double)dr.it_layout[0] * (t->L64.alg_bytes + vec);
-        for (int l = 0; l < 3; ++l) tb += (double)dr.it_layout[l + 1] * (R.spmv_bytes_level[l] + vec);
+        tb += (double)dr.it_layout[0] * (nsp * t->L64.alg_bytes + vec);
+        for (int l = 0; l < 3; ++l) tb += (double)dr.it_layout[l + 1] * (nsp * R.spmv_bytes_level[l] + vec);
         R.total_bytes = tb;
     }
     R.rel_residual_true = NAN;

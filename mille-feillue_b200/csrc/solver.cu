@@ -1622,20 +1622,29 @@ struct EpiDot2 {  // t = A s, ts += t*s, tt += t*t
     }
 };
 
+// MIXED: both SpMVs run on the low-precision layouts (FP32 copies of p and
+// s are their input on FP32-x layouts); x, r, p, s, t, v, the dots and the
+// scalars stay FP64. r is replaced by the FP64 true residual b - A x every
+// replace_every iterations and before the solve stops, rho = r^.r is
+// recomputed from it, and the levels and the FP64 fallback follow k_cg.
+template <bool MIXED>
 __global__ void __launch_bounds__(NTHREADS, 1) k_bicgstab(KParams P) {
     extern __shared__ __align__(128) uint8_t dyn[];
     __shared__ Smem S;
-    kernel_setup(P, S, 1);
+    kernel_setup(P, S, P.nlay);
     const int g = blockIdx.x, tid = threadIdx.x;
     Pipe pp;
     uint32_t phase = 0;
     const uint64_t vpol = policy_evict_last();
+    const int lay64 = 0;
+    int lay = MIXED ? P.start_layout : 0;
     const int rb_lo = P.lay[0].cta_rb[g], rb_hi = P.lay[0].cta_rb[g + 1];
     const int vlo = rb_lo * 16, vhi = rb_hi * 16;  // own rows, zero padded past rowA
     double *x = P.x, *r = P.r, *p = P.d, *v = P.q, *s = P.s, *t = P.t, *rh = P.rh;
+    float *p32 = P.p32, *s32 = P.s32;
     const double *b = P.b;
     EpiResidual er{b, r, 0.0, vpol};
-    if (!cta_spmv<false>(P, 0, x, S, dyn, pp, er)) return;
+    if (!cta_spmv<false>(P, lay64, x, S, dyn, pp, er)) return;
     __syncthreads();
     double bbp = 0.0, rhop = 0.0;
     MF_PAIRS(4, vlo, vhi, {
@@ -1649,6 +1658,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_bicgstab(KParams P) {
         MF_FOR_VB if (MF_LIVE(u, vhi)) {
             st2_hint(rh + 2 * MF_PI(u), rv[u], vpol);
             st2_hint(p + 2 * MF_PI(u), rv[u], vpol);
+            if (MIXED)
+                stf2_hint(p32 + 2 * MF_PI(u), make_float2(__double2float_rn(rv[u].x), __double2float_rn(rv[u].y)),
+                          vpol);
             bbp += bv[u].x * bv[u].x + bv[u].y * bv[u].y;
             rhop += rv[u].x * rv[u].x + rv[u].y * rv[u].y;
         }
@@ -1662,14 +1674,60 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_bicgstab(KParams P) {
     const double tol = P.tol;
     uint32_t ep = 1;
     publish(P, ep);
-    int it = 0, status = MF_OK;
+    int it = 0, status = MF_OK, repl = 0, switches = 0, fellback = 0;
+    int it_lay[KMAX_LAYOUTS] = {0, 0, 0, 0};
     double rel = bnorm > 0 ? sqrt(rr) / bnorm : 0.0;
+    double rr_best = rr;
+    bool pending = false;
     const bool fixed = P.fixed_iterations > 0;
     const int maxit = fixed ? P.fixed_iterations : P.maxiter;
-    while (it < maxit && (fixed || rel > tol)) {
-        if (!wait_deps(P, S, 0, ep)) return;
+    while (it < maxit && (fixed || rel > tol || pending)) {
+        if (MIXED && (pending || (P.replace_every > 0 && it > 0 && it % P.replace_every == 0))) {
+            // r = b - A x on the FP64 layout, rho = r^.r from it
+            if (!wait_deps(P, S, lay64, ep)) return;
+            EpiResidual e2{b, r, 0.0, vpol};
+            if (!cta_spmv<false>(P, lay64, x, S, dyn, pp, e2)) return;
+            double rhr = 0.0;
+            MF_PAIRS(4, vlo, vhi, {
+                double2 rv[_vb], hv[_vb];
+#pragma unroll
+                MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                    rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+                    hv[u] = ld2_hint(rh + 2 * MF_PI(u), vpol);
+                }
+#pragma unroll
+                MF_FOR_VB if (MF_LIVE(u, vhi)) rhr += rv[u].x * hv[u].x + rv[u].y * hv[u].y;
+            })
+            double c2[2] = {e2.rr, rhr}, d2[2];
+            if (!grid_sum<2>(P, S, c2, d2, phase)) return;
+            rr = d2[0];
+            rho = d2[1];
+            ++repl;
+            rel = bnorm > 0 ? sqrt(rr) / bnorm : 0.0;
+            if (pending) {
+                pending = false;
+                if (rel <= tol) break;
+            }
+            if (lay != lay64) {
+                if (rr < rr_best) rr_best = rr;
+                if (!(rr <= 1e4 * rr_best)) {
+                    lay = lay64;
+                    fellback = 1;
+                }
+                while (lay != lay64 && lay < P.nlay - 1 && rel < P.level_rel[lay]) {
+                    ++lay;
+                    ++switches;
+                }
+            }
+        }
+        if (it >= maxit) break;
+        ++it_lay[lay];
+        if (!wait_deps(P, S, lay, ep)) return;
         EpiDot ev{rh, v, 0.0, vpol};
-        if (!cta_spmv<false>(P, 0, p, S, dyn, pp, ev)) return;
+        bool ok;
+        if (MIXED && lay != lay64) ok = cta_spmv<true>(P, lay, P.lay[lay].x32 ? (const void *)p32 : p, S, dyn, pp, ev);
+        else ok = cta_spmv<false>(P, lay64, p, S, dyn, pp, ev);
+        if (!ok) return;
         double a1[1] = {ev.dot}, b1[1];
         if (!grid_sum<1>(P, S, a1, b1, phase)) return;
         if (!(b1[0] != 0.0) || !isfinite(b1[0])) {
@@ -1690,13 +1748,17 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_bicgstab(KParams P) {
                 o.x = rv[u].x - alpha * vv[u].x;
                 o.y = rv[u].y - alpha * vv[u].y;
                 st2_hint(s + 2 * MF_PI(u), o, vpol);
+                if (MIXED)
+                    stf2_hint(s32 + 2 * MF_PI(u), make_float2(__double2float_rn(o.x), __double2float_rn(o.y)), vpol);
             }
         })
         ++ep;
         publish(P, ep);
-        if (!wait_deps(P, S, 0, ep)) return;
+        if (!wait_deps(P, S, lay, ep)) return;
         EpiDot2 et{s, t, 0.0, 0.0, vpol};
-        if (!cta_spmv<false>(P, 0, s, S, dyn, pp, et)) return;
+        if (MIXED && lay != lay64) ok = cta_spmv<true>(P, lay, P.lay[lay].x32 ? (const void *)s32 : s, S, dyn, pp, et);
+        else ok = cta_spmv<false>(P, lay64, s, S, dyn, pp, et);
+        if (!ok) return;
         double a2[2] = {et.ts, et.tt}, b2[2];
         if (!grid_sum<2>(P, S, a2, b2, phase)) return;
         if (!(b2[1] != 0.0) || !isfinite(b2[1])) {
@@ -1738,7 +1800,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_bicgstab(KParams P) {
             status = MF_ERR_BREAKDOWN;
             break;
         }
-        if (!fixed && rel <= tol) break;
+        const bool stop = !fixed && rel <= tol;
+        if (stop && !(MIXED && P.true_check)) break;
+        if (stop) pending = true;  // confirm with the FP64 true residual (p still advances)
         const double beta = (rho1 * alpha) / (rho * omega);
         MF_PAIRS(4, vlo, vhi, {
             double2 rv[_vb], pv[_vb], vv[_vb];
@@ -1754,6 +1818,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_bicgstab(KParams P) {
                 o.x = rv[u].x + beta * (pv[u].x - omega * vv[u].x);
                 o.y = rv[u].y + beta * (pv[u].y - omega * vv[u].y);
                 st2_hint(p + 2 * MF_PI(u), o, vpol);
+                if (MIXED)
+                    stf2_hint(p32 + 2 * MF_PI(u), make_float2(__double2float_rn(o.x), __double2float_rn(o.y)), vpol);
             }
         })
         rho = rho1;
@@ -1764,13 +1830,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_bicgstab(KParams P) {
         if (status == MF_OK && !fixed && rel > tol) status = MF_ERR_NOT_CONVERGED;
         P.res->iterations = it;
         P.res->status = status;
-        P.res->replacements = 0;
-        P.res->level_switches = 0;
+        P.res->replacements = repl;
+        P.res->level_switches = switches;
         P.res->rr = rr;
         P.res->bb = bb;
-        P.res->final_layout = 0;
-        P.res->it_layout[0] = it;
-        for (int l = 1; l < KMAX_LAYOUTS; ++l) P.res->it_layout[l] = 0;
+        P.res->final_layout = lay;
+        for (int l = 0; l < KMAX_LAYOUTS; ++l) P.res->it_layout[l] = MIXED ? it_lay[l] : (l == 0 ? it : 0);
+        P.res->pad = fellback;
     }
 }
 
@@ -1991,7 +2057,8 @@ int kernel_config(mf_tiles *t, int *G_out) {
         set_last_error("slab_bytes too large: the stage ring does not fit shared memory");
         return MF_ERR_ARG;
     }
-    const void *kerns[] = {(const void *)k_cg<false>, (const void *)k_cg<true>, (const void *)k_bicgstab,
+    const void *kerns[] = {(const void *)k_cg<false>, (const void *)k_cg<true>, (const void *)k_bicgstab<false>,
+                           (const void *)k_bicgstab<true>,
                            (const void *)k_spmv<false>, (const void *)k_spmv<true>, (const void *)k_cgcg,
                            (const void *)k_batch_cg, (const void *)k_cgcg_tm, (const void *)k_pcg};
     int occ_min = 1 << 30;
@@ -2084,7 +2151,7 @@ int launch_solver(mf_tiles *t, int kind, KParams &P, cudaStream_t s) {
                     : kind == 2 ? (const void *)k_cgcg
                     : kind == 3 ? (const void *)k_cgcg_tm
                     : kind == 4 ? (const void *)k_pcg
-                                : (const void *)k_bicgstab;
+                                : (P.nlay > 1 ? (const void *)k_bicgstab<true> : (const void *)k_bicgstab<false>);
     MF_CUDA_TRY(cudaLaunchCooperativeKernel(k, dim3(t->G), dim3(NTHREADS), args, dyn, s));
     return MF_OK;
 }

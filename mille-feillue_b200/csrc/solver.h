@@ -47,6 +47,7 @@ struct KParams {
     uint32_t *sync;
     double *partial;
     double *x, *r, *d, *q, *s, *t, *rh;
+    float *p32, *s32;  // FP32 copies of the mixed BiCGSTAB's SpMV inputs
     const double *b;
     double tol;
     int maxiter, fixed_iterations, replace_every;
