@@ -344,6 +344,9 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_slabs(const SlabPlan *__r
                     pv[lane] = (uint8_t)__nv_cvt_double_to_fp8(v / (double)ps, __NV_SATFINITE, __NV_E4M3);
                 }
                 cursor_next(A, c);
+            } else if (lane < 16 && !gather) {
+                // padding entry: value 0 (the zeroed slab) at the zero slot
+                reinterpret_cast<uint16_t *>(idxb)[k * 16 + lane] = (uint16_t)(XZERO_OFF / (segbytes / 16u));
             }
             voff += 16u * prec_width(pp);
         }

@@ -110,9 +110,12 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
     if (KIND == LAYOUT_FP64) {
         const double *vals = reinterpret_cast<const double *>(blk + rb_vals_off(W, false, gather));
         if (!gather) {
+            // all W planes: padding entries add x(zero slot) * 0 = +0 to a sum
+            // that is never -0, which leaves it unchanged; the trip count is
+            // the same for the 16 lanes of the row block
             const uint16_t *idx = reinterpret_cast<const uint16_t *>(blk + rb_idx_off(W, false));
 #pragma unroll 4
-            for (int k = 0; k < len; ++k) {
+            for (int k = 0; k < W; ++k) {
                 const uint32_t id = idx[k * 16 + r];
                 const double v = vals[k * 16 + r];
                 const XT x = xstage[id & IDX16_POS];
@@ -178,7 +181,7 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
         if (!gather) {
             const uint16_t *idx = reinterpret_cast<const uint16_t *>(idxb);
 #pragma unroll 4
-            for (int k = 0; k < len; ++k) {
+            for (int k = 0; k < W; ++k) {
                 const uint32_t id = idx[k * 16 + r];
                 const float v = v32[k * 16 + r];
                 const XT x = xstage[id & IDX16_POS];
@@ -609,7 +612,11 @@ __device__ bool wait_deps(const KParams &P, Smem &S, int lay, uint32_t ep) {
 }
 
 __device__ void kernel_setup(const KParams &P, Smem &S, int nlay) {
+    extern __shared__ __align__(128) uint8_t dyn[];
     const int tid = threadIdx.x;
+    if (tid < STAGES)
+        *reinterpret_cast<uint4 *>(dyn + (size_t)tid * P.stage_stride + P.slab_area + XZERO_OFF) =
+            make_uint4(0u, 0u, 0u, 0u);
     if (tid == 0) {
         for (int k = 0; k < STAGES; ++k) {
             mbar_init(&S.full[k], 1);
@@ -1901,6 +1908,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_batch_cg(BatchParams B) {
     __shared__ int s_rng[4];
     KParams P0;  // only the fields kernel_setup reads
     P0.nlay = 0;
+    P0.stage_stride = B.stage_stride;
+    P0.slab_area = B.slab_area;
     kernel_setup(P0, S, 0);
     const int tid = threadIdx.x;
     const int grp = blockIdx.x / B.gs, rank = blockIdx.x % B.gs;
@@ -2053,7 +2062,8 @@ int kernel_config(mf_tiles *t, int *G_out) {
     const int dyn = dyn_smem(slab_max);
     int optin = 0;
     MF_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, t->device));
-    if (dyn + (int)sizeof(Smem) > optin) {
+    // static shared memory: Smem, plus the TMEM kernel's per-thread partials
+    if (dyn + (int)sizeof(Smem) + NTHREADS * 8 + 64 > optin) {
         set_last_error("slab_bytes too large: the stage ring does not fit shared memory");
         return MF_ERR_ARG;
     }

@@ -18,7 +18,8 @@ enum { SYNC_ARRIVE = 0, SYNC_ERROR = 32, SYNC_SITE = 33, SYNC_FLAGS = 64 };
 inline size_t sync_words(int G) { return (size_t)SYNC_FLAGS + (size_t)G * FLAG_STRIDE + 32; }
 
 inline int slab_area_of(int slab_max) { return (slab_max + 127) & ~127; }
-inline int stage_stride_of(int slab_max) { return slab_area_of(slab_max) + XSEG_MAX * 128; }
+// slab | x window (XSEG_MAX 128-byte segments) | 128 bytes holding the zero slot
+inline int stage_stride_of(int slab_max) { return slab_area_of(slab_max) + XSEG_MAX * 128 + 128; }
 
 struct LayoutArgs {
     const uint8_t *slabs;

@@ -73,6 +73,11 @@ constexpr int STAGES = 4;
 constexpr int MAXRUNS = 24;
 constexpr int XSEG_MAX = 112;      // staged x segments per slab (14 KB of FP64 x)
 constexpr int XSEG_MAX32 = 224;    // the same 14 KB holding FP32 x
+// Byte offset, inside a stage's x window, of 16 zero bytes that no copy
+// writes. The padding entries of staged planes (plane k >= the row's length)
+// index it with value 0, so a loop over all W planes of a row block adds
+// 0 * 0 for them whatever x holds.
+constexpr uint32_t XZERO_OFF = XSEG_MAX * 128;
 constexpr int MAXW = 255;          // planes per row block (rowlen is u8)
 constexpr int MAXW_MIXED = 32;     // planes per row block in mixed layouts
 constexpr int SLAB_MAX_DEFAULT = 40960;
