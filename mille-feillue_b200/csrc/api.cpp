@@ -508,7 +508,8 @@ static int solve_dev_once(mf_tiles *t, int kind, const double *b_dev, double *x_
         int rows_max = 0;
         for (size_t g = 0; g + 1 < t->h_cta_rb.size(); ++g)
             rows_max = std::max(rows_max, 16 * (t->h_cta_rb[g + 1] - t->h_cta_rb[g]));
-        if (rows_max <= TMEM_ROWS_MAX) launch_kind = 3;
+        const int slab_max = t->opt.slab_bytes > 0 ? t->opt.slab_bytes : SLAB_MAX_DEFAULT;
+        if (rows_max <= TMEM_ROWS_MAX && tm_vectors_fit(rows_max, slab_max)) launch_kind = 3;
     }
     rc = launch_solver(t, launch_kind, P, 0);
     cudaEventRecord(e1, 0);

@@ -39,6 +39,7 @@ namespace mf {
 struct __align__(16) Smem {
     uint64_t full[STAGES];   // slab + x runs landed (producer arrive + tx bytes)
     uint64_t empty[STAGES];  // every consumer warp is done with the stage
+    uint64_t upd;            // bulk copies of the own rows' vectors (vector pass)
     uint32_t abort;
     uint32_t pad;
     int slab0[KMAX_LAYOUTS], slab1[KMAX_LAYOUTS];
@@ -622,6 +623,7 @@ __device__ void kernel_setup(const KParams &P, Smem &S, int nlay) {
             mbar_init(&S.full[k], 1);
             mbar_init(&S.empty[k], NWARPS);
         }
+        mbar_init(&S.upd, 1);
         mbar_fence_init();
         S.abort = 0;
     }
@@ -1374,57 +1376,72 @@ __device__ void tm_store(const TmemRows &T, double *xg, double *rg, uint64_t pol
     }
 }
 
-// The fused vector pass of k_cgcg on TMEM-resident x, r:
+// The vector pass of k_cgcg on TMEM-resident x, r:
 //   p = r + beta p;  s = w + beta s;  x += alpha p;  r -= alpha s;  r32 = r
-// (p, s rounded to FP32 before use, as in k_cgcg). r also goes to global
-// memory when rg. Returns the thread's share of the new r.r.
-__device__ double tm_update(const TmemRows &T, double alpha, double beta, float *pv, float *sv, const float *wv,
-                            float *r32, double *rg, uint64_t pol) {
+// p and s are stored in FP32, so they are formed by FP32 fused multiply-adds
+// (p = fma(beta, p, float(r)), s = fma(beta, s, w)); x and r stay FP64. That
+// is four FP32 <-> FP64 conversions a row instead of eight: conversions run
+// on a narrow pipe and bounded this pass. The own rows' p, s, w
+// (FP32) come into the copy ring, idle between two SpMVs, by three bulk
+// copies issued while the reduction runs: one 12-byte-per-row transfer
+// instead of per-thread loads waiting on L2. The host launches this kernel
+// only when 12 bytes per own row fit the ring (tm_vectors_fit).
+// Thread 0, after every thread's writes of p, s, w were fenced for the async
+// proxy and a barrier: the copies complete on S.upd.
+__device__ void tm_upd_issue(Smem &S, uint8_t *dyn, const float *pv, const float *sv, const float *wv, int vlo,
+                             int nrows, uint64_t pol) {
+    const uint32_t bytes = 4u * (uint32_t)nrows;  // nrows is a multiple of 16: 64-byte multiples
+    mbar_arrive_expect_tx(&S.upd, 3u * bytes);
+    bulk_g2s(dyn, pv + vlo, bytes, &S.upd, pol);
+    bulk_g2s(dyn + bytes, sv + vlo, bytes, &S.upd, pol);
+    bulk_g2s(dyn + 2u * bytes, wv + vlo, bytes, &S.upd, pol);
+}
+// The pass itself, with p, s, w read from the ring copy (sp, ss, sw: own-row
+// index); p, s, r32 (and r when rg) go to global memory. Returns the
+// thread's share of the new r.r.
+__device__ double tm_update_smem(const TmemRows &T, double alpha, double beta, const float *sp,
+                                              const float *ss, const float *sw, float *pv, float *sv, float *r32,
+                                              double *rg, uint64_t pol) {
     double rr = 0.0;
+    const float bf = (float)beta;
     for (int k = T.k0; k < T.nblk; k += 4 * TM_CB) {
         uint32_t t[TM_CB][16];
-        float4 pf[TM_CB], sf[TM_CB], wf[TM_CB];
         __syncwarp();
 #pragma unroll
-        for (int u = 0; u < TM_CB; ++u) {
-            const int kk = k + 4 * u;
-            if (kk < T.nblk) {
-                tmem_ld16(T.addr(kk), t[u]);
-                const int i = T.row_of(kk);
-                if (i < T.nrows) {
-                    pf[u] = ldf4_hint(pv + T.vlo + i, pol);
-                    sf[u] = ldf4_hint(sv + T.vlo + i, pol);
-                    wf[u] = ldf4_hint(wv + T.vlo + i, pol);
-                } else {
-                    pf[u] = sf[u] = wf[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-                }
-            }
-        }
+        for (int u = 0; u < TM_CB; ++u)
+            if (k + 4 * u < T.nblk) tmem_ld16(T.addr(k + 4 * u), t[u]);
 #pragma unroll
         for (int u = 0; u < TM_CB; ++u) {
             const int kk = k + 4 * u;
             __syncwarp();
             if (kk < T.nblk) {
                 tmem_wait_ld16(t[u]);
-                const float pin[4] = {pf[u].x, pf[u].y, pf[u].z, pf[u].w};
-                const float sin_[4] = {sf[u].x, sf[u].y, sf[u].z, sf[u].w};
-                const float win[4] = {wf[u].x, wf[u].y, wf[u].z, wf[u].w};
+                const int i = T.row_of(kk);
+                const bool live = i < T.nrows;
+                float4 pf = make_float4(0.f, 0.f, 0.f, 0.f), sf = pf, wf = pf;
+                if (live) {
+                    pf = *reinterpret_cast<const float4 *>(sp + i);
+                    sf = *reinterpret_cast<const float4 *>(ss + i);
+                    wf = *reinterpret_cast<const float4 *>(sw + i);
+                }
+                const float pin[4] = {pf.x, pf.y, pf.z, pf.w};
+                const float sin_[4] = {sf.x, sf.y, sf.z, sf.w};
+                const float win[4] = {wf.x, wf.y, wf.z, wf.w};
                 float pn[4], sn[4], rn[4];
                 double rsq = 0.0;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     double xv = tm_x(t[u], j), rv = tm_r(t[u], j);
-                    pn[j] = __double2float_rn(rv + beta * (double)pin[j]);
-                    sn[j] = __double2float_rn((double)win[j] + beta * (double)sin_[j]);
-                    xv = xv + alpha * (double)pn[j];
-                    rv = rv - alpha * (double)sn[j];
+                    pn[j] = __fmaf_rn(bf, pin[j], __double2float_rn(rv));
+                    sn[j] = __fmaf_rn(bf, sin_[j], win[j]);
+                    xv = fma(alpha, (double)pn[j], xv);
+                    rv = fma(-alpha, (double)sn[j], rv);
                     tm_set(t[u], j, xv, rv);
                     rn[j] = __double2float_rn(rv);
                     rsq += rv * rv;
                 }
                 tmem_st16_wait(T.addr(kk), t[u]);
-                const int i = T.row_of(kk);
-                if (i < T.nrows) {
+                if (live) {
                     const int row = T.vlo + i;
                     stf4_hint(pv + row, make_float4(pn[0], pn[1], pn[2], pn[3]), pol);
                     stf4_hint(sv + row, make_float4(sn[0], sn[1], sn[2], sn[3]), pol);
@@ -1451,6 +1468,10 @@ __device__ __forceinline__ void cgcg_tm_body(const KParams &P, Smem &S, uint8_t 
     int lay = P.start_layout;
     const int rb_lo = P.lay[0].cta_rb[g], rb_hi = P.lay[0].cta_rb[g + 1];
     const int vlo = rb_lo * 16, vhi = rb_hi * 16;
+    if (12ll * (vhi - vlo) > (long long)STAGES * P.stage_stride) {  // the host checks this first
+        set_error(P, (uint32_t)MF_ERR_UNSUPPORTED, 31);
+        return;
+    }
     double *x = P.x, *r = P.r;
     float *pv32 = reinterpret_cast<float *>(P.d), *sv32 = reinterpret_cast<float *>(P.q),
           *wv32 = reinterpret_cast<float *>(P.s);
@@ -1487,6 +1508,7 @@ __device__ __forceinline__ void cgcg_tm_body(const KParams &P, Smem &S, uint8_t 
     bool first = true, pending = false;
     const bool fixed = P.fixed_iterations > 0;
     const int maxit = fixed ? P.fixed_iterations : P.maxiter;
+    uint32_t uph = 0;
     while (true) {
         const bool repl_now = pending || (P.replace_every > 0 && it > 0 && it % P.replace_every == 0);
         if (repl_now) {
@@ -1533,8 +1555,21 @@ __device__ __forceinline__ void cgcg_tm_body(const KParams &P, Smem &S, uint8_t 
         else ok = cta_spmv<false>(P, lay64, r, S, dyn, pp, ew);
         if (!ok) return;
         MF_TRACE(it, 2);
+        // the ring is idle until the next SpMV: p, s, w of the own rows come
+        // into it while the reduction runs (every writer fences its stores
+        // for the async proxy before the barrier)
+        fence_proxy_async_global();
+        __syncthreads();
+        if (tid == 0) tm_upd_issue(S, dyn, pv32, sv32, wv32, vlo, vhi - vlo, vpol);
         double a2[2] = {s_gpart[tid], ew.dl}, c2[2];
-        if (!grid_sum<2>(P, S, a2, c2, phase)) return;
+        const bool red_ok = grid_sum<2>(P, S, a2, c2, phase);
+        // no path leaves with the copies in flight
+        if (!wait_bar(&S.upd, uph, P.limit_ns)) {
+            set_error(P, (uint32_t)MF_ERR_TIMEOUT, 30);
+            return;
+        }
+        uph ^= 1u;
+        if (!red_ok) return;
         MF_TRACE(it, 3);
         gam = c2[0];
         const double delta = c2[1];
@@ -1556,8 +1591,9 @@ __device__ __forceinline__ void cgcg_tm_body(const KParams &P, Smem &S, uint8_t 
             status = MF_ERR_BREAKDOWN;
             break;
         }
-        s_gpart[tid] = tm_update(tm_rows(P, s_tmem), alpha, beta, pv32, sv32, wv32, r32, lay == lay64 ? r : nullptr,
-                                 vpol);
+        const float *sp = reinterpret_cast<const float *>(dyn);
+        s_gpart[tid] = tm_update_smem(tm_rows(P, s_tmem), alpha, beta, sp, sp + (vhi - vlo), sp + 2 * (vhi - vlo),
+                                      pv32, sv32, r32, lay == lay64 ? r : nullptr, vpol);
         gamma_old = gam;
         alpha_old = alpha;
         MF_TRACE(it, 4);

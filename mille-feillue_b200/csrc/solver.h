@@ -106,6 +106,10 @@ int launch_to_f32(int n, const double *src, float *dst, size_t npad, cudaStream_
 // kind 0 CG, 1 BiCGSTAB, 2 single-reduction CG, 3 the same with x and r in
 // TMEM (every CTA's rows <= TMEM_ROWS_MAX), 4 Jacobi-preconditioned CG.
 constexpr int TMEM_ROWS_MAX = 128 * 128;
+// The TMEM kernel's vector pass copies 12 bytes per own row into the ring.
+inline bool tm_vectors_fit(int rows_max, int slab_max) {
+    return 12ll * rows_max <= (long long)STAGES * stage_stride_of(slab_max);
+}
 int launch_solver(mf_tiles *t, int kind, KParams &P, cudaStream_t s);
 int launch_residual_norms(int n, const double *b, const double *ax, double *out, cudaStream_t s);
 // minv[i] = 1 / diag[i] for i < n (1 where diag is 0), 0 up to npad.
