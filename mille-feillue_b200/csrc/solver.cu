@@ -303,6 +303,47 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
     return dadd(acc, low ? (double)sumf : sum);
 }
 
+// Two staged row blocks of one half-warp whose W planes are all FP32 and
+// equal in number, interleaved in one loop: two independent load and
+// accumulate chains per lane, each in the order of slab_row (identical
+// results). Returns false (nothing computed) when the pair does not qualify.
+__device__ __forceinline__ bool pair_rows32(const uint8_t *st, int j1, int j2, int r, const float *xs, double &a1,
+                                            double &a2) {
+    const RbDir *dir = reinterpret_cast<const RbDir *>(st + slab_rbdir_off());
+    const RbDir d1 = dir[j1], d2 = dir[j2];
+    const int W = (int)(d1.W & 0xffffu);
+    if ((int)(d2.W & 0xffffu) != W || W == 0 || W > 32) return false;
+    const uint8_t *b1 = st + d1.off, *b2 = st + d2.off;
+    const uint64_t p1 = *reinterpret_cast<const uint64_t *>(b1 + rb_pinfo_off());
+    const uint64_t p2 = *reinterpret_cast<const uint64_t *>(b2 + rb_pinfo_off());
+    if (p1 != (0x5555555555555555ull & ((2ull << (2 * W - 1)) - 1ull)) || p2 != p1) return false;
+    const uint16_t *i1 = reinterpret_cast<const uint16_t *>(b1 + rb_idx_off(W, true)) + r;
+    const uint16_t *i2 = reinterpret_cast<const uint16_t *>(b2 + rb_idx_off(W, true)) + r;
+    const float *v1 = reinterpret_cast<const float *>(b1 + rb_vals_off(W, true, false)) + r;
+    const float *v2 = reinterpret_cast<const float *>(b2 + rb_vals_off(W, true, false)) + r;
+    double c1 = 0.0, c2 = 0.0;
+    float s1 = 0.0f, s2 = 0.0f;
+#pragma unroll 2
+    for (int k = 0; k < W; ++k) {
+        const uint32_t id1 = i1[k * 16], id2 = i2[k * 16];
+        const float w1 = v1[k * 16], w2 = v2[k * 16];
+        const float x1 = xs[id1 & IDX16_POS], x2 = xs[id2 & IDX16_POS];
+        if (id1 & IDX16_START) {
+            c1 = dadd(c1, (double)s1);
+            s1 = 0.0f;
+        }
+        if (id2 & IDX16_START) {
+            c2 = dadd(c2, (double)s2);
+            s2 = 0.0f;
+        }
+        s1 = __fmaf_rn(x1, w1, s1);
+        s2 = __fmaf_rn(x2, w2, s2);
+    }
+    a1 = dadd(c1, (double)s1);
+    a2 = dadd(c2, (double)s2);
+    return true;
+}
+
 // Global tile arrays (the oversize path) and the source of one SpMV.
 struct SpmvSrc {
     const uint8_t *slabs;
@@ -428,26 +469,48 @@ __device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const void *xv,
                 int j0 = 2 * w + half - base;
                 if (j0 < 0) j0 += 2 * NWARPS;
                 base = (base + h.nrb) % (2 * NWARPS);
-                for (int j = j0; j < h.nrb; j += 2 * NWARPS) {
-                    const int row = (h.rb0 + j) * 16 + r;
-                    const bool live = row < L.gt.rowA;
-                    // the pre-loaded value keeps its own type until the epilogue:
-                    // a conversion here would wait for the load before the
-                    // row's arithmetic instead of overlapping it
-                    const double *xsg = reinterpret_cast<const double *>(st + slab_area);
-                    using PV = decltype(epi.pre(0));
-                    PV pv;
+                const double *xsg = reinterpret_cast<const double *>(st + slab_area);
+                using PV = decltype(epi.pre(0));
+                // the pre-loaded value keeps its own type until the epilogue:
+                // a conversion here would wait for the load before the row's
+                // arithmetic instead of overlapping it
+                auto pre_of = [&](int jj, int row, bool live) -> PV {
                     if constexpr (Epi::kUsesX) {
                         // the row's own x value from the stage (rows this CTA
                         // wrote just before load slowly from global memory);
                         // an FP64 value is not taken from an FP32 stage
-                        const uint32_t ds = reinterpret_cast<const RbDir *>(st + slab_rbdir_off())[j].W >> 16;
-                        if (ds == 0u || !live || (L.x32 && sizeof(PV) == 8)) pv = live ? epi.pre(row) : PV(0);
-                        else if (L.x32) pv = PV(reinterpret_cast<const float *>(xsg)[(ds - 1u) * 16u + r]);
-                        else pv = PV(xsg[(ds - 1u) * 16u + r]);
+                        const uint32_t ds = reinterpret_cast<const RbDir *>(st + slab_rbdir_off())[jj].W >> 16;
+                        if (ds == 0u || !live || (L.x32 && sizeof(PV) == 8)) return live ? epi.pre(row) : PV(0);
+                        if (L.x32) return PV(reinterpret_cast<const float *>(xsg)[(ds - 1u) * 16u + r]);
+                        return PV(xsg[(ds - 1u) * 16u + r]);
                     } else {
-                        pv = live ? epi.pre(row) : PV(0);
+                        return live ? epi.pre(row) : PV(0);
                     }
+                };
+                int jstart = j0;
+                if (MIXED && L.kind == LAYOUT_LOW && h.mode == SLAB_STAGED) {
+                    // all-FP32 row blocks j and j + 2 NWARPS of this half-warp
+                    // computed together; a pair that does not qualify (or a
+                    // lone last row block) goes to the loop below
+                    const float *xs = reinterpret_cast<const float *>(st + slab_area);
+                    for (; jstart + 2 * NWARPS < h.nrb; jstart += 4 * NWARPS) {
+                        const int j2 = jstart + 2 * NWARPS;
+                        const int row1 = (h.rb0 + jstart) * 16 + r, row2 = (h.rb0 + j2) * 16 + r;
+                        const bool live1 = row1 < L.gt.rowA, live2 = row2 < L.gt.rowA;
+                        const PV pv1 = pre_of(jstart, row1, live1), pv2 = pre_of(j2, row2, live2);
+                        double a1, a2;
+                        if (!pair_rows32(st, jstart, j2, r, xs, a1, a2)) {
+                            a1 = slab_row<LAYOUT_LOW, GB>(st, h, jstart, r, xs, static_cast<const float *>(xv));
+                            a2 = slab_row<LAYOUT_LOW, GB>(st, h, j2, r, xs, static_cast<const float *>(xv));
+                        }
+                        if (live1) epi(row1, a1, pv1);
+                        if (live2) epi(row2, a2, pv2);
+                    }
+                }
+                for (int j = jstart; j < h.nrb; j += 2 * NWARPS) {
+                    const int row = (h.rb0 + j) * 16 + r;
+                    const bool live = row < L.gt.rowA;
+                    const PV pv = pre_of(j, row, live);
                     const double *xg = static_cast<const double *>(xv);
                     double acc;
                     if (!MIXED || L.kind == LAYOUT_FP64) acc = slab_row<LAYOUT_FP64, GB>(st, h, j, r, xsg, xg);
