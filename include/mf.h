@@ -88,8 +88,9 @@ typedef struct {
                                 mf_spmv, at solve for the solvers);
                                 reserved[4] = CTAs per system group of
                                 mf_batch_create (0 = 4); reserved[5] = 1:
-                                the single-reduction CG keeps x and r in
-                                global memory instead of tensor memory;
+                                the CG kernels (FP64 and single-reduction
+                                mixed) keep x and r in global memory
+                                instead of tensor memory;
                                 reserved[6] = N > 0: reference iteration
                                 count for the learned selector's fallback   */
 } mf_options;

@@ -503,13 +503,16 @@ static int solve_dev_once(mf_tiles *t, int kind, const double *b_dev, double *x_
         if (rj) return rj;
     }
     int launch_kind = kind == 2 ? 4 : (mixed && kind == 0 && opt.reserved[2] != 1) ? 2 : kind;
-    if (launch_kind == 2 && opt.reserved[5] != 1) {
-        // x and r stay in tensor memory when every CTA's rows fit it
+    // x and r stay in tensor memory when every CTA's rows fit it, the ring
+    // holds the vector passes' copies, and one CTA runs per SM (each CTA
+    // allocates all of the SM's tensor memory)
+    if ((launch_kind == 2 || (launch_kind == 0 && !mixed)) && opt.reserved[5] != 1 && t->G == t->nsm) {
         int rows_max = 0;
         for (size_t g = 0; g + 1 < t->h_cta_rb.size(); ++g)
             rows_max = std::max(rows_max, 16 * (t->h_cta_rb[g + 1] - t->h_cta_rb[g]));
         const int slab_max = t->opt.slab_bytes > 0 ? t->opt.slab_bytes : SLAB_MAX_DEFAULT;
-        if (rows_max <= TMEM_ROWS_MAX && tm_vectors_fit(rows_max, slab_max)) launch_kind = 3;
+        if (rows_max <= TMEM_ROWS_MAX && tm_vectors_fit(rows_max, slab_max))
+            launch_kind = launch_kind == 2 ? 3 : 5;
     }
     rc = launch_solver(t, launch_kind, P, 0);
     cudaEventRecord(e1, 0);

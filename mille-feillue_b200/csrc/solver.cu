@@ -1454,6 +1454,7 @@ __device__ void tm_store(const TmemRows &T, double *xg, double *rg, uint64_t pol
 __device__ void tm_upd_issue(Smem &S, uint8_t *dyn, const float *pv, const float *sv, const float *wv, int vlo,
                              int nrows, uint64_t pol) {
     const uint32_t bytes = 4u * (uint32_t)nrows;  // nrows is a multiple of 16: 64-byte multiples
+    fence_proxy_async_smem();  // the ring was last read by generic loads
     mbar_arrive_expect_tx(&S.upd, 3u * bytes);
     bulk_g2s(dyn, pv + vlo, bytes, &S.upd, pol);
     bulk_g2s(dyn + bytes, sv + vlo, bytes, &S.upd, pol);
@@ -1695,6 +1696,239 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cgcg_tm(KParams P) {
     __syncthreads();
     tcgen05_fence_after_sync();
     cgcg_tm_body(P, S, dyn, &s_tmem, s_gpart);
+    tcgen05_fence_before_sync();
+    __syncthreads();
+    tcgen05_fence_after_sync();
+    if (w == 0) tmem_dealloc512(s_tmem);
+}
+
+// ------------------------------------------------------- FP64 CG with TMEM
+// The reference's CG recurrence (as k_cg<false>) with x and r of the own
+// rows resident in tensor memory for the whole solve; d (the SpMV input,
+// read by the neighbours' x windows) and q stay in global memory. Each of
+// the two vector passes reads its global vector from a bulk copy into the
+// idle ring, issued before the grid reduction that precedes the pass:
+//   r -= alpha q            (q copied while d.q is reduced)
+//   x += alpha d; d = r + beta d   (d copied while r.r is reduced)
+// Global traffic per row and iteration: q 8 + d 16 bytes instead of 64.
+
+// r -= alpha q over the TMEM rows, q from the ring copy (own-row index);
+// returns the thread's share of the new r.r.
+__device__ double tm_cg_r(const TmemRows &T, double alpha, const double *sq) {
+    double rr = 0.0;
+    for (int k = T.k0; k < T.nblk; k += 4 * TM_CB) {
+        uint32_t t[TM_CB][16];
+        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < TM_CB; ++u)
+            if (k + 4 * u < T.nblk) tmem_ld16(T.addr(k + 4 * u), t[u]);
+#pragma unroll
+        for (int u = 0; u < TM_CB; ++u) {
+            const int kk = k + 4 * u;
+            __syncwarp();
+            if (kk < T.nblk) {
+                tmem_wait_ld16(t[u]);
+                const int i = T.row_of(kk);
+                if (i < T.nrows) {
+                    const double2 q01 = *reinterpret_cast<const double2 *>(sq + i);
+                    const double2 q23 = *reinterpret_cast<const double2 *>(sq + i + 2);
+                    const double qv[4] = {q01.x, q01.y, q23.x, q23.y};
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const double rv = tm_r(t[u], j) - alpha * qv[j];
+                        tm_set(t[u], j, tm_x(t[u], j), rv);
+                        rr += rv * rv;
+                    }
+                }
+                tmem_st16_wait(T.addr(kk), t[u]);
+            }
+        }
+    }
+    return rr;
+}
+// x += alpha d and (unless done) d = r + beta d to global memory, d from the
+// ring copy.
+__device__ void tm_cg_xd(const TmemRows &T, double alpha, double beta, bool done, const double *sd, double *dg,
+                         uint64_t pol) {
+    for (int k = T.k0; k < T.nblk; k += 4 * TM_CB) {
+        uint32_t t[TM_CB][16];
+        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < TM_CB; ++u)
+            if (k + 4 * u < T.nblk) tmem_ld16(T.addr(k + 4 * u), t[u]);
+#pragma unroll
+        for (int u = 0; u < TM_CB; ++u) {
+            const int kk = k + 4 * u;
+            __syncwarp();
+            if (kk < T.nblk) {
+                tmem_wait_ld16(t[u]);
+                const int i = T.row_of(kk);
+                if (i < T.nrows) {
+                    const double2 d01 = *reinterpret_cast<const double2 *>(sd + i);
+                    const double2 d23 = *reinterpret_cast<const double2 *>(sd + i + 2);
+                    const double dv[4] = {d01.x, d01.y, d23.x, d23.y};
+                    double dn[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const double rv = tm_r(t[u], j);
+                        tm_set(t[u], j, tm_x(t[u], j) + alpha * dv[j], rv);
+                        dn[j] = rv + beta * dv[j];
+                    }
+                    if (!done) {
+                        st2_hint(dg + T.vlo + i, make_double2(dn[0], dn[1]), pol);
+                        st2_hint(dg + T.vlo + i + 2, make_double2(dn[2], dn[3]), pol);
+                    }
+                }
+                tmem_st16_wait(T.addr(kk), t[u]);
+            }
+        }
+    }
+}
+// Thread 0: one bulk copy of the own rows of an FP64 vector into the ring.
+__device__ void tm_vec_issue(Smem &S, uint8_t *dyn, const double *v, int vlo, int nrows, uint64_t pol) {
+    const uint32_t bytes = 8u * (uint32_t)nrows;  // nrows is a multiple of 16
+    fence_proxy_async_smem();  // the ring was last read by generic loads
+    mbar_arrive_expect_tx(&S.upd, bytes);
+    bulk_g2s(dyn, v + vlo, bytes, &S.upd, pol);
+}
+
+__device__ __forceinline__ void cg_tm_body(const KParams &P, Smem &S, uint8_t *dyn, const volatile uint32_t *s_tmem) {
+    const int g = blockIdx.x, tid = threadIdx.x;
+    Pipe pp;
+    uint32_t phase = 0, uph = 0;
+    const uint64_t vpol = policy_evict_last();
+    const int rb_lo = P.lay[0].cta_rb[g], rb_hi = P.lay[0].cta_rb[g + 1];
+    const int vlo = rb_lo * 16, vhi = rb_hi * 16;
+    if (8ll * (vhi - vlo) > (long long)STAGES * P.stage_stride) {  // the host checks this first
+        set_error(P, (uint32_t)MF_ERR_UNSUPPORTED, 32);
+        return;
+    }
+    double *x = P.x, *r = P.r, *d = P.d, *q = P.q;
+    const double *b = P.b;
+    const double *sv = reinterpret_cast<const double *>(dyn);
+    if (P.inject_wait) {
+        // test hook (as in k_cg): an epoch no CTA publishes; the bounded wait
+        // must end the solve with MF_ERR_TIMEOUT
+        if (!wait_deps(P, S, 0, 0xffffffffu)) return;
+    }
+    // the bulk copy of the own rows of v (written by this CTA's threads
+    // before: each fences its stores for the async proxy, then the barrier)
+    auto copy_own = [&](const double *v) {
+        fence_proxy_async_global();
+        __syncthreads();
+        if (tid == 0) tm_vec_issue(S, dyn, v, vlo, vhi - vlo, vpol);
+    };
+    auto copy_wait = [&]() -> bool {
+        if (!wait_bar(&S.upd, uph, P.limit_ns)) {
+            set_error(P, (uint32_t)MF_ERR_TIMEOUT, 33);
+            return false;
+        }
+        uph ^= 1u;
+        return true;
+    };
+    // r = b - A x0 (global), d = r; x, r into TMEM; (rr, bb)
+    EpiResidual er{b, r, 0.0, vpol};
+    if (!cta_spmv<false>(P, 0, x, S, dyn, pp, er)) return;
+    __syncthreads();
+    double bbp = 0.0;
+    MF_PAIRS(4, vlo, vhi, {
+        double2 rv[_vb], bv[_vb];
+#pragma unroll
+        MF_FOR_VB if (MF_LIVE(u, vhi)) {
+            rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+            bv[u] = ld2_hint(b + 2 * MF_PI(u), vpol);
+        }
+#pragma unroll
+        MF_FOR_VB if (MF_LIVE(u, vhi)) {
+            st2_hint(d + 2 * MF_PI(u), rv[u], vpol);
+            bbp += bv[u].x * bv[u].x + bv[u].y * bv[u].y;
+        }
+    })
+    __syncthreads();
+    tm_load(tm_rows(P, s_tmem), x, r, vpol);
+    double v2[2] = {er.rr, bbp}, o2[2];
+    if (!grid_sum<2>(P, S, v2, o2, phase)) return;
+    double rr = o2[0];
+    const double bb = o2[1];
+    const double bnorm = sqrt(bb);
+    const double tol = P.tol;
+    uint32_t ep = 1;
+    publish(P, ep);
+    int it = 0, status = MF_OK;
+    double rel = bnorm > 0 ? sqrt(rr) / bnorm : 0.0;
+    const bool fixed = P.fixed_iterations > 0;
+    const int maxit = fixed ? P.fixed_iterations : P.maxiter;
+    while (it < maxit && (fixed || rel > tol)) {
+        MF_TRACE(it, 0);
+        if (!wait_deps(P, S, 0, ep)) return;
+        MF_TRACE(it, 1);
+        EpiQ eq{d, q, 0.0, vpol};
+        if (!cta_spmv<false>(P, 0, d, S, dyn, pp, eq)) return;
+        MF_TRACE(it, 2);
+        copy_own(q);
+        double v1[1] = {eq.dq}, o1[1];
+        const bool ok1 = grid_sum<1>(P, S, v1, o1, phase);
+        if (!copy_wait() || !ok1) return;  // no path leaves with the copy in flight
+        MF_TRACE(it, 3);
+        const double dq = o1[0];
+        if (!(dq != 0.0) || !isfinite(dq)) {
+            status = MF_ERR_BREAKDOWN;
+            break;
+        }
+        const double alpha = rr / dq;
+        const double rrp = tm_cg_r(tm_rows(P, s_tmem), alpha, sv);
+        MF_TRACE(it, 4);
+        // every thread is done reading q from the ring before d lands there
+        __syncthreads();
+        copy_own(d);
+        double w1[1] = {rrp}, u1[1];
+        const bool ok2 = grid_sum<1>(P, S, w1, u1, phase);
+        if (!copy_wait() || !ok2) return;
+        MF_TRACE(it, 5);
+        const double rrn = u1[0];
+        ++it;
+        rel = bnorm > 0 ? sqrt(rrn) / bnorm : 0.0;
+        const double beta = rrn / rr;
+        const bool done = !fixed && rel <= tol;
+        tm_cg_xd(tm_rows(P, s_tmem), alpha, beta, done, sv, d, vpol);
+        rr = rrn;
+        ++ep;
+        publish(P, ep);
+        MF_TRACE(it - 1, 6);
+        if (!isfinite(rrn)) {
+            status = MF_ERR_BREAKDOWN;
+            break;
+        }
+    }
+    __syncthreads();
+    tm_store(tm_rows(P, s_tmem), x, r, vpol);
+    if (g == 0 && tid == 0) {
+        if (status == MF_OK && !fixed && rel > tol) status = MF_ERR_NOT_CONVERGED;
+        P.res->iterations = it;
+        P.res->status = status;
+        P.res->replacements = 0;
+        P.res->level_switches = 0;
+        P.res->rr = rr;
+        P.res->bb = bb;
+        P.res->final_layout = 0;
+        for (int l = 0; l < KMAX_LAYOUTS; ++l) P.res->it_layout[l] = l == 0 ? it : 0;
+        P.res->pad = 0;
+    }
+}
+
+// One CTA per SM holds all 512 TMEM columns for the whole solve; every exit
+// of the body (including aborts) comes back here to release them.
+__global__ void __launch_bounds__(NTHREADS, 1) k_cg_tm(KParams P) {
+    extern __shared__ __align__(128) uint8_t dyn[];
+    __shared__ Smem S;
+    __shared__ uint32_t s_tmem;
+    kernel_setup(P, S, 1);
+    const int w = threadIdx.x >> 5;
+    if (w == 0) tmem_alloc512(&s_tmem);
+    tcgen05_fence_before_sync();
+    __syncthreads();
+    tcgen05_fence_after_sync();
+    cg_tm_body(P, S, dyn, &s_tmem);
     tcgen05_fence_before_sync();
     __syncthreads();
     tcgen05_fence_after_sync();
@@ -2169,7 +2403,8 @@ int kernel_config(mf_tiles *t, int *G_out) {
     const void *kerns[] = {(const void *)k_cg<false>, (const void *)k_cg<true>, (const void *)k_bicgstab<false>,
                            (const void *)k_bicgstab<true>,
                            (const void *)k_spmv<false>, (const void *)k_spmv<true>, (const void *)k_cgcg,
-                           (const void *)k_batch_cg, (const void *)k_cgcg_tm, (const void *)k_pcg};
+                           (const void *)k_batch_cg, (const void *)k_cgcg_tm, (const void *)k_pcg,
+                           (const void *)k_cg_tm};
     int occ_min = 1 << 30;
     for (const void *k : kerns) {
         MF_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
@@ -2260,6 +2495,7 @@ int launch_solver(mf_tiles *t, int kind, KParams &P, cudaStream_t s) {
                     : kind == 2 ? (const void *)k_cgcg
                     : kind == 3 ? (const void *)k_cgcg_tm
                     : kind == 4 ? (const void *)k_pcg
+                    : kind == 5 ? (const void *)k_cg_tm
                                 : (P.nlay > 1 ? (const void *)k_bicgstab<true> : (const void *)k_bicgstab<false>);
     MF_CUDA_TRY(cudaLaunchCooperativeKernel(k, dim3(t->G), dim3(NTHREADS), args, dyn, s));
     return MF_OK;
