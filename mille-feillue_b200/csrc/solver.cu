@@ -41,7 +41,7 @@ struct __align__(16) Smem {
     uint64_t empty[STAGES];  // every consumer warp is done with the stage
     uint64_t upd;            // bulk copies of the own rows' vectors (vector pass)
     uint32_t abort;
-    uint32_t pad;
+    uint8_t res_tag[STAGES];  // 1 + layout whose slab (index = stage) the stage holds; 0: none
     int slab0[KMAX_LAYOUTS], slab1[KMAX_LAYOUTS];
     double red[NWARPS + 1][4];
     double bres[4];
@@ -349,6 +349,7 @@ struct SpmvSrc {
     const uint8_t *slabs;
     const uint8_t *head;  // STAGES issue records (shared memory)
     int ns, kind, site;
+    int resident_ok;      // slabs may stay in the ring between SpMVs (site = layout index)
     int x32;              // x staged in FP32 (the input vector is FP32)
     GTiles gt;
 };
@@ -436,8 +437,25 @@ __device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const void *xv,
                     if (C.prefetch && h->pf_bytes) bulk_prefetch_l2(L.slabs + (size_t)h->pf_off16 * 16, h->pf_bytes);
                 }
                 fence_proxy_async_smem();
-                issue_slab(S, st, slab_area, k, off16, bytes, xbytes, nruns, runs, L.slabs,
-                           static_cast<const uint8_t *>(xv), L.x32 ? 64u : 128u, pm, pv);
+                // a CTA with at most STAGES slabs puts slab i in stage i on
+                // every SpMV: when the stage still holds it (same layout,
+                // nothing else written into the ring since), only its x
+                // window is copied
+                const bool keep = L.resident_ok && ns <= STAGES;
+                if (keep && S.res_tag[k] == (uint8_t)(L.site + 1)) {
+                    mbar_arrive_expect_tx(&S.full[k], xbytes);
+                    const uint32_t segb = L.x32 ? 64u : 128u;
+                    for (int q = 0; q < nruns; ++q) {
+                        const XRun rr = runs[q];
+                        bulk_g2s(st + slab_area + (size_t)rr.slot0 * segb,
+                                 static_cast<const uint8_t *>(xv) + (size_t)rr.seg0 * segb, (uint32_t)rr.nseg * segb,
+                                 &S.full[k], pv);
+                    }
+                } else {
+                    issue_slab(S, st, slab_area, k, off16, bytes, xbytes, nruns, runs, L.slabs,
+                               static_cast<const uint8_t *>(xv), L.x32 ? 64u : 128u, pm, pv);
+                    S.res_tag[k] = keep ? (uint8_t)(L.site + 1) : (uint8_t)0;
+                }
             }
         }
         __syncwarp();
@@ -541,6 +559,7 @@ __device__ bool cta_spmv(const KParams &P, int lay, const void *xv, Smem &S, uin
     L.kind = P.lay[lay].kind;
     L.x32 = P.lay[lay].x32;
     L.site = lay;
+    L.resident_ok = 1;
     L.gt = gtiles_of(P);
     const PipeCfg C{P.stage_stride, P.slab_area, P.limit_ns, P.sync, P.prefetch};
     return cta_spmv_src<MIXED, Epi, GB>(L, C, xv, S, dyn, pp, epi);
@@ -675,12 +694,19 @@ __device__ bool wait_deps(const KParams &P, Smem &S, int lay, uint32_t ep) {
     return wait_deps_x(ctx_of(P), S, P.lay[lay].cta_dep[2 * blockIdx.x], P.lay[lay].cta_dep[2 * blockIdx.x + 1], ep);
 }
 
+// The zero slot of every stage (XZERO_OFF): written at set-up, and again
+// after a vector pass whose bulk copies went through the ring (the caller
+// has a barrier between the pass's last reads of the ring and this).
+__device__ __forceinline__ void zero_slots(uint8_t *dyn, int stage_stride, int slab_area) {
+    if (threadIdx.x < STAGES)
+        *reinterpret_cast<uint4 *>(dyn + (size_t)threadIdx.x * stage_stride + slab_area + XZERO_OFF) =
+            make_uint4(0u, 0u, 0u, 0u);
+}
+
 __device__ void kernel_setup(const KParams &P, Smem &S, int nlay) {
     extern __shared__ __align__(128) uint8_t dyn[];
     const int tid = threadIdx.x;
-    if (tid < STAGES)
-        *reinterpret_cast<uint4 *>(dyn + (size_t)tid * P.stage_stride + P.slab_area + XZERO_OFF) =
-            make_uint4(0u, 0u, 0u, 0u);
+    zero_slots(dyn, P.stage_stride, P.slab_area);
     if (tid == 0) {
         for (int k = 0; k < STAGES; ++k) {
             mbar_init(&S.full[k], 1);
@@ -689,6 +715,7 @@ __device__ void kernel_setup(const KParams &P, Smem &S, int nlay) {
         mbar_init(&S.upd, 1);
         mbar_fence_init();
         S.abort = 0;
+        for (int k = 0; k < STAGES; ++k) S.res_tag[k] = 0;
     }
     for (int l = 0; l < nlay; ++l) {
         const uint8_t *src = P.lay[l].head + (size_t)blockIdx.x * STAGES * ISSUE_REC;
@@ -1455,6 +1482,7 @@ __device__ void tm_upd_issue(Smem &S, uint8_t *dyn, const float *pv, const float
                              int nrows, uint64_t pol) {
     const uint32_t bytes = 4u * (uint32_t)nrows;  // nrows is a multiple of 16: 64-byte multiples
     fence_proxy_async_smem();  // the ring was last read by generic loads
+    for (int k = 0; k < STAGES; ++k) S.res_tag[k] = 0;  // the copies overwrite the slabs
     mbar_arrive_expect_tx(&S.upd, 3u * bytes);
     bulk_g2s(dyn, pv + vlo, bytes, &S.upd, pol);
     bulk_g2s(dyn + bytes, sv + vlo, bytes, &S.upd, pol);
@@ -1640,6 +1668,7 @@ __device__ __forceinline__ void cgcg_tm_body(const KParams &P, Smem &S, uint8_t 
         rel = bnorm > 0 ? sqrt(gam) / bnorm : 0.0;
         if (!fixed && rel <= tol) {
             pending = true;  // confirm with the FP64 true residual
+            zero_slots(dyn, P.stage_stride, P.slab_area);  // the copies overwrote them
             continue;
         }
         double alpha, beta;
@@ -1665,6 +1694,10 @@ __device__ __forceinline__ void cgcg_tm_body(const KParams &P, Smem &S, uint8_t 
         ++it;
         ++ep;
         publish(P, ep);
+        // the copies overwrote the zero slots: restored after publish's
+        // barrier (the pass is done reading the ring) and before the next
+        // SpMV (the halo wait ends with a barrier)
+        zero_slots(dyn, P.stage_stride, P.slab_area);
         MF_TRACE(it - 1, 6);
     }
     tm_store(tm_rows(P, s_tmem), x, r, vpol);
@@ -1788,6 +1821,7 @@ __device__ void tm_cg_xd(const TmemRows &T, double alpha, double beta, bool done
 __device__ void tm_vec_issue(Smem &S, uint8_t *dyn, const double *v, int vlo, int nrows, uint64_t pol) {
     const uint32_t bytes = 8u * (uint32_t)nrows;  // nrows is a multiple of 16
     fence_proxy_async_smem();  // the ring was last read by generic loads
+    for (int k = 0; k < STAGES; ++k) S.res_tag[k] = 0;  // the copy overwrites the slabs
     mbar_arrive_expect_tx(&S.upd, bytes);
     bulk_g2s(dyn, v + vlo, bytes, &S.upd, pol);
 }
@@ -1894,6 +1928,7 @@ __device__ __forceinline__ void cg_tm_body(const KParams &P, Smem &S, uint8_t *d
         rr = rrn;
         ++ep;
         publish(P, ep);
+        zero_slots(dyn, P.stage_stride, P.slab_area);  // as in k_cgcg_tm
         MF_TRACE(it - 1, 6);
         if (!isfinite(rrn)) {
             status = MF_ERR_BREAKDOWN;
@@ -2270,6 +2305,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_batch_cg(BatchParams B) {
             s_rng[1] = D.cta_rb[rank];
             s_rng[2] = D.cta_rb[rank + 1];
             s_rng[3] = 0;
+            // the ring holds the previous system's slabs
+            for (int k = 0; k < STAGES; ++k) S.res_tag[k] = 0;
         }
         __syncthreads();
         const int dep_lo = D.cta_dep[2 * rank], dep_hi = D.cta_dep[2 * rank + 1];
@@ -2279,6 +2316,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_batch_cg(BatchParams B) {
         L.ns = s_rng[0];
         L.kind = D.kind;
         L.site = 40;
+        L.resident_ok = 1;  // within this system's solve
         L.x32 = 0;  // FP64 layouts
         L.gt = D.gt;
         const int vlo = s_rng[1] * 16, vhi = s_rng[2] * 16;
