@@ -424,12 +424,27 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
     std::vector<XRun> run_all;
     std::vector<int> slab_cta;
     std::vector<int> cta_slab(G + 1, 0);
-    std::vector<int> cur, merged, rbsegs;
-    auto count_runs = [](const std::vector<int> &v) {
-        int r = 0;
-        for (size_t i = 0; i < v.size(); ++i)
-            if (i == 0 || v[i] != v[i - 1] + 1) ++r;
-        return r;
+    std::vector<int> cur;
+    // x segments (tile columns) of the slab being planned, kept incrementally
+    // since a row block adds only a few: membership (offset by one so that
+    // s - 1 and s + 1 are always addressable), the members in insertion
+    // order, and the number of runs of consecutive segments
+    std::vector<uint8_t> inseg((size_t)t->tilen + 2, 0);
+    std::vector<int> members;
+    int seg_runs = 0;
+    auto seg_add = [&](int s) {
+        if (inseg[s + 1]) return;
+        inseg[s + 1] = 1;
+        members.push_back(s);
+        seg_runs += 1 - inseg[s] - inseg[s + 2];
+    };
+    auto seg_drop_to = [&](size_t n) {  // undo the adds past the first n, newest first
+        while (members.size() > n) {
+            const int s = members.back();
+            members.pop_back();
+            inseg[s + 1] = 0;
+            seg_runs -= 1 - inseg[s] - inseg[s + 2];
+        }
     };
     int n_gather = 0, n_over = 0, xseg_max = XSEG_MAX, rbps = RB_PER_SLAB_X64;
     uint32_t segbytes = 128u;
@@ -450,8 +465,8 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
             while (rb < cta_rb[g + 1]) {
                 SlabPlan P{};
                 P.rb0 = rb;
-                rbsegs.assign(tc.begin() + tp[rb], tc.begin() + tp[rb + 1]);  // ascending already
-                const bool staged0 = (int)rbsegs.size() <= xseg_max && count_runs(rbsegs) <= MAXRUNS;
+                for (int k = tp[rb]; k < tp[rb + 1]; ++k) seg_add(tc[k]);
+                const bool staged0 = (int)members.size() <= xseg_max && seg_runs <= MAXRUNS;
                 const uint32_t tot0 = slab_blocks_off(1) + rb_bytes(rb, !staged0);
                 if (tot0 > (uint32_t)slab_max || rbW[rb] > maxw) {
                     P.mode = SLAB_OVERSIZE;
@@ -464,7 +479,6 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
                 } else {
                     const bool staged = staged0;
                     P.mode = staged ? SLAB_STAGED : SLAB_GATHER;
-                    if (staged) cur = rbsegs;
                     P.nrb = 1;
                     P.ntiles = tp[rb + 1] - tp[rb];
                     uint32_t body = rb_bytes(rb, !staged);
@@ -474,11 +488,12 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
                         const uint32_t bx = rb_bytes(nx, !staged);
                         if (slab_blocks_off(P.nrb + 1) + body + bx > (uint32_t)slab_max) break;
                         if (staged) {
-                            merged.clear();
-                            std::set_union(cur.begin(), cur.end(), tc.begin() + tp[nx], tc.begin() + tp[nx + 1],
-                                           std::back_inserter(merged));
-                            if ((int)merged.size() > xseg_max || count_runs(merged) > MAXRUNS) break;
-                            cur.swap(merged);
+                            const size_t n0 = members.size();
+                            for (int k = tp[nx]; k < tp[nx + 1]; ++k) seg_add(tc[k]);
+                            if ((int)members.size() > xseg_max || seg_runs > MAXRUNS) {
+                                seg_drop_to(n0);
+                                break;
+                            }
                         }
                         P.nrb += 1;
                         P.ntiles += tp[nx + 1] - tp[nx];
@@ -490,6 +505,8 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
                     rb = nx;
                 }
                 if (P.mode == SLAB_STAGED) {
+                    cur.assign(members.begin(), members.end());
+                    std::sort(cur.begin(), cur.end());
                     P.seg_off = (int)seg_all.size();
                     P.nseg = (int)cur.size();
                     seg_all.insert(seg_all.end(), cur.begin(), cur.end());
@@ -500,6 +517,7 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
                     }
                     P.nruns = (int)run_all.size() - P.run_off;
                 }
+                seg_drop_to(0);
                 plans.push_back(P);
                 slab_cta.push_back(g);
             }
