@@ -163,15 +163,23 @@ def cpu_reference_arm(args, rank):
         t0 = time.perf_counter()
         iters, _, _ = o.cg(b, TOL, MAXITER)
         full_ms = (time.perf_counter() - t0) * 1e3
-    times = []
+    # each step times a short and a long sample (tol 0: exactly that many
+    # iterations); their difference is the cost of sample_iters iterations
+    # alone, the short one less its iterations is the call's fixed part (x
+    # set-up, the initial residual SpMV, thread start-up), counted once
+    times, fixed = [], []
     for step in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        it, _, _ = o.cg(b, 0.0, sample_iters)  # tol 0: exactly sample_iters iterations
-        dt = time.perf_counter() - t0
+        o.cg(b, 0.0, sample_iters)
+        t1 = time.perf_counter()
+        o.cg(b, 0.0, 2 * sample_iters)
+        t2 = time.perf_counter()
         if step >= args.warmup:
-            times.append(dt / max(it, 1))
+            per = ((t2 - t1) - (t1 - t0)) / sample_iters
+            times.append(per)
+            fixed.append(max(0.0, (t1 - t0) - per * sample_iters))
     per_it = statistics.median(times)
-    value = per_it * iters * 1e3
+    value = (statistics.median(fixed) + per_it * iters) * 1e3
     cores = os.cpu_count()
     return {
         "metric": METRIC, "impl": "reference", "value": value, "unit": "ms", "n_gpus": args.gpus,
@@ -180,9 +188,10 @@ def cpu_reference_arm(args, rank):
         "config": {"workload": "varpoisson3d_128 CG to 1e-10 true residual", "n": n, "nnz": int(len(v)),
                    "x0": "zeros", "tol": TOL},
         "cpu_baseline": {"value": value, "unit": "ms", "cores": cores, "kind": "port",
-                         "sample": f"{sample_iters} CG iterations of the oracle (reference recurrence, tiled "
-                                   f"SpMV order, OpenMP) on the full matrix per step, median per-iteration "
-                                   f"time x {iters} iterations to 1e-10", "ms_per_iteration": per_it * 1e3,
+                         "sample": f"{sample_iters} and {2 * sample_iters} CG iterations of the oracle "
+                                   f"(reference recurrence, tiled SpMV order, OpenMP) on the full matrix per "
+                                   f"step; median per-iteration time (their difference) x {iters} iterations "
+                                   f"to 1e-10, plus the call's fixed part once", "ms_per_iteration": per_it * 1e3,
                          "iterations": int(iters), "full_solve_ms": full_ms, "tile_encode_s": enc_s},
         "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -266,22 +275,27 @@ def gpu_arm(args, world, rank, local, dist):
     x_h = torch.zeros(n, dtype=torch.float64).pin_memory()
     L = mf.lib()
     csr = mf.MfCsr(n, n, int(len(v)), rp_h.data_ptr(), ci_h.data_ptr(), v_h.data_ptr())
-    e2e = []
+    e2e, parts = [], []
     for step in range(1 + max(1, args.e2e_steps)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         h = mf._p()
         rc = L.mf_encode(C.byref(csr), C.byref(opts), C.byref(h))
         assert rc == 0, rc
+        t1 = time.perf_counter()
         x_h.zero_()
         r2 = mf.MfResult()
         rc = L.mf_solve_cg(h, C.c_void_p(b_h.data_ptr()), C.c_void_p(x_h.data_ptr()), TOL, MAXITER,
                            C.byref(opts), C.byref(r2))
+        t2 = time.perf_counter()
         L.mf_free(h)
         torch.cuda.synchronize()
+        t3 = time.perf_counter()
         if step > 0:
-            e2e.append((time.perf_counter() - t0) * 1e3)
+            e2e.append((t3 - t0) * 1e3)
+            parts.append(((t1 - t0) * 1e3, (t2 - t1) * 1e3, (t3 - t2) * 1e3))
     e2e_ms = _max_over_ranks(dist, statistics.median(e2e))
+    e2e_parts = {k: statistics.median(p[i] for p in parts) for i, k in enumerate(("encode_ms", "solve_ms", "free_ms"))}
     h2d = rp.nbytes + ci.nbytes + v.nbytes + b.nbytes + n * 8  # CSR, b, x0
     d2h = n * 8 + 8  # x and the result scalars
 
@@ -334,6 +348,7 @@ def gpu_arm(args, world, rank, local, dist):
                                       "gflops": 2.0 * len(v) / spmv_mx_ms / 1e6}},
             "clocks": clk,
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    **e2e_parts,
                     "path": "mf_encode(host CSR) + mf_solve_cg(host b, host x) + mf_free"},
             "gpu_launches": args.steps * launches_per_solve,
             "encode_s": enc_s, "encode_ms_device": info["encode_ms"], "layout_ms": info["layout_ms"],
@@ -424,7 +439,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--cpu-sample-iters", type=int, default=20)
+    ap.add_argument("--cpu-sample-iters", type=int, default=100)
     ap.add_argument("--fp64-iters", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="poisson128", choices=["poisson128", "batch"])

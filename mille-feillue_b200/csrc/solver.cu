@@ -748,11 +748,19 @@ struct EpiStore {
     __device__ void operator()(int row, double acc, double) const { y[row] = acc; }
 };
 
+// Launched with programmatic stream serialization: the next SpMV in the
+// stream may be scheduled as soon as this one starts (it occupies an SM only
+// once this grid's CTA there has exited), does its set-up (barriers, issue
+// records of the constant layout), and waits for this grid to complete
+// before it reads x or writes y. Without that launch attribute both
+// instructions do nothing.
 template <bool MIXED>
 __global__ void __launch_bounds__(NTHREADS, 1) k_spmv(KParams P, const void *x, double *y, int lay, int reps) {
     extern __shared__ __align__(128) uint8_t dyn[];
     __shared__ Smem S;
+    asm volatile("griddepcontrol.launch_dependents;");
     kernel_setup(P, S, lay + 1);
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     Pipe pp;
     EpiStore epi{y};
     for (int it = 0; it < reps; ++it) {
@@ -2518,11 +2526,18 @@ int launch_spmv(mf_tiles *t, int level, const void *x, double *y, int reps, cuda
         mixed = true;
     }
     const int dyn = dyn_smem(t->L64.slab_max);
-    if (mixed)
-        k_spmv<true><<<t->G, NTHREADS, dyn, s>>>(P, x, y, lay, reps);
-    else
-        k_spmv<false><<<t->G, NTHREADS, dyn, s>>>(P, x, y, lay, reps);
-    MF_CUDA_TRY(cudaGetLastError());
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(t->G);
+    cfg.blockDim = dim3(NTHREADS);
+    cfg.dynamicSmemBytes = dyn;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    if (mixed) MF_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_spmv<true>, P, x, y, lay, reps));
+    else MF_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_spmv<false>, P, x, y, lay, reps));
     return MF_OK;
 }
 
