@@ -506,13 +506,18 @@ static int solve_dev_once(mf_tiles *t, int kind, const double *b_dev, double *x_
     // x and r stay in tensor memory when every CTA's rows fit it, the ring
     // holds the vector passes' copies, and one CTA runs per SM (each CTA
     // allocates all of the SM's tensor memory)
-    if ((launch_kind == 2 || (launch_kind == 0 && !mixed)) && opt.reserved[5] != 1 && t->G == t->nsm) {
+    if ((launch_kind == 2 || launch_kind == 4 || (launch_kind == 0 && !mixed)) && opt.reserved[5] != 1 &&
+        t->G == t->nsm) {
         int rows_max = 0;
         for (size_t g = 0; g + 1 < t->h_cta_rb.size(); ++g)
             rows_max = std::max(rows_max, 16 * (t->h_cta_rb[g + 1] - t->h_cta_rb[g]));
         const int slab_max = t->opt.slab_bytes > 0 ? t->opt.slab_bytes : SLAB_MAX_DEFAULT;
         if (rows_max <= TMEM_ROWS_MAX && tm_vectors_fit(rows_max, slab_max))
-            launch_kind = launch_kind == 2 ? 3 : 5;
+            launch_kind = launch_kind == 2 ? 3 : launch_kind == 4 ? 6 : 5;
+    }
+    if (launch_kind == 6) {  // the FP32 copy of 1/a_ii that the ring copies carry
+        int rj = launch_to_f32((int)n16, v.s, v.p32, n16, 0);
+        if (rj) return rj;
     }
     rc = launch_solver(t, launch_kind, P, 0);
     cudaEventRecord(e1, 0);

@@ -1978,6 +1978,241 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cg_tm(KParams P) {
     if (w == 0) tmem_dealloc512(s_tmem);
 }
 
+// ------------------------------------------- Jacobi PCG with TMEM (k_pcg_tm)
+// k_pcg's recurrence with x and r in tensor memory (as k_cg_tm); d and q in
+// global memory. The Jacobi scaling 1/a_ii is applied from an FP32 copy that
+// rides with q (r pass) and with d (x/d pass) in the ring: 12 bytes a row.
+
+// Thread 0: q (or d) and the FP32 scaling of the own rows into the ring.
+__device__ void tm_vec2_issue(Smem &S, uint8_t *dyn, const double *v, const float *m32, int vlo, int nrows,
+                              uint64_t pol) {
+    const uint32_t b8 = 8u * (uint32_t)nrows, b4 = 4u * (uint32_t)nrows;  // nrows is a multiple of 16
+    fence_proxy_async_smem();  // the ring was last read by generic loads
+    for (int k = 0; k < STAGES; ++k) S.res_tag[k] = 0;  // the copies overwrite the slabs
+    mbar_arrive_expect_tx(&S.upd, b8 + b4);
+    bulk_g2s(dyn, v + vlo, b8, &S.upd, pol);
+    bulk_g2s(dyn + b8, m32 + vlo, b4, &S.upd, pol);
+}
+// r -= alpha q, z = m r; returns the thread's shares of r.z (rz) and r.r.
+__device__ double tm_pcg_r(const TmemRows &T, double alpha, const double *sq, const float *sm, double &rz) {
+    double rr = 0.0;
+    rz = 0.0;
+    for (int k = T.k0; k < T.nblk; k += 4 * TM_CB) {
+        uint32_t t[TM_CB][16];
+        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < TM_CB; ++u)
+            if (k + 4 * u < T.nblk) tmem_ld16(T.addr(k + 4 * u), t[u]);
+#pragma unroll
+        for (int u = 0; u < TM_CB; ++u) {
+            const int kk = k + 4 * u;
+            __syncwarp();
+            if (kk < T.nblk) {
+                tmem_wait_ld16(t[u]);
+                const int i = T.row_of(kk);
+                if (i < T.nrows) {
+                    const double2 q01 = *reinterpret_cast<const double2 *>(sq + i);
+                    const double2 q23 = *reinterpret_cast<const double2 *>(sq + i + 2);
+                    const float4 m4 = *reinterpret_cast<const float4 *>(sm + i);
+                    const double qv[4] = {q01.x, q01.y, q23.x, q23.y};
+                    const double mv[4] = {(double)m4.x, (double)m4.y, (double)m4.z, (double)m4.w};
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const double rv = tm_r(t[u], j) - alpha * qv[j];
+                        tm_set(t[u], j, tm_x(t[u], j), rv);
+                        rz += rv * (mv[j] * rv);
+                        rr += rv * rv;
+                    }
+                }
+                tmem_st16_wait(T.addr(kk), t[u]);
+            }
+        }
+    }
+    return rr;
+}
+// x += alpha d and (unless done) d = m r + beta d to global memory.
+__device__ void tm_pcg_xd(const TmemRows &T, double alpha, double beta, bool done, const double *sd, const float *sm,
+                          double *dg, uint64_t pol) {
+    for (int k = T.k0; k < T.nblk; k += 4 * TM_CB) {
+        uint32_t t[TM_CB][16];
+        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < TM_CB; ++u)
+            if (k + 4 * u < T.nblk) tmem_ld16(T.addr(k + 4 * u), t[u]);
+#pragma unroll
+        for (int u = 0; u < TM_CB; ++u) {
+            const int kk = k + 4 * u;
+            __syncwarp();
+            if (kk < T.nblk) {
+                tmem_wait_ld16(t[u]);
+                const int i = T.row_of(kk);
+                if (i < T.nrows) {
+                    const double2 d01 = *reinterpret_cast<const double2 *>(sd + i);
+                    const double2 d23 = *reinterpret_cast<const double2 *>(sd + i + 2);
+                    const float4 m4 = *reinterpret_cast<const float4 *>(sm + i);
+                    const double dv[4] = {d01.x, d01.y, d23.x, d23.y};
+                    const double mv[4] = {(double)m4.x, (double)m4.y, (double)m4.z, (double)m4.w};
+                    double dn[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const double rv = tm_r(t[u], j);
+                        tm_set(t[u], j, tm_x(t[u], j) + alpha * dv[j], rv);
+                        dn[j] = mv[j] * rv + beta * dv[j];
+                    }
+                    if (!done) {
+                        st2_hint(dg + T.vlo + i, make_double2(dn[0], dn[1]), pol);
+                        st2_hint(dg + T.vlo + i + 2, make_double2(dn[2], dn[3]), pol);
+                    }
+                }
+                tmem_st16_wait(T.addr(kk), t[u]);
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void pcg_tm_body(const KParams &P, Smem &S, uint8_t *dyn, const volatile uint32_t *s_tmem) {
+    const int g = blockIdx.x, tid = threadIdx.x;
+    Pipe pp;
+    uint32_t phase = 0, uph = 0;
+    const uint64_t vpol = policy_evict_last();
+    const int vlo = P.lay[0].cta_rb[g] * 16, vhi = P.lay[0].cta_rb[g + 1] * 16;
+    const int nrows = vhi - vlo;
+    if (12ll * nrows > (long long)STAGES * P.stage_stride) {  // the host checks this first
+        set_error(P, (uint32_t)MF_ERR_UNSUPPORTED, 34);
+        return;
+    }
+    double *x = P.x, *r = P.r, *d = P.d, *q = P.q;
+    const float *m32 = P.p32;  // FP32 1/a_ii
+    const double *b = P.b;
+    const double *sv = reinterpret_cast<const double *>(dyn);
+    const float *sm = reinterpret_cast<const float *>(dyn + 8 * (size_t)nrows);
+    auto copy_own = [&](const double *v) {
+        fence_proxy_async_global();
+        __syncthreads();
+        if (tid == 0) tm_vec2_issue(S, dyn, v, m32, vlo, nrows, vpol);
+    };
+    auto copy_wait = [&]() -> bool {
+        if (!wait_bar(&S.upd, uph, P.limit_ns)) {
+            set_error(P, (uint32_t)MF_ERR_TIMEOUT, 35);
+            return false;
+        }
+        uph ^= 1u;
+        return true;
+    };
+    // r = b - A x0 (global); d = z = m r; x, r into TMEM; (rr, rz, bb)
+    EpiResidual er{b, r, 0.0, vpol};
+    if (!cta_spmv<false>(P, 0, x, S, dyn, pp, er)) return;
+    __syncthreads();
+    double rzp = 0.0, bbp = 0.0;
+    MF_PAIRS(2, vlo, vhi, {
+        double2 rv[_vb], bv[_vb];
+        float2 mv[_vb];
+#pragma unroll
+        MF_FOR_VB if (MF_LIVE(u, vhi)) {
+            rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+            bv[u] = ld2_hint(b + 2 * MF_PI(u), vpol);
+            mv[u] = *reinterpret_cast<const float2 *>(m32 + 2 * MF_PI(u));
+        }
+#pragma unroll
+        MF_FOR_VB if (MF_LIVE(u, vhi)) {
+            double2 z;
+            z.x = (double)mv[u].x * rv[u].x;
+            z.y = (double)mv[u].y * rv[u].y;
+            st2_hint(d + 2 * MF_PI(u), z, vpol);
+            rzp += rv[u].x * z.x + rv[u].y * z.y;
+            bbp += bv[u].x * bv[u].x + bv[u].y * bv[u].y;
+        }
+    })
+    __syncthreads();
+    tm_load(tm_rows(P, s_tmem), x, r, vpol);
+    double v3[3] = {er.rr, rzp, bbp}, o3[3];
+    if (!grid_sum<3>(P, S, v3, o3, phase)) return;
+    double rr = o3[0], rz = o3[1];
+    const double bb = o3[2];
+    const double bnorm = sqrt(bb);
+    const double tol = P.tol;
+    uint32_t ep = 1;
+    publish(P, ep);
+    int it = 0, status = MF_OK;
+    double rel = bnorm > 0 ? sqrt(rr) / bnorm : 0.0;
+    const bool fixed = P.fixed_iterations > 0;
+    const int maxit = fixed ? P.fixed_iterations : P.maxiter;
+    while (it < maxit && (fixed || rel > tol)) {
+        MF_TRACE(it, 0);
+        if (!wait_deps(P, S, 0, ep)) return;
+        MF_TRACE(it, 1);
+        EpiQ eq{d, q, 0.0, vpol};
+        if (!cta_spmv<false>(P, 0, d, S, dyn, pp, eq)) return;
+        MF_TRACE(it, 2);
+        copy_own(q);
+        double v1[1] = {eq.dq}, o1[1];
+        const bool ok1 = grid_sum<1>(P, S, v1, o1, phase);
+        if (!copy_wait() || !ok1) return;  // no path leaves with the copies in flight
+        MF_TRACE(it, 3);
+        const double dq = o1[0];
+        if (!(dq != 0.0) || !isfinite(dq)) {
+            status = MF_ERR_BREAKDOWN;
+            break;
+        }
+        const double alpha = rz / dq;
+        double rzn;
+        const double rrn_p = tm_pcg_r(tm_rows(P, s_tmem), alpha, sv, sm, rzn);
+        MF_TRACE(it, 4);
+        __syncthreads();  // every thread is done reading q before d lands there
+        copy_own(d);
+        double w2[2] = {rzn, rrn_p}, u2[2];
+        const bool ok2 = grid_sum<2>(P, S, w2, u2, phase);
+        if (!copy_wait() || !ok2) return;
+        MF_TRACE(it, 5);
+        rr = u2[1];
+        ++it;
+        rel = bnorm > 0 ? sqrt(rr) / bnorm : 0.0;
+        const double beta = u2[0] / rz;
+        rz = u2[0];
+        const bool done = !fixed && rel <= tol;
+        tm_pcg_xd(tm_rows(P, s_tmem), alpha, beta, done, sv, sm, d, vpol);
+        ++ep;
+        publish(P, ep);
+        zero_slots(dyn, P.stage_stride, P.slab_area);  // as in k_cgcg_tm
+        MF_TRACE(it - 1, 6);
+        if (!isfinite(rr)) {
+            status = MF_ERR_BREAKDOWN;
+            break;
+        }
+    }
+    __syncthreads();
+    tm_store(tm_rows(P, s_tmem), x, r, vpol);
+    if (g == 0 && tid == 0) {
+        if (status == MF_OK && !fixed && rel > tol) status = MF_ERR_NOT_CONVERGED;
+        P.res->iterations = it;
+        P.res->status = status;
+        P.res->replacements = 0;
+        P.res->level_switches = 0;
+        P.res->rr = rr;
+        P.res->bb = bb;
+        P.res->final_layout = 0;
+        for (int l = 0; l < KMAX_LAYOUTS; ++l) P.res->it_layout[l] = l == 0 ? it : 0;
+        P.res->pad = 0;
+    }
+}
+
+__global__ void __launch_bounds__(NTHREADS, 1) k_pcg_tm(KParams P) {
+    extern __shared__ __align__(128) uint8_t dyn[];
+    __shared__ Smem S;
+    __shared__ uint32_t s_tmem;
+    kernel_setup(P, S, 1);
+    const int w = threadIdx.x >> 5;
+    if (w == 0) tmem_alloc512(&s_tmem);
+    tcgen05_fence_before_sync();
+    __syncthreads();
+    tcgen05_fence_after_sync();
+    pcg_tm_body(P, S, dyn, &s_tmem);
+    tcgen05_fence_before_sync();
+    __syncthreads();
+    tcgen05_fence_after_sync();
+    if (w == 0) tmem_dealloc512(s_tmem);
+}
+
 // -------------------------------------------------------------- BiCGSTAB
 struct EpiDot {  // y = A p, dot += z*y
     static constexpr bool kUsesX = false;
@@ -2450,7 +2685,7 @@ int kernel_config(mf_tiles *t, int *G_out) {
                            (const void *)k_bicgstab<true>,
                            (const void *)k_spmv<false>, (const void *)k_spmv<true>, (const void *)k_cgcg,
                            (const void *)k_batch_cg, (const void *)k_cgcg_tm, (const void *)k_pcg,
-                           (const void *)k_cg_tm};
+                           (const void *)k_cg_tm, (const void *)k_pcg_tm};
     int occ_min = 1 << 30;
     for (const void *k : kerns) {
         MF_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
@@ -2549,6 +2784,7 @@ int launch_solver(mf_tiles *t, int kind, KParams &P, cudaStream_t s) {
                     : kind == 3 ? (const void *)k_cgcg_tm
                     : kind == 4 ? (const void *)k_pcg
                     : kind == 5 ? (const void *)k_cg_tm
+                    : kind == 6 ? (const void *)k_pcg_tm
                                 : (P.nlay > 1 ? (const void *)k_bicgstab<true> : (const void *)k_bicgstab<false>);
     MF_CUDA_TRY(cudaLaunchCooperativeKernel(k, dim3(t->G), dim3(NTHREADS), args, dyn, s));
     return MF_OK;
