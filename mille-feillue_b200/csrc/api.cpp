@@ -15,7 +15,8 @@
 using namespace mf;
 
 namespace mf {
-int build_mixed_levels(mf_tiles *t, cudaStream_t s);  // precision.cpp
+int build_mixed_levels(mf_tiles *t, cudaStream_t s);                                  // precision.cu
+int abs_range(const double *v, long long n, double *lo, double *hi, cudaStream_t s);  // precision.cu
 }
 
 template <class T>
@@ -514,6 +515,16 @@ static int solve_dev_once(mf_tiles *t, int kind, const double *b_dev, double *x_
         const int slab_max = t->opt.slab_bytes > 0 ? t->opt.slab_bytes : SLAB_MAX_DEFAULT;
         if (rows_max <= TMEM_ROWS_MAX && tm_vectors_fit(rows_max, slab_max))
             launch_kind = launch_kind == 2 ? 3 : launch_kind == 4 ? 6 : 5;
+    }
+    if (launch_kind == 6) {
+        // the tensor-memory PCG applies 1/a_ii from an FP32 copy: only when
+        // every 1/a_ii is an FP32 normal number (checked once per handle)
+        if (t->minv_f32_ok < 0) {
+            double lo = 0.0, hi = 0.0;
+            if ((rc = abs_range(v.s, (long long)n16, &lo, &hi, 0)) != MF_OK) return rc;
+            t->minv_f32_ok = (lo == 0.0 || lo >= 1.2e-38) && hi <= 3.0e38 ? 1 : 0;
+        }
+        if (!t->minv_f32_ok) launch_kind = 4;
     }
     if (launch_kind == 6) {  // the FP32 copy of 1/a_ii that the ring copies carry
         int rj = launch_to_f32((int)n16, v.s, v.p32, n16, 0);

@@ -140,24 +140,6 @@ MF_DEV void tmem_alloc512(uint32_t *dst) {
 MF_DEV void tmem_dealloc512(uint32_t taddr) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(taddr) : "memory");
 }
-// Four consecutive columns of the thread's lane. The wait takes the loaded
-// registers as operands so that no use of them moves above it.
-MF_DEV void tmem_ld4(uint32_t taddr, uint32_t (&v)[4]) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
-                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
-                 : "r"(taddr));
-}
-MF_DEV void tmem_wait_ld(uint32_t (&v)[4]) {
-    asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3])::"memory");
-}
-// Store four columns and wait for the store, before the source registers can
-// be reused.
-MF_DEV void tmem_st4_wait(uint32_t taddr, const uint32_t (&v)[4]) {
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), "r"(v[0]), "r"(v[1]),
-                 "r"(v[2]), "r"(v[3])
-                 : "memory");
-    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-}
 // Sixteen consecutive columns of the thread's lane.
 MF_DEV void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
     asm volatile(

@@ -74,25 +74,34 @@ __global__ void k_absminmax(const double *v, long long n, unsigned long long *mn
 
 }  // namespace
 
-// The whole-matrix features f2 and f4 (a device reduction over the values).
-int matrix_features(const mf_tiles *t, float *lognnz, float *logrange, cudaStream_t s) {
-    *lognnz = (float)std::log10(std::max(1.0, (double)t->csrsize));
-    *logrange = 0.0f;
-    if (t->csrsize == 0) return MF_OK;
+// Smallest nonzero and largest |v[i]| over n device values (lo = hi = 0 when
+// every value is zero).
+int abs_range(const double *v, long long n, double *lo, double *hi, cudaStream_t s) {
+    *lo = *hi = 0.0;
+    if (n <= 0) return MF_OK;
     DevArray<unsigned long long> d;
     if (d.alloc(2)) return MF_ERR_NOMEM;
     const unsigned long long init[2] = {~0ull, 0ull};
     MF_CUDA_TRY(cudaMemcpyAsync(d.p, init, sizeof init, cudaMemcpyHostToDevice, s));
-    k_absminmax<<<592, 256, 0, s>>>(t->val.p, (long long)t->csrsize, d.p, d.p + 1);
+    k_absminmax<<<592, 256, 0, s>>>(v, n, d.p, d.p + 1);
     MF_CUDA_TRY(cudaGetLastError());
     unsigned long long h[2];
     MF_CUDA_TRY(cudaMemcpyAsync(h, d.p, sizeof h, cudaMemcpyDeviceToHost, s));
     MF_CUDA_TRY(cudaStreamSynchronize(s));
     if (h[0] == ~0ull || h[1] == 0ull) return MF_OK;
-    double lo, hi;
-    std::memcpy(&lo, &h[0], sizeof lo);
-    std::memcpy(&hi, &h[1], sizeof hi);
-    *logrange = (float)std::log10(hi / lo);
+    std::memcpy(lo, &h[0], sizeof *lo);
+    std::memcpy(hi, &h[1], sizeof *hi);
+    return MF_OK;
+}
+
+// The whole-matrix features f2 and f4 (a device reduction over the values).
+int matrix_features(const mf_tiles *t, float *lognnz, float *logrange, cudaStream_t s) {
+    *lognnz = (float)std::log10(std::max(1.0, (double)t->csrsize));
+    *logrange = 0.0f;
+    double lo = 0.0, hi = 0.0;
+    const int rc = abs_range(t->val.p, (long long)t->csrsize, &lo, &hi, s);
+    if (rc) return rc;
+    if (lo > 0.0) *logrange = (float)std::log10(hi / lo);
     return MF_OK;
 }
 

@@ -2478,34 +2478,6 @@ __global__ void k_residual_norms(int n, const double *b, const double *ax, doubl
 }
 
 // ------------------------------------------------------------ batched CG
-// Deterministic block reduction (fixed order) broadcast to every thread.
-template <int NV>
-__device__ void block_sum(Smem &S, const double (&v)[NV], double (&out)[NV]) {
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    double t[NV];
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-        t[k] = v[k];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) t[k] += __shfl_xor_sync(0xffffffffu, t[k], o);
-    }
-    if (lane == 0)
-#pragma unroll
-        for (int k = 0; k < NV; ++k) S.red[w][k] = t[k];
-    __syncthreads();
-    if (tid == 0)
-#pragma unroll
-        for (int k = 0; k < NV; ++k) {
-            double a = 0.0;
-            for (int q = 0; q <= NWARPS; ++q) a += S.red[q][k];
-            S.bres[k] = a;
-        }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < NV; ++k) out[k] = S.bres[k];
-    __syncthreads();
-}
-
 // The grid is split into groups of B.gs CTAs. Rank 0 of a group takes the
 // next system from a device queue (largest first) and a group reduction
 // hands it to the other ranks; the group then runs the FP64 CG recurrence of

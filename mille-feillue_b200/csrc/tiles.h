@@ -203,6 +203,7 @@ struct mf_tiles {
     mf::DevArray<float> x32buf;  // FP32 copy of x for layouts staging FP32 x
     mf::DevArray<uint64_t> trace;  // phase timestamps of the last traced solve
     int trace_iters = 0;
+    int minv_f32_ok = -1;  // every 1/a_ii fits FP32 (-1: not checked yet)
 };
 
 namespace mf {
