@@ -27,6 +27,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -62,7 +63,7 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"mf_bench_clocks_rank{device}.csv")
 
     def start(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
