@@ -119,8 +119,8 @@ int mf_encode_dev(int n, int ncols, int nnz, const int *rp, const int *ci, const
 int mf_encode(const mf_csr *A, const mf_options *opt, mf_tiles **out) {
     if (!A || !out || A->n <= 0 || A->ncols <= 0 || A->nnz < 0 || !A->row_ptr) return MF_ERR_ARG;
     if (A->row_ptr[0] != 0 || A->row_ptr[A->n] != A->nnz) return MF_ERR_ARG;
-    for (int i = 0; i < A->nnz; ++i)
-        if (A->col_idx[i] < 0 || A->col_idx[i] >= A->ncols) return MF_ERR_ARG;
+    // the column indices and the row pointers' order are checked on the GPU
+    // by the encoder (as for mf_encode_dev)
     const int dev = opt ? opt->device : 0;
     MF_CUDA_TRY(cudaSetDevice(dev));
     DevArray<int> rp, ci;

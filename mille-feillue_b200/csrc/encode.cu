@@ -360,6 +360,22 @@ int exclusive_scan_int(int *d, long long n, cudaStream_t s) {
 }
 
 // Encodes rows [0, n) of a device CSR whose columns lie in [0, ncols).
+// The CSR checks every encode needs before any kernel indexes by it:
+// row_ptr starts at 0, ends at nnz and never decreases; 0 <= col_idx < ncols.
+__global__ void enc_validate(int n, int ncols, int nnz, const int *__restrict__ rp, const int *__restrict__ ci,
+                             int *bad) {
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    int b = 0;
+    for (long long i = tid; i < nnz; i += stride) {
+        const int c = ci[i];
+        b |= (c < 0) | (c >= ncols);
+    }
+    for (long long i = tid; i < n; i += stride) b |= rp[i] > rp[i + 1];
+    if (tid == 0) b |= (rp[0] != 0) | (rp[n] != nnz);
+    if (__any_sync(0xffffffffu, b) && (threadIdx.x & 31) == 0) atomicOr(bad, 1);
+}
+
 int encode_device(mf_tiles *t, int n, int ncols, int nnz, const int *rp, const int *ci, const double *val,
                   cudaStream_t s) {
     const int rowA = n, colA = ncols;
@@ -376,14 +392,20 @@ int encode_device(mf_tiles *t, int n, int ncols, int nnz, const int *rp, const i
     cudaEventRecord(e0, s);
 
     DevArray<int> perm, maxm;
-    if (perm.alloc(nnz) || maxm.alloc(1)) return MF_ERR_NOMEM;
+    if (perm.alloc(nnz) || maxm.alloc(2)) return MF_ERR_NOMEM;  // [0] max entries of a row block, [1] invalid CSR
     if (t->tile_ptr.alloc(tilem + 1)) return MF_ERR_NOMEM;
     MF_CUDA_TRY(cudaMemsetAsync(t->tile_ptr.p, 0, sizeof(int) * (tilem + 1), s));
-    MF_CUDA_TRY(cudaMemsetAsync(maxm.p, 0, sizeof(int), s));
+    MF_CUDA_TRY(cudaMemsetAsync(maxm.p, 0, 2 * sizeof(int), s));
+    enc_validate<<<592, 256, 0, s>>>(rowA, colA, nnz, rp, ci, maxm.p + 1);
     enc_rowblock_sizes<<<nblk(tilem, 256), 256, 0, s>>>(rowA, tilem, rp, maxm.p);
-    int hmax = 0;
-    MF_CUDA_TRY(cudaMemcpyAsync(&hmax, maxm.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    int hmv[2] = {0, 0};
+    MF_CUDA_TRY(cudaMemcpyAsync(hmv, maxm.p, sizeof hmv, cudaMemcpyDeviceToHost, s));
     MF_CUDA_TRY(cudaStreamSynchronize(s));
+    if (hmv[1]) {
+        set_last_error("invalid CSR: row_ptr must run from 0 to nnz without decreasing, col_idx within [0, ncols)");
+        return MF_ERR_ARG;
+    }
+    const int hmax = hmv[0];
     long long cap = 1;
     while (cap < hmax) cap <<= 1;
     const bool any_big = hmax > ENC_CAP;

@@ -124,16 +124,63 @@ int tile_features(mf_tiles *t, std::vector<float> &feat, cudaStream_t s) {
 // Unit roundoffs of FP8-E4M3, FP16, FP32.
 static const double kU[4] = {0x1p-53, 0x1p-24, 0x1p-11, 0x1p-4};
 
-uint8_t rule_precision(const float *f, double tau) {
-    const double m = std::pow(10.0, (double)f[0]);
+struct RuleThresholds {
+    float mag[4];           // largest log10 tile magnitude that passes, per precision
+    float range16, range8;  // largest log10 tile range allowed for FP16 / FP8
+};
+
+// The magnitude rule for a tile with features f (f0 = log10 of its scaled
+// magnitude m, f1 = log10 of its value range, f3 = diagonal tile): the lowest
+// precision p with u_p * m <= tau, FP8 only for an off-diagonal tile of range
+// <= 4096, FP16 only for one of range <= 1e8, FP32 before FP64. Each test
+// (u_p * 10^f0 <= tau, 10^f1 <= R, evaluated in double) increases with f, so
+// it holds exactly for the floats up to the largest one that passes it,
+// found once per level by bisection over the ordered float values; a tile
+// then needs float comparisons only (NaN features fail every test: FP64).
+namespace {
+int32_t fkey(float f) {
+    int32_t b;
+    std::memcpy(&b, &f, 4);
+    return b >= 0 ? b : -(b & 0x7fffffff);
+}
+float fval(int32_t k) {
+    const int32_t b = k >= 0 ? k : (int32_t)((uint32_t)(-k) | 0x80000000u);
+    float f;
+    std::memcpy(&f, &b, 4);
+    return f;
+}
+template <class Pred>
+float largest_passing(Pred pass) {  // pass holds on (-inf, x] for some float x
+    int64_t lo = fkey(-INFINITY), hi = fkey(INFINITY);  // the span exceeds int32
+    if (!pass(fval((int32_t)lo))) return NAN;  // nothing passes
+    if (pass(fval((int32_t)hi))) return INFINITY;
+    while (hi - lo > 1) {  // pass(lo), !pass(hi)
+        const int64_t mid = lo + (hi - lo) / 2;
+        if (pass(fval((int32_t)mid))) lo = mid;
+        else hi = mid;
+    }
+    return fval((int32_t)lo);
+}
+}  // namespace
+
+RuleThresholds rule_thresholds(double tau) {
+    RuleThresholds r;
+    for (int p = MF_PREC_FP32; p <= MF_PREC_FP8; ++p)
+        r.mag[p] = largest_passing([&](float f) { return kU[p] * std::pow(10.0, (double)f) <= tau; });
+    r.range16 = largest_passing([](float f) { return std::pow(10.0, (double)f) <= 1e8; });
+    r.range8 = largest_passing([](float f) { return std::pow(10.0, (double)f) <= 4096.0; });
+    return r;
+}
+
+uint8_t rule_precision_fast(const float *f, const RuleThresholds &r) {
+    const float f0 = f[0], f1 = f[1];
     const bool diag = f[3] > 0.5f;
-    const double range = std::pow(10.0, (double)f[1]);
-    if (!std::isfinite(m)) return MF_PREC_FP64;
-    if (!diag && kU[MF_PREC_FP8] * m <= tau && range <= 4096.0) return MF_PREC_FP8;
-    if (!diag && kU[MF_PREC_FP16] * m <= tau && range <= 1e8) return MF_PREC_FP16;
-    if (kU[MF_PREC_FP32] * m <= tau) return MF_PREC_FP32;
+    if (!diag && f0 <= r.mag[MF_PREC_FP8] && f1 <= r.range8) return MF_PREC_FP8;
+    if (!diag && f0 <= r.mag[MF_PREC_FP16] && f1 <= r.range16) return MF_PREC_FP16;
+    if (f0 <= r.mag[MF_PREC_FP32]) return MF_PREC_FP32;
     return MF_PREC_FP64;
 }
+
 
 // Row blocks whose tiles are mostly FP32 keep every low-precision tile in
 // FP32: a row block whose planes all hold FP32 runs the lean FP32 loop, and
@@ -214,7 +261,8 @@ int build_mixed_levels(mf_tiles *t, cudaStream_t s) {
     std::vector<uint8_t> prev;
     for (int l = 0; l < MF_NLEVELS; ++l) {
         std::vector<uint8_t> p(t->tilenum);
-        for (int k = 0; k < t->tilenum; ++k) p[k] = rule_precision(&feat[(size_t)k * 6], kLevelTau[l] * scale);
+        const RuleThresholds thr = rule_thresholds(kLevelTau[l] * scale);
+        for (int k = 0; k < t->tilenum; ++k) p[k] = rule_precision_fast(&feat[(size_t)k * 6], thr);
         promote_minority(t, p);
         if (l > 0 && p == prev) break;  // identical to the previous level
         rc = build_layout(t, t->Lmix[l], p, s);

@@ -209,3 +209,33 @@ def test_autotune_keeps_results_and_picks_the_fastest(mf, mode):
     # the dot products' rounding follows the row-to-thread mapping, which the
     # slab grouping changes: iteration counts may move by a little
     assert abs(r1["iterations"] - r0["iterations"]) <= max(2, 0.02 * r0["iterations"])
+
+
+@pytest.mark.parametrize("defect", ["col_high", "col_negative", "row_ptr_decreasing"])
+def test_encode_rejects_invalid_csr(mf, defect):
+    """The encoder checks the CSR on the GPU before any kernel indexes by it,
+    for host (mf_encode) and device (mf_encode_dev) input alike."""
+    import ctypes as C
+
+    import torch
+
+    A = mf.Matrix.poisson2d(16)
+    rp, ci, v = A.csr()
+    rp, ci, v = rp.astype(np.int32).copy(), ci.astype(np.int32).copy(), v.copy()
+    if defect == "col_high":
+        ci[len(ci) // 2] = A.n
+    elif defect == "col_negative":
+        ci[3] = -1
+    else:
+        rp[10], rp[11] = rp[11], rp[10]
+    L = mf.lib()
+    opts = mf.options()
+    h = mf._p()
+    csr = mf.MfCsr(A.n, A.n, len(v), rp.ctypes.data, ci.ctypes.data, v.ctypes.data)
+    assert L.mf_encode(C.byref(csr), C.byref(opts), C.byref(h)) == mf.MF_ERR_ARG
+    assert b"invalid CSR" in L.mf_last_error()
+    drp, dci, dv = (torch.tensor(a, device="cuda") for a in (rp, ci, v))
+    h2 = mf._p()
+    rc = L.mf_encode_dev(A.n, A.n, len(v), C.c_void_p(drp.data_ptr()), C.c_void_p(dci.data_ptr()),
+                         C.c_void_p(dv.data_ptr()), C.byref(opts), C.byref(h2))
+    assert rc == mf.MF_ERR_ARG
