@@ -16,6 +16,8 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <functional>
+#include <thread>
 
 #include "common.cuh"
 #include "tiles.h"
@@ -418,49 +420,45 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
     // layout is planned again with FP64 x.
     bool x32 = mixed;
     for (size_t k = 0; k < prec.size() && x32; ++k) x32 = prec[k] != MF_PREC_FP64;
-    // slabs
+    // slabs: the CTAs' row-block ranges are planned independently (on up to
+    // 16 host threads for large matrices) and concatenated in CTA order
     std::vector<SlabPlan> plans;
     std::vector<int> seg_all;
     std::vector<XRun> run_all;
     std::vector<int> slab_cta;
     std::vector<int> cta_slab(G + 1, 0);
-    std::vector<int> cur;
-    // x segments (tile columns) of the slab being planned, kept incrementally
-    // since a row block adds only a few: membership (offset by one so that
-    // s - 1 and s + 1 are always addressable), the members in insertion
-    // order, and the number of runs of consecutive segments
-    std::vector<uint8_t> inseg((size_t)t->tilen + 2, 0);
-    std::vector<int> members;
-    int seg_runs = 0;
-    auto seg_add = [&](int s) {
-        if (inseg[s + 1]) return;
-        inseg[s + 1] = 1;
-        members.push_back(s);
-        seg_runs += 1 - inseg[s] - inseg[s + 2];
-    };
-    auto seg_drop_to = [&](size_t n) {  // undo the adds past the first n, newest first
-        while (members.size() > n) {
-            const int s = members.back();
-            members.pop_back();
-            inseg[s + 1] = 0;
-            seg_runs -= 1 - inseg[s] - inseg[s + 2];
-        }
+    struct Part {  // one thread's CTAs
+        std::vector<SlabPlan> plans;
+        std::vector<int> segs, nslab;
+        std::vector<XRun> runs;
+        int n_gather = 0, n_over = 0;
     };
     int n_gather = 0, n_over = 0, xseg_max = XSEG_MAX, rbps = RB_PER_SLAB_X64;
     uint32_t segbytes = 128u;
-    for (;;) {
-        xseg_max = x32 ? XSEG_MAX32 : XSEG_MAX;
-        segbytes = x32 ? 64u : 128u;
-        rbps = t->opt.rb_per_slab > 0 ? std::min(t->opt.rb_per_slab, RB_PER_SLAB_MAX)
-                                      : (x32 ? RB_PER_SLAB_MAX : RB_PER_SLAB_X64);
-        plans.clear();
-        seg_all.clear();
-        run_all.clear();
-        slab_cta.clear();
-        cta_slab.assign(G + 1, 0);
-        n_gather = n_over = 0;
-        for (int g = 0; g < G; ++g) {
-            cta_slab[g] = (int)plans.size();
+    auto plan_ctas = [&](int g0, int g1, Part &out) {
+        // x segments (tile columns) of the slab being planned, kept
+        // incrementally since a row block adds only a few: membership (offset
+        // by one so that s - 1 and s + 1 are always addressable), the members
+        // in insertion order, and the number of runs of consecutive segments
+        std::vector<uint8_t> inseg((size_t)t->tilen + 2, 0);
+        std::vector<int> members, cur;
+        int seg_runs = 0;
+        auto seg_add = [&](int s) {
+            if (inseg[s + 1]) return;
+            inseg[s + 1] = 1;
+            members.push_back(s);
+            seg_runs += 1 - inseg[s] - inseg[s + 2];
+        };
+        auto seg_drop_to = [&](size_t n) {  // undo the adds past the first n, newest first
+            while (members.size() > n) {
+                const int s = members.back();
+                members.pop_back();
+                inseg[s + 1] = 0;
+                seg_runs -= 1 - inseg[s] - inseg[s + 2];
+            }
+        };
+        for (int g = g0; g < g1; ++g) {
+            const size_t first = out.plans.size();
             int rb = cta_rb[g];
             while (rb < cta_rb[g + 1]) {
                 SlabPlan P{};
@@ -473,8 +471,8 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
                     P.nrb = 1;
                     P.ntiles = tp[rb + 1] - tp[rb];
                     P.bytes = slab_blocks_off(0);
-                    for (int k = tp[rb]; k < tp[rb + 1]; ++k) prec[k] = MF_PREC_FP64;
-                    ++n_over;
+                    for (int k = tp[rb]; k < tp[rb + 1]; ++k) prec[k] = MF_PREC_FP64;  // this CTA's tiles only
+                    ++out.n_over;
                     rb += 1;
                 } else {
                     const bool staged = staged0;
@@ -501,26 +499,72 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
                         ++nx;
                     }
                     P.bytes = slab_blocks_off(P.nrb) + body;
-                    if (!staged) ++n_gather;
+                    if (!staged) ++out.n_gather;
                     rb = nx;
                 }
                 if (P.mode == SLAB_STAGED) {
                     cur.assign(members.begin(), members.end());
                     std::sort(cur.begin(), cur.end());
-                    P.seg_off = (int)seg_all.size();
+                    P.seg_off = (int)out.segs.size();  // within this part; offset at the merge
                     P.nseg = (int)cur.size();
-                    seg_all.insert(seg_all.end(), cur.begin(), cur.end());
-                    P.run_off = (int)run_all.size();
+                    out.segs.insert(out.segs.end(), cur.begin(), cur.end());
+                    P.run_off = (int)out.runs.size();
                     for (size_t i = 0; i < cur.size(); ++i) {
-                        if (i == 0 || cur[i] != cur[i - 1] + 1) run_all.push_back(XRun{cur[i], 0, (uint16_t)i});
-                        run_all.back().nseg++;
+                        if (i == 0 || cur[i] != cur[i - 1] + 1) out.runs.push_back(XRun{cur[i], 0, (uint16_t)i});
+                        out.runs.back().nseg++;
                     }
-                    P.nruns = (int)run_all.size() - P.run_off;
+                    P.nruns = (int)out.runs.size() - P.run_off;
                 }
                 seg_drop_to(0);
-                plans.push_back(P);
-                slab_cta.push_back(g);
+                out.plans.push_back(P);
             }
+            out.nslab.push_back((int)(out.plans.size() - first));
+        }
+    };
+    for (;;) {
+        xseg_max = x32 ? XSEG_MAX32 : XSEG_MAX;
+        segbytes = x32 ? 64u : 128u;
+        rbps = t->opt.rb_per_slab > 0 ? std::min(t->opt.rb_per_slab, RB_PER_SLAB_MAX)
+                                      : (x32 ? RB_PER_SLAB_MAX : RB_PER_SLAB_X64);
+        const unsigned hw = std::thread::hardware_concurrency();
+        const int nth = tilem >= 16384 ? std::max(1, std::min({16, (int)(hw ? hw : 1), G})) : 1;
+        std::vector<Part> parts(nth);
+        if (nth == 1) {
+            plan_ctas(0, G, parts[0]);
+        } else {
+            std::vector<std::thread> th;
+            for (int i = 0; i < nth; ++i)
+                th.emplace_back(plan_ctas, (int)((long long)G * i / nth), (int)((long long)G * (i + 1) / nth),
+                                std::ref(parts[i]));
+            for (auto &x : th) x.join();
+        }
+        plans.clear();
+        seg_all.clear();
+        run_all.clear();
+        slab_cta.clear();
+        cta_slab.assign(G + 1, 0);
+        n_gather = n_over = 0;
+        int g = 0;
+        for (auto &pt : parts) {
+            const int soff = (int)seg_all.size(), roff = (int)run_all.size();
+            size_t k = 0;
+            for (int cnt : pt.nslab) {
+                cta_slab[g] = (int)plans.size();
+                for (int j = 0; j < cnt; ++j, ++k) {
+                    SlabPlan P = pt.plans[k];
+                    if (P.mode == SLAB_STAGED) {
+                        P.seg_off += soff;
+                        P.run_off += roff;
+                    }
+                    plans.push_back(P);
+                    slab_cta.push_back(g);
+                }
+                ++g;
+            }
+            seg_all.insert(seg_all.end(), pt.segs.begin(), pt.segs.end());
+            run_all.insert(run_all.end(), pt.runs.begin(), pt.runs.end());
+            n_gather += pt.n_gather;
+            n_over += pt.n_over;
         }
         cta_slab[G] = (int)plans.size();
         if (x32 && n_over > 0) {
