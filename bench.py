@@ -130,7 +130,8 @@ def _max_over_ranks(dist, value):
         return value
     import torch
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -462,19 +463,10 @@ def batch_arm(args, world, rank, local, dist):
     dev = local
     torch.cuda.set_device(dev)
     sizes = mf.batch_sizes(512, 1000, 200000, 2)
-    # LPT split of the systems over ranks by estimated nnz (17 per row)
-    loads = [0.0] * world
-    mine = []
-    for s in sorted(range(len(sizes)), key=lambda i: -sizes[i]):
-        rk = min(range(world), key=lambda k: loads[k])
-        loads[rk] += float(sizes[s])
-        if rk == rank:
-            mine.append(s)
-    mine.sort()
+    # LPT split of the systems over ranks by size (nnz grows with n)
+    mine = mf.split_systems(sizes, world)[rank]
     t0 = time.perf_counter()
-    mats = mf.generate_spd_batch([sizes[s] for s in mine], seed=2)
-    # generate_spd_batch seeds by position; reseed by global index
-    mats = [mf.Matrix.spd_random(int(sizes[s]), 2 * 1000003 + s + 1) for s in mine] if world > 1 else mats
+    mats = mf.generate_spd_batch([sizes[s] for s in mine], seed=2, index=mine)
     gen_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     bopt = mf.options(device=dev)

@@ -539,13 +539,34 @@ class Tiles:
             pass
 
 
-def generate_spd_batch(sizes, seed=2, threads=16):
+def generate_spd_batch(sizes, seed=2, threads=16, index=None):
     """The random SPD systems of a batch (system s drawn with seed
-    seed * 1000003 + s + 1), generated in parallel host threads."""
+    seed * 1000003 + s + 1), generated in parallel host threads. `index`
+    gives each size's position in the whole batch (default 0, 1, ...), so a
+    rank that holds a subset draws the same systems as a single process."""
     from concurrent.futures import ThreadPoolExecutor
 
+    idx = list(range(len(sizes))) if index is None else [int(i) for i in index]
+    if len(idx) != len(sizes):
+        raise ValueError("index must give one position per size")
     with ThreadPoolExecutor(max_workers=threads) as ex:
-        return list(ex.map(lambda a: Matrix.spd_random(int(a[1]), seed * 1000003 + a[0] + 1), enumerate(sizes)))
+        return list(ex.map(lambda a: Matrix.spd_random(int(a[1]), seed * 1000003 + a[0] + 1), zip(idx, sizes)))
+
+
+def split_systems(sizes, world):
+    """Longest-processing-time split of a batch over `world` ranks: systems
+    in decreasing size, each to the rank with the least load so far (ties to
+    the lowest rank). Returns one ascending index list per rank; every rank
+    computes the same split without communicating."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    loads = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for s in sorted(range(len(sizes)), key=lambda i: (-int(sizes[i]), i)):
+        rk = min(range(world), key=lambda k: (loads[k], k))
+        loads[rk] += float(sizes[s])
+        parts[rk].append(s)
+    return [sorted(p) for p in parts]
 
 
 class Batch:
