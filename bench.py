@@ -452,6 +452,43 @@ def cusparse_arm(args, rank, local):
             "cases": rows}
 
 
+def multi_rhs_arm(args, rank, local):
+    """CG on 16 right-hand sides at once (one shared panel product per
+    iteration) against 16 single-right-hand-side solves of the same columns
+    (the tensor-memory CG kernel), on the 128^3 variable-coefficient Poisson
+    matrix with 16 seeded U[-1, 1] right-hand sides; device time of each
+    solve to 1e-10."""
+    if rank != 0:
+        return None
+    import torch
+
+    mf = importlib.import_module("mille-feillue_b200")
+    torch.cuda.set_device(local)
+    A = mf.Matrix.varpoisson3d(N_GRID)
+    n = A.n
+    B = np.random.default_rng(7).uniform(-1, 1, (n, 16))
+    mf.solve_cg_multi(A, B[:, :2], tol=TOL, maxiter=50)  # warm
+    X, it, rel, multi_ms = mf.solve_cg_multi(A, B, tol=TOL, maxiter=MAXITER)
+    t = mf.Tiles(A)
+    x = torch.zeros(n, dtype=torch.float64, device=f"cuda:{local}")
+    b0 = torch.tensor(np.ascontiguousarray(B[:, 0]), device=f"cuda:{local}")
+    t.solve_cg_dev(b0.data_ptr(), x.data_ptr(), TOL, 50)  # warm
+    single_ms, single_it = 0.0, []
+    for j in range(16):
+        b = torch.tensor(np.ascontiguousarray(B[:, j]), device=f"cuda:{local}")
+        x.zero_()
+        r = t.solve_cg_dev(b.data_ptr(), x.data_ptr(), TOL, MAXITER)
+        single_ms += r["time_ms"]
+        single_it.append(int(r["iterations"]))
+    return {"metric": "16-RHS CG time to 1e-10 (shared panel product) vs 16 single-RHS solves",
+            "value": multi_ms, "unit": "ms", "n_gpus": 1, "higher_is_better": False, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "varpoisson3d 128^3, 16 RHS U[-1,1] seed 7, x0 = 0, CG to 1e-10 per column"},
+            "iterations_min_max": [int(it.min()), int(it.max())], "max_rel_residual": float(rel.max()),
+            "single_rhs_total_ms": single_ms, "single_iterations_min_max": [min(single_it), max(single_it)],
+            "speedup_vs_single_rhs": single_ms / multi_ms}
+
+
 def batch_arm(args, world, rank, local, dist):
     """512 random SPD systems, n log-uniform in [1e3, 2e5] (seed 2), FP64 CG
     to 1e-10: one persistent launch (CUDA-graph replay) against one
@@ -529,7 +566,7 @@ def main():
     ap.add_argument("--cpu-sample-iters", type=int, default=100)
     ap.add_argument("--fp64-iters", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="poisson128", choices=["poisson128", "batch", "vs_cusparse"])
+    ap.add_argument("--workload", default="poisson128", choices=["poisson128", "batch", "vs_cusparse", "multi16"])
     ap.add_argument("--no-each", action="store_true", help="batch: skip the one-launch-per-system comparison")
     ap.add_argument("--batch-group", type=int, default=0, help="batch: CTAs per system group (0 = default)")
     args = ap.parse_args()
@@ -539,8 +576,8 @@ def main():
         if out is not None:
             print(json.dumps(out))
         return
-    if args.workload == "vs_cusparse":
-        out = cusparse_arm(args, rank, local)
+    if args.workload in ("vs_cusparse", "multi16"):
+        out = (cusparse_arm if args.workload == "vs_cusparse" else multi_rhs_arm)(args, rank, local)
         if out is not None:
             print(json.dumps(out))
         return

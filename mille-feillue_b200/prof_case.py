@@ -3,11 +3,14 @@
   python mille-feillue_b200/prof_case.py --kernel spmv --grid 128 --reps 3
   python mille-feillue_b200/prof_case.py --kernel cg --grid 128 --iters 50
   python mille-feillue_b200/prof_case.py --kernel bicgstab --grid 64 --iters 20
+  python mille-feillue_b200/prof_case.py --kernel multi --grid 128 --iters 50
 
 spmv: `reps` launches of the tiled SpMV (k_spmv) on x*.
 cg / bicgstab: one persistent-solver launch with a fixed iteration count
-(0 = to the 1e-10 tolerance). Matrix: the 3D variable-coefficient Poisson
-(cg, spmv) or convection-diffusion (bicgstab) of the given grid.
+(0 = to the 1e-10 tolerance). multi: CG on 16 right-hand sides (U[-1, 1],
+seed 0) for `iters` iterations (panel product, scalar and update kernels).
+Matrix: the 3D variable-coefficient Poisson (cg, spmv, multi) or
+convection-diffusion (bicgstab) of the given grid.
 """
 import argparse
 import importlib
@@ -21,7 +24,7 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel", default="spmv", choices=["spmv", "cg", "pcg", "bicgstab"])
+    ap.add_argument("--kernel", default="spmv", choices=["spmv", "cg", "pcg", "bicgstab", "multi"])
     ap.add_argument("--grid", type=int, default=128)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--iters", type=int, default=50)
@@ -41,6 +44,12 @@ def main():
         A = mf.Matrix.convdiff3d(args.grid)
     else:
         A = mf.Matrix.varpoisson3d(args.grid)
+    if args.kernel == "multi":
+        B = np.random.default_rng(0).uniform(-1, 1, (A.n, 16))
+        X, it, rel, ms = mf.solve_cg_multi(A, B, tol=1e-30, maxiter=args.iters)
+        print("multi 16 rhs: %d iterations %.2f ms -> %.1f us/iteration"
+              % (int(it.max()), ms, ms * 1e3 / max(1, int(it.max()))))
+        return
     kw = {}
     level = -1
     if args.mode == "mixed":

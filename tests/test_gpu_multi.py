@@ -53,3 +53,65 @@ def test_multi_rhs_argument_checks(mf):
                                     mf._ptr(rel), C.byref(ms))
     assert rc == mf.MF_ERR_ARG
     assert b"ascend" in mf.lib().mf_last_error()
+
+
+def _dev_multi(mf, n, rp, ci, v, B, tol=1e-10, maxiter=20000):
+    import ctypes as C
+
+    import torch
+
+    k = B.shape[1]
+    d = lambda a: torch.tensor(np.ascontiguousarray(a), device="cuda")
+    rpd, cid, vd = d(np.asarray(rp, np.int32)), d(np.asarray(ci, np.int32)), d(np.asarray(v, np.float64))
+    Bd = d(np.asfortranarray(B).T.reshape(-1))  # column-major n x k
+    Xd = torch.zeros_like(Bd)
+    it = np.zeros(k, np.int32)
+    rel = np.zeros(k)
+    ms = C.c_double()
+    rc = mf.lib().mf_solve_cg_multi_dev(n, rpd.data_ptr(), cid.data_ptr(), vd.data_ptr(), k, Bd.data_ptr(),
+                                        Xd.data_ptr(), tol, maxiter, mf._ptr(it), mf._ptr(rel), C.byref(ms))
+    torch.cuda.synchronize()
+    return rc, Xd.cpu().numpy().reshape(k, n).T, it, rel
+
+
+@pytest.mark.gpu
+def test_multi_rhs_long_rows_use_csr_loop(mf):
+    """An arrow matrix (first row and column full, 300 entries) is longer
+    than the padded copy takes: the CSR loop solves it."""
+    import scipy.sparse as sp
+
+    n = 300
+    rng = np.random.default_rng(5)
+    D = np.diag(np.full(n, 2.0 * n))
+    D[0, 1:] = rng.uniform(-1, 0, n - 1)
+    D[1:, 0] = D[0, 1:]
+    A = sp.csr_matrix(D)
+    A.sort_indices()
+    B = rng.uniform(-1, 1, (n, 3))
+    rc, X, it, rel = _dev_multi(mf, n, A.indptr, A.indices, A.data, B)
+    assert rc == 0, mf.lib().mf_last_error()
+    for j in range(3):
+        assert np.linalg.norm(B[:, j] - A @ X[:, j]) / np.linalg.norm(B[:, j]) <= 2e-10
+
+
+@pytest.mark.gpu
+def test_multi_rhs_dev_rejects_invalid_csr(mf):
+    A = mf.Matrix.poisson2d(8)
+    n = A.n
+    rp, ci, v = A.csr()
+    B = np.ones((n, 2))
+    bad_col = ci.copy()
+    bad_col[5] = n
+    rc, _, _, _ = _dev_multi(mf, n, rp, bad_col, v, B, maxiter=10)
+    assert rc == mf.MF_ERR_ARG and b"outside" in mf.lib().mf_last_error()
+    bad_rp = rp.copy()
+    bad_rp[3] = bad_rp[4] + 1
+    rc, _, _, _ = _dev_multi(mf, n, bad_rp, ci, v, B, maxiter=10)
+    assert rc == mf.MF_ERR_ARG and b"row_ptr" in mf.lib().mf_last_error()
+    desc = ci.copy()
+    desc[rp[1]:rp[2]] = desc[rp[1]:rp[2]][::-1]
+    rc, _, _, _ = _dev_multi(mf, n, rp, desc, v, B, maxiter=10)
+    assert rc == mf.MF_ERR_ARG and b"ascend" in mf.lib().mf_last_error()
+    # the valid matrix still solves through the same entry point
+    rc, X, _, rel = _dev_multi(mf, n, rp, ci, v, B)
+    assert rc == 0 and rel.max() <= 1e-10
