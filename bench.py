@@ -141,8 +141,34 @@ def _barrier(dist):
         dist.barrier()
 
 
+def _cpu_spmv_reference(O, n, rp, ci, v, x):
+    """The reference's own blockspmv_cpu (compiled unmodified from its
+    sources into oracle/_ref) on the same matrix: serial as in the reference
+    (1 core), best of 10 after 2 warm-ups; its own Tile_create (OpenMP) is
+    timed apart."""
+    if not os.path.exists(O.REF_SO):
+        return {"unavailable": "oracle/_ref/libmfref.so not built (needs the reference sources at build time)"}
+    t0 = time.perf_counter()
+    R = O.RefTiles(n, n, rp, ci, v)
+    create_s = time.perf_counter() - t0
+    times = []
+    for rep in range(12):
+        t0 = time.perf_counter()
+        R.spmv(x)
+        if rep >= 2:
+            times.append(time.perf_counter() - t0)
+    ms = min(times) * 1e3
+    sz = R.sizes
+    alg = 9.0 * sz["csrsize"] + 8.0 * sz["tilenum"] + 16.0 * n  # FP64 values + 1-byte columns, tile index, x, y
+    return {"kind": "reference", "cores": 1, "ms": ms, "alg_bytes": alg, "gbs": alg / ms / 1e6,
+            "tile_create_s": create_s,
+            "sample": "blockspmv_cpu of the reference (serial, as shipped) on the full matrix, FP64; best of 10 "
+                      "after 2 warm-ups, each call with the reference's own per-call allocations"}
+
+
 def cpu_reference_arm(args, rank):
-    """CPU CG of the reference recurrence (oracle port) on all host cores."""
+    """CPU CG of the reference recurrence (oracle port) on all host cores,
+    and the reference's own serial tiled SpMV."""
     if rank != 0:
         return None
     sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -183,6 +209,7 @@ def cpu_reference_arm(args, rank):
     per_it = statistics.median(times)
     value = (statistics.median(fixed) + per_it * iters) * 1e3
     cores = os.cpu_count()
+    spmv_ref = _cpu_spmv_reference(O, n, rp, ci, v, A.xstar())
     return {
         "metric": METRIC, "impl": "reference", "value": value, "unit": "ms", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False,
@@ -194,7 +221,8 @@ def cpu_reference_arm(args, rank):
                                    f"(reference recurrence, tiled SpMV order, OpenMP) on the full matrix per "
                                    f"step; median per-iteration time (their difference) x {iters} iterations "
                                    f"to 1e-10, plus the call's fixed part once", "ms_per_iteration": per_it * 1e3,
-                         "iterations": int(iters), "full_solve_ms": full_ms, "tile_encode_s": enc_s},
+                         "iterations": int(iters), "full_solve_ms": full_ms, "tile_encode_s": enc_s,
+                         "spmv_reference_1core": spmv_ref},
         "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -596,6 +624,9 @@ def main():
         a2.fp64_iters = args.fp64_iters or out["fp64"]["iterations"]
         ref = cpu_reference_arm(a2, 0)
         out["cpu_baseline"] = ref["cpu_baseline"]
+        sr = ref["cpu_baseline"].get("spmv_reference_1core", {})
+        if "ms" in sr:
+            out["spmv"]["fp64"]["speedup_vs_cpu_reference_1core"] = sr["ms"] / out["spmv"]["fp64"]["ms"]
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
