@@ -284,7 +284,10 @@ int mf_true_residual(mf_tiles *t, const double *b_dev, const double *x_dev,
  * matrix streams once per iteration for all of them. B, X: n x k column-major
  * (column j = right-hand side j; X holds x0 on entry). The SpMM keeps
  * blockspmv_cpu's order per column (FP64); the CSR columns must ascend within
- * each row. Per right-hand side: iterations and recursive relative residual;
+ * each row. The _dev variant checks the CSR on the GPU before use (row_ptr[0]
+ * == 0, row_ptr non-decreasing, columns in [0, n) and ascending) and returns
+ * MF_ERR_ARG otherwise; it reads row_ptr[n] entries of col_idx_dev/val_dev.
+ * Per right-hand side: iterations and recursive relative residual;
  * *time_ms = device time of the whole call. MF_ERR_NOT_CONVERGED if any
  * column missed tol within maxiter.                                          */
 int mf_solve_cg_multi(const mf_csr *A, int k, const double *B_host,
