@@ -166,6 +166,26 @@ def _cpu_spmv_reference(O, n, rp, ci, v, x):
                       "after 2 warm-ups, each call with the reference's own per-call allocations"}
 
 
+def _cpu_small_configs(O, mf):
+    """Full oracle solves (all host cores, best of 3) of the two smaller
+    configurations: C1 = CG on the 2D 5-point Poisson 256^2, C2 = BiCGSTAB
+    on the 3D convection-diffusion 64^3, both to 1e-10 from x0 = 0."""
+    out = {}
+    for name, A, solver in (("C1_poisson2d_256_cg", mf.Matrix.poisson2d(256), "cg"),
+                            ("C2_convdiff3d_64_bicgstab", mf.Matrix.convdiff3d(64), "bicgstab")):
+        rp, ci, v = A.csr()
+        b = A.b()
+        o = O.OracleTiles(A.n, A.n, rp, ci, v)
+        best, it, rel = None, 0, 0.0
+        for _ in range(3):
+            t0 = time.perf_counter()
+            it, _, rel = getattr(o, solver)(b, TOL, MAXITER)
+            dt = (time.perf_counter() - t0) * 1e3
+            best = dt if best is None else min(best, dt)
+        out[name] = {"ms": best, "iterations": int(it), "rel_residual": float(rel)}
+    return out
+
+
 def cpu_reference_arm(args, rank):
     """CPU CG of the reference recurrence (oracle port) on all host cores,
     and the reference's own serial tiled SpMV."""
@@ -213,6 +233,7 @@ def cpu_reference_arm(args, rank):
         spmv_ref = _cpu_spmv_reference(O, n, rp, ci, v, A.xstar())
     except (OSError, RuntimeError, ValueError) as e:  # the solve's baseline stands without it
         spmv_ref = {"unavailable": f"{type(e).__name__}: {e}"}
+    small = _cpu_small_configs(O, mf)
     return {
         "metric": METRIC, "impl": "reference", "value": value, "unit": "ms", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False,
@@ -225,7 +246,7 @@ def cpu_reference_arm(args, rank):
                                    f"step; median per-iteration time (their difference) x {iters} iterations "
                                    f"to 1e-10, plus the call's fixed part once", "ms_per_iteration": per_it * 1e3,
                          "iterations": int(iters), "full_solve_ms": full_ms, "tile_encode_s": enc_s,
-                         "spmv_reference_1core": spmv_ref},
+                         "spmv_reference_1core": spmv_ref, "other_configs": small},
         "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 

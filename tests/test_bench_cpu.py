@@ -1,5 +1,6 @@
 """CPU legs of bench.py: the reference's own serial tiled SpMV timing
-returns a well-formed record, and its product is the oracle's."""
+returns a well-formed record (and its product is the oracle's), and the CPU
+solves of the two smaller configurations reach the tolerance."""
 import numpy as np
 
 
@@ -17,3 +18,12 @@ def test_cpu_spmv_reference_record(mf, O):
     assert r["alg_bytes"] == 9.0 * len(v) + 8.0 * tiles.sizes["tilenum"] + 16.0 * A.n
     y, _, _, _ = tiles.spmv(A.xstar())
     assert np.array_equal(y, O.OracleTiles(A.n, A.n, rp, ci, v).spmv(A.xstar()))
+
+
+def test_cpu_small_configs(mf, O):
+    import bench
+
+    r = bench._cpu_small_configs(O, mf)
+    assert set(r) == {"C1_poisson2d_256_cg", "C2_convdiff3d_64_bicgstab"}
+    for v in r.values():
+        assert v["ms"] > 0 and v["iterations"] > 0 and v["rel_residual"] <= bench.TOL
