@@ -614,7 +614,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="mixed", choices=["fp64", "mixed"])
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-sample-iters", type=int, default=100)
     ap.add_argument("--fp64-iters", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
