@@ -195,6 +195,9 @@ def cpu_reference_arm(args, rank):
     mf = importlib.import_module("mille-feillue_b200")
     import _oracle as O
 
+    # every host core this process may run on (torchrun sets OMP_NUM_THREADS=1)
+    cores = O.set_threads(len(os.sched_getaffinity(0)))
+
     A = mf.Matrix.varpoisson3d(N_GRID)
     n = A.n
     rp, ci, v = A.csr()
@@ -228,7 +231,6 @@ def cpu_reference_arm(args, rank):
             fixed.append(max(0.0, (t1 - t0) - per * sample_iters))
     per_it = statistics.median(times)
     value = (statistics.median(fixed) + per_it * iters) * 1e3
-    cores = os.cpu_count()
     try:
         spmv_ref = _cpu_spmv_reference(O, n, rp, ci, v, A.xstar())
     except (OSError, RuntimeError, ValueError) as e:  # the solve's baseline stands without it

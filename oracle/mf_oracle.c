@@ -7,6 +7,7 @@
 #include "mf_oracle.h"
 
 #include <math.h>
+#include <omp.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -704,4 +705,9 @@ float mfo_mlp_grad(const float *W1, const float *b1, const float *W2, const floa
         }
     }
     return (float)(loss / batch);
+}
+
+int mfo_set_threads(int n) {
+    if (n > 0) omp_set_num_threads(n);
+    return omp_get_max_threads();
 }

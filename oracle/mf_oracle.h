@@ -105,6 +105,12 @@ float mfo_mlp_grad(const float *W1, const float *b1, const float *W2, const floa
                    int batch, float *gW1, float *gb1, float *gW2, float *gb2, float *gW3,
                    float *gb3);
 
+/* OpenMP threads of the calling thread's later parallel regions (n > 0;
+ * n <= 0 leaves them); returns the count now in effect. A launcher such as
+ * torchrun sets OMP_NUM_THREADS=1 per process, which a timed CPU baseline
+ * overrides here to use every host core it may run on. */
+int mfo_set_threads(int n);
+
 #ifdef __cplusplus
 }
 #endif

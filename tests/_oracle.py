@@ -44,6 +44,8 @@ def lib():
         _lib = C.CDLL(ORACLE_SO)
         L = _lib
         L.mfo_tile_create.argtypes = [_i, _i, _p, _p, _p, C.POINTER(MfoTiles)]
+        L.mfo_set_threads.argtypes = [_i]
+        L.mfo_set_threads.restype = _i
         L.mfo_tiles_free.argtypes = [C.POINTER(MfoTiles)]
         L.mfo_blockspmv.argtypes = [C.POINTER(MfoTiles), _p, _p, _p, _p, _p]
         L.mfo_row_compress.argtypes = [C.POINTER(MfoTiles), _p, _p, _p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
@@ -294,6 +296,12 @@ class RefTiles:
             ref().ref_tile_free(self.h)
         except Exception:
             pass
+
+
+def set_threads(n):
+    """OpenMP threads of the oracle's (and the reference code's) parallel
+    loops on this thread; returns the count in effect."""
+    return int(lib().mfo_set_threads(int(n)))
 
 
 def ref_read_mtx(path):

@@ -1,7 +1,8 @@
 """The multi-rank path on CPU: two gloo ranks take the steps bench.py takes
 under torchrun (the batch workload's longest-processing-time split, the
-barrier, the max over ranks of the step time), and the split itself is a
-balanced partition that every rank computes identically."""
+barrier, the max over ranks of the step time), the split itself is a
+balanced partition that every rank computes identically, and the CPU
+reference arm runs under torchrun with two ranks."""
 import json
 import multiprocessing as mp
 import os
@@ -84,3 +85,26 @@ def test_two_gloo_ranks(mf, tmp_path):
     assert sorted(seen) == list(range(len(small)))
     for i, m in enumerate(whole):
         assert seen[i] == (int(m.info()[2]), float(m.csr()[2].sum()))
+
+
+def test_reference_arm_under_torchrun_two_ranks():
+    """`bench.py --impl reference` launched as the scaling run launches it:
+    rank 0 alone prints one JSON line, rank 1 exits 0 without work, and the
+    CPU baseline uses every core the process may run on although torchrun
+    sets OMP_NUM_THREADS=1 (short samples keep the test quick)."""
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(_free_port()), os.path.join(root, "bench.py"),
+           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "1", "--cpu-sample-iters", "5",
+           "--fp64-iters", "50"]
+    p = subprocess.run(cmd, cwd=root, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = [ln for ln in p.stdout.splitlines() if ln.strip()]
+    assert len(lines) == 1, p.stdout
+    r = json.loads(lines[0])
+    assert r["impl"] == "reference" and r["n_gpus"] == 2 and r["value"] > 0
+    assert r["cpu_baseline"]["cores"] == len(os.sched_getaffinity(0))
+    assert r["e2e"]["h2d_bytes_per_step"] == 0 and r["e2e"]["value"] == r["value"]
