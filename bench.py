@@ -16,8 +16,9 @@ shard (every iteration needs grid-wide dot products), so each rank solves
 its own replica (weak scaling, replicas only); the time is the max over
 ranks. The reference arm times the CPU implementation of the same solve
 (the oracle's restatement of the reference recurrence with the reference's
-tiled SpMV order, OpenMP over all host cores) on a bounded sample of
-iterations and projects the full solve by the iteration count.
+tiled SpMV order, OpenMP over all host cores): one whole solve to the
+tolerance per step, on a matrix built by the oracle's own generator (the
+product library is not loaded in that arm).
 """
 import argparse
 import ctypes as C
@@ -39,9 +40,6 @@ METRIC = "solve time to 1e-10 true residual & SpMV HBM GB/s: mixed vs FP64, same
 N_GRID = 128
 TOL = 1e-10
 MAXITER = 40000
-# Iterations of the FP64 recurrence to 1e-10 on this matrix, used to project
-# the CPU arm's sampled per-iteration time to a full solve. Measured by the
-# GPU FP64 solve, whose count the tests hold within 2 % of the CPU oracle.
 
 
 def _peaks():
@@ -166,91 +164,85 @@ def _cpu_spmv_reference(O, n, rp, ci, v, x):
                       "after 2 warm-ups, each call with the reference's own per-call allocations"}
 
 
-def _cpu_small_configs(O, mf):
+def _cpu_small_configs(O):
     """Full oracle solves (all host cores, best of 3) of the two smaller
     configurations: C1 = CG on the 2D 5-point Poisson 256^2, C2 = BiCGSTAB
     on the 3D convection-diffusion 64^3, both to 1e-10 from x0 = 0."""
     out = {}
-    for name, A, solver in (("C1_poisson2d_256_cg", mf.Matrix.poisson2d(256), "cg"),
-                            ("C2_convdiff3d_64_bicgstab", mf.Matrix.convdiff3d(64), "bicgstab")):
-        rp, ci, v = A.csr()
-        b = A.b()
-        o = O.OracleTiles(A.n, A.n, rp, ci, v)
+    for name, S, solver in (("C1_poisson2d_256_cg", O.gen_poisson2d(256), "cg"),
+                            ("C2_convdiff3d_64_bicgstab", O.gen_convdiff3d(64), "bicgstab")):
+        o = O.OracleTiles(S.n, S.n, *S.csr())
         best, it, rel = None, 0, 0.0
         for _ in range(3):
             t0 = time.perf_counter()
-            it, _, rel = getattr(o, solver)(b, TOL, MAXITER)
+            it, _, rel = getattr(o, solver)(S.b, TOL, MAXITER)
             dt = (time.perf_counter() - t0) * 1e3
             best = dt if best is None else min(best, dt)
         out[name] = {"ms": best, "iterations": int(it), "rel_residual": float(rel)}
     return out
 
 
-def cpu_reference_arm(args, rank):
-    """CPU CG of the reference recurrence (oracle port) on all host cores,
-    and the reference's own serial tiled SpMV."""
+def _config(world, grid):
+    """The workload of both arms (identical keys and values). The 7-point
+    matrix of a grid^3 problem has 7 n - 6 grid^2 nonzeros."""
+    l2 = ("matrix (172 MB in the FP64 tile format) larger than the 126 MB L2; not flushed" if grid == 128
+          else "reduced grid (test size): the matrix may sit in L2; not flushed")
+    return {"workload": f"varpoisson3d_{grid} CG to 1e-10 true residual", "n": grid ** 3,
+            "nnz": 7 * grid ** 3 - 6 * grid ** 2, "x0": "zeros", "tol": TOL,
+            "parallelism": "replicas" if world > 1 else "single", "l2": l2}
+
+
+def cpu_reference_arm(args, rank, world=1, small=True):
+    """CPU CG of the reference recurrence (the oracle's restatement, tiled
+    SpMV in the reference's order, OpenMP over all host cores): every step is
+    one whole solve of the headline system to the tolerance, timed on its
+    own. The matrix comes from the oracle's generator; the product library
+    is not loaded. Beside it, the reference's own serial blockspmv_cpu."""
     if rank != 0:
         return None
     sys.path.insert(0, os.path.join(ROOT, "tests"))
-    mf = importlib.import_module("mille-feillue_b200")
     import _oracle as O
 
     # every host core this process may run on (torchrun sets OMP_NUM_THREADS=1)
     cores = O.set_threads(len(os.sched_getaffinity(0)))
 
-    A = mf.Matrix.varpoisson3d(N_GRID)
-    n = A.n
-    rp, ci, v = A.csr()
-    b = A.b()
+    S = O.gen_varpoisson3d(args.grid)
+    n = S.n
+    rp, ci, v = S.csr()
     t0 = time.perf_counter()
     o = O.OracleTiles(n, n, rp, ci, v)
     enc_s = time.perf_counter() - t0
-    sample_iters = args.cpu_sample_iters
-    # iterations to the tolerance: given by the GPU leg of the default run,
-    # else one full oracle solve counts them (and is timed as a whole)
-    iters = args.fp64_iters
-    full_ms = None
-    if not iters:
-        t0 = time.perf_counter()
-        iters, _, _ = o.cg(b, TOL, MAXITER)
-        full_ms = (time.perf_counter() - t0) * 1e3
-    # each step times a short and a long sample (tol 0: exactly that many
-    # iterations); their difference is the cost of sample_iters iterations
-    # alone, the short one less its iterations is the call's fixed part (x
-    # set-up, the initial residual SpMV, thread start-up), counted once
-    times, fixed = [], []
+    times, iters, rel, err = [], 0, 0.0, None
     for step in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        o.cg(b, 0.0, sample_iters)
-        t1 = time.perf_counter()
-        o.cg(b, 0.0, 2 * sample_iters)
-        t2 = time.perf_counter()
+        iters, x, rel = o.cg(S.b, TOL, MAXITER)
+        dt = (time.perf_counter() - t0) * 1e3
         if step >= args.warmup:
-            per = ((t2 - t1) - (t1 - t0)) / sample_iters
-            times.append(per)
-            fixed.append(max(0.0, (t1 - t0) - per * sample_iters))
-    per_it = statistics.median(times)
-    value = (statistics.median(fixed) + per_it * iters) * 1e3
+            times.append(dt)
+            err = float(np.linalg.norm(x - S.xstar) / np.linalg.norm(S.xstar))
+    value = statistics.median(times)
     try:
-        spmv_ref = _cpu_spmv_reference(O, n, rp, ci, v, A.xstar())
+        spmv_ref = _cpu_spmv_reference(O, n, rp, ci, v, S.xstar)
     except (OSError, RuntimeError, ValueError) as e:  # the solve's baseline stands without it
         spmv_ref = {"unavailable": f"{type(e).__name__}: {e}"}
-    small = _cpu_small_configs(O, mf)
-    return {
+    out = {
         "metric": METRIC, "impl": "reference", "value": value, "unit": "ms", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "varpoisson3d_128 CG to 1e-10 true residual", "n": n, "nnz": int(len(v)),
-                   "x0": "zeros", "tol": TOL},
+        "config": _config(world, args.grid), "mode": "fp64",
         "cpu_baseline": {"value": value, "unit": "ms", "cores": cores, "kind": "port",
-                         "sample": f"{sample_iters} and {2 * sample_iters} CG iterations of the oracle "
-                                   f"(reference recurrence, tiled SpMV order, OpenMP) on the full matrix per "
-                                   f"step; median per-iteration time (their difference) x {iters} iterations "
-                                   f"to 1e-10, plus the call's fixed part once", "ms_per_iteration": per_it * 1e3,
-                         "iterations": int(iters), "full_solve_ms": full_ms, "tile_encode_s": enc_s,
-                         "spmv_reference_1core": spmv_ref, "other_configs": small},
+                         "sample": f"one whole FP64 CG solve to 1e-10 per step ({int(iters)} iterations of the "
+                                   f"oracle: reference recurrence, tiled SpMV in the reference's order, OpenMP on "
+                                   f"{cores} threads), median of {args.steps} steps after {args.warmup} warm-up "
+                                   f"solves; matrix from the oracle's generator",
+                         "iterations": int(iters), "rel_residual": float(rel), "x_err_vs_xstar": err,
+                         "step_ms_min_max": [min(times), max(times)], "tile_encode_s": enc_s,
+                         "spmv_reference_1core": spmv_ref},
         "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if small:
+        out["cpu_baseline"]["other_configs"] = _cpu_small_configs(O)
+    return out
 
 
 def _time_solves(torch, tiles, bd, xd, opts, steps, warmup, dist, solver="cg"):
@@ -282,7 +274,7 @@ def gpu_arm(args, world, rank, local, dist):
     mf = importlib.import_module("mille-feillue_b200")
     dev = local
     torch.cuda.set_device(dev)
-    A = mf.Matrix.varpoisson3d(N_GRID)
+    A = mf.Matrix.varpoisson3d(args.grid)
     n = A.n
     rp, ci, v = A.csr()
     b = A.b()
@@ -331,6 +323,12 @@ def gpu_arm(args, world, rank, local, dist):
     errmx = float(np.linalg.norm(xmx - xstar) / np.linalg.norm(xstar))
     mx_vs_64 = float(np.linalg.norm(xmx - x64) / nx)
     ms, kms, res = (msmx, kmx, resmx) if headline == "mixed" else (ms64, k64, res64)
+    if headline == "mixed":
+        names = ("FP64", "FP32", "FP16", "FP8-E4M3")
+        used = [f"{names[i]} {100 * f:.0f}%" for i, f in enumerate(resmx["tile_frac"]) if f > 0]
+        dtype = "mixed: tile values " + ", ".join(used) + "; FP64 vectors, dots, scalars"
+    else:
+        dtype = "f64"
 
     # ---- end to end through the C ABI with pinned host buffers:
     # CSR + b host->device, GPU encode, persistent solve, x device->host
@@ -383,12 +381,9 @@ def gpu_arm(args, world, rank, local, dist):
         out = {
             "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "varpoisson3d_128 CG to 1e-10 true residual", "n": n, "nnz": int(len(v)),
-                       "mode": headline, "x0": "zeros", "tol": TOL,
-                       "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "matrix (%.0f MB FP64) larger than L2; not flushed" % (spmv_bytes / 1e6),
-                       "ctas": info["nctas"], "slabs": info["nslabs"]},
+            "vs_baseline": None, "dtype": dtype, "data": "synthetic",
+            "config": _config(world, args.grid), "mode": headline,
+            "layout": {"ctas": info["nctas"], "slabs": info["nslabs"], "spmv_fp64_alg_bytes": spmv_bytes},
             "iterations": res["iterations"], "rel_residual_true": res["rel_residual_true"],
             "mixed": {"ms": msmx, "kernel_ms": kmx, "iterations": resmx["iterations"],
                       "iters_per_level": resmx["iters_level"], "replacements": resmx["replacements"],
@@ -609,6 +604,92 @@ def batch_arm(args, world, rank, local, dist):
     }
 
 
+def profile_case(args):
+    """One kernel of the solver on a fixed workload, for profilers
+    (`--workload profile`):
+
+      spmv      `--reps` launches of the tiled SpMV (k_spmv) on x*; with
+                `--time`, the CUDA-event time of 50-launch batches instead
+      cg / pcg  one persistent-solver launch of `--iters` iterations
+                (0 = to the 1e-10 tolerance); `--trace N` prints the median
+                phase times of the first N CG iterations
+      bicgstab  the same on the convection-diffusion matrix
+      multi     CG on 16 right-hand sides (U[-1, 1], seed 0), `--iters`
+                iterations (panel product, scalar and update kernels)
+
+    Matrix: the 3D variable-coefficient Poisson (cg, pcg, spmv, multi) or
+    convection-diffusion (bicgstab) of `--grid`. `--prec` picks the storage:
+    fp64, mixed (the magnitude rule's first level), or all tiles fixed at
+    fp32 / fp16 / fp8."""
+    import torch
+
+    mf = importlib.import_module("mille-feillue_b200")
+    A = mf.Matrix.convdiff3d(args.grid) if args.kernel == "bicgstab" else mf.Matrix.varpoisson3d(args.grid)
+    if args.kernel == "multi":
+        B = np.random.default_rng(0).uniform(-1, 1, (A.n, 16))
+        X, it, rel, ms = mf.solve_cg_multi(A, B, tol=1e-30, maxiter=args.iters)
+        print("multi 16 rhs: %d iterations %.2f ms -> %.1f us/iteration"
+              % (int(it.max()), ms, ms * 1e3 / max(1, int(it.max()))))
+        return
+    prec = args.prec or args.mode
+    kw, level = {}, -1
+    if prec == "mixed":
+        kw, level = dict(precision_mode=mf.MODE_MIXED_RULE), 0
+    elif prec in ("fp32", "fp16", "fp8"):
+        kw = dict(precision_mode=mf.MODE_FIXED, fixed_precision={"fp32": 1, "fp16": 2, "fp8": 3}[prec])
+        level = 0
+    kw.update(slab_bytes=args.slab_bytes, rb_per_slab=args.rb_per_slab, ctas_per_sm=args.ctas_per_sm)
+    opts = mf.options(**kw)
+    if args.prefetch:
+        opts.reserved[3] = 1
+    t = mf.Tiles(A, opts)
+    n = A.n
+    b = torch.tensor(A.b(), device="cuda")
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    if args.kernel == "spmv":
+        xs = torch.tensor(A.xstar() if A.xstar() is not None else np.ones(n), device="cuda")
+        if args.time:
+            ms, nbytes = t.spmv_bench(xs.data_ptr(), x.data_ptr(), args.reps, level)
+            inf = t.info()
+            print(f"spmv slab_bytes={args.slab_bytes} rb_per_slab={args.rb_per_slab} ctas={inf['nctas']} "
+                  f"slabs={inf['nslabs']} ms={ms:.4f} GB/s={nbytes / ms / 1e6:.0f}")
+            return
+        for _ in range(args.reps):
+            if level >= 0:
+                t.spmv_level_dev(level, xs.data_ptr(), x.data_ptr())
+            else:
+                t.spmv_dev(xs.data_ptr(), x.data_ptr())
+        torch.cuda.synchronize()
+        print("spmv done", float(x.abs().sum()))
+        return
+    o = mf.options(fixed_iterations=args.iters, **kw)
+    if args.trace > 0:
+        o.reserved[1] = args.trace
+    if args.prefetch:
+        o.reserved[3] = 1
+    if args.no_tmem:
+        o.reserved[5] = 1
+    if args.kernel in ("cg", "pcg"):
+        fn = t.solve_cg_dev if args.kernel == "cg" else t.solve_pcg_dev
+        res = fn(b.data_ptr(), x.data_ptr(), 1e-10, MAXITER, o)
+        if args.trace > 0:
+            tr = t.trace(args.trace).astype(np.float64)
+            tr = tr[(tr[:, 0] > 0) & (tr[:, 6] > 0)]
+            names = ["halo wait", "SpMV", "dot d.q", "r update", "dot r.r", "x/d update+publish"]
+            if prec != "fp64":  # single-reduction CG
+                names = ["halo wait", "SpMV (w = A r)", "reduction (r.r, w.r)", "p,s,x,r update", "-", "publish"]
+            d = np.diff(tr[:, :7], axis=1) / 1e3
+            it_us = np.diff(tr[:, 0]) / 1e3
+            print("trace over %d iterations (us, median):" % len(tr))
+            for k, nm in enumerate(names):
+                print("  %-22s %8.2f" % (nm, np.median(d[:, k])))
+            print("  %-22s %8.2f" % ("iteration", np.median(it_us)))
+    else:
+        res = t.solve_bicgstab_dev(b.data_ptr(), x.data_ptr(), 1e-10, 10000, o)
+    torch.cuda.synchronize()
+    print(args.kernel, res)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -616,17 +697,34 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--grid", type=int, default=N_GRID,
+                    help="grid edge of the headline Poisson system (128 = the measured configuration; "
+                         "smaller only for quick checks)")
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--cpu-sample-iters", type=int, default=100)
-    ap.add_argument("--fp64-iters", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="poisson128", choices=["poisson128", "batch", "vs_cusparse", "multi16"])
+    ap.add_argument("--workload", default="poisson128",
+                    choices=["poisson128", "batch", "vs_cusparse", "multi16", "profile"])
+    # --workload profile: one kernel on a fixed case, for profilers (profile_case)
+    ap.add_argument("--kernel", default="spmv", choices=["spmv", "cg", "pcg", "bicgstab", "multi"])
+    ap.add_argument("--prec", default=None, choices=["fp64", "mixed", "fp32", "fp16", "fp8"])
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--iters", type=int, default=50)
+    ap.add_argument("--slab-bytes", type=int, default=0)
+    ap.add_argument("--rb-per-slab", type=int, default=0)
+    ap.add_argument("--ctas-per-sm", type=int, default=0)
+    ap.add_argument("--time", action="store_true")
+    ap.add_argument("--trace", type=int, default=0)
+    ap.add_argument("--prefetch", action="store_true")
+    ap.add_argument("--no-tmem", action="store_true")
     ap.add_argument("--no-each", action="store_true", help="batch: skip the one-launch-per-system comparison")
     ap.add_argument("--batch-group", type=int, default=0, help="batch: CTAs per system group (0 = default)")
     args = ap.parse_args()
+    if args.workload == "profile":
+        profile_case(args)
+        return
     world, rank, local, dist = _dist_setup(args)
     if args.impl == "reference":
-        out = cpu_reference_arm(args, rank)
+        out = cpu_reference_arm(args, rank, world)
         if out is not None:
             print(json.dumps(out))
         return
@@ -645,9 +743,9 @@ def main():
         return
     out = gpu_arm(args, world, rank, local, dist)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # one whole oracle solve (about 10 s of CPU work)
         a2 = argparse.Namespace(**vars(args))
-        a2.steps, a2.warmup = 1, 1
-        a2.fp64_iters = args.fp64_iters or out["fp64"]["iterations"]
+        a2.steps, a2.warmup = 1, 0
         ref = cpu_reference_arm(a2, 0)
         out["cpu_baseline"] = ref["cpu_baseline"]
         sr = ref["cpu_baseline"].get("spmv_reference_1core", {})

@@ -263,8 +263,10 @@ int mf_solve_bicgstab_dev(mf_tiles *t, const double *b_dev, double *x_dev,
  * Limit: n rounded up to 16 <= MF_NOALLOC_MAX_ROWS, else MF_ERR_ARG.
  * Always FP64 (mixed layouts unused); time_ms is 0; reserved[1] is ignored.
  * The first call on a device sets up (looks up the scratch address): make it
- * before any stream capture. One scratch per device: overlapping calls on one
- * device race and must be serialized by the caller.                        */
+ * before any stream capture. The address is kept for the life of the
+ * process, so cudaDeviceReset on that device makes later calls invalid.
+ * One scratch per device: overlapping calls on one device race and must be
+ * serialized by the caller.                                                */
 #define MF_NOALLOC_MAX_ROWS 131072
 int mf_solve_cg_dev_noalloc(mf_tiles *t, const double *b_dev, double *x_dev,
                             double tol, int maxiter, const mf_options *opt,

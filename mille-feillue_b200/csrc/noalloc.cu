@@ -16,7 +16,9 @@
 //
 // Set-up: the first call on each device (with that device current) looks up
 // the scratch address with cudaGetSymbolAddress. Make that first call before
-// any stream capture begins.
+// any stream capture begins. The address is cached for the life of the
+// process: a cudaDeviceReset on that device invalidates it, and calls after
+// such a reset are not supported.
 //
 // Concurrency: there is one scratch per device, so calls in flight at the same
 // time on one device (from two threads, or on two streams) race on it. Callers

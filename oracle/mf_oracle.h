@@ -105,6 +105,22 @@ float mfo_mlp_grad(const float *W1, const float *b1, const float *W2, const floa
                    int batch, float *gW1, float *gb1, float *gW2, float *gb2, float *gW3,
                    float *gb3);
 
+/* A generated system: 0-based CSR (columns ascending), right-hand side b and,
+ * where the workload defines one, the exact solution x* (else NULL). All
+ * arrays are malloc'ed; mfo_system_free releases them. */
+typedef struct {
+    int n, nnz;
+    int *row_ptr, *col_idx;
+    double *val, *b, *xstar;
+} mfo_system;
+
+/* The synthetic workloads (oracle/workloads.c). Return 0, or -1 on bad
+ * arguments / allocation failure. */
+int mfo_gen_poisson2d(int N, mfo_system *m);
+int mfo_gen_convdiff3d(int N, double vx, double vy, double vz, uint64_t seed, mfo_system *m);
+int mfo_gen_varpoisson3d(int N, double klo, double khi, uint64_t seed, mfo_system *m);
+void mfo_system_free(mfo_system *m);
+
 /* OpenMP threads of the calling thread's later parallel regions (n > 0;
  * n <= 0 leaves them); returns the count now in effect. A launcher such as
  * torchrun sets OMP_NUM_THREADS=1 per process, which a timed CPU baseline

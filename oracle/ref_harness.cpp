@@ -115,6 +115,17 @@ int ref_read_mtx(const char *path, int *m, int *n, int *nnz, int **rp, int **ci,
     return sym;
 }
 
+// binary_read_csr (biio.h:22-72): the .cbd file into malloc'd arrays (row
+// pointers are 64-bit there). Returns its status (0 ok, -1 failure).
+int ref_read_cbd(const char *path, int *m, int *n, int64_t *nnz, int64_t **rp, int **ci, double **val) {
+    return binary_read_csr(m, n, nnz, rp, ci, val, (char *)path);
+}
+
+// binary_write_csr (biio.h:74-97).
+void ref_write_cbd(const char *path, int m, int n, int64_t nnz, int64_t *rp, int *ci, double *val) {
+    binary_write_csr(m, n, nnz, rp, ci, val, (char *)path);
+}
+
 void ref_free(void *p) { free(p); }
 
 }  // extern "C"

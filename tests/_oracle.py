@@ -76,7 +76,58 @@ def lib():
         L.mfo_mlp_forward.restype = C.c_float
         L.mfo_mlp_grad.argtypes = [_p] * 8 + [_i] + [_p] * 6
         L.mfo_mlp_grad.restype = C.c_float
+        L.mfo_gen_poisson2d.argtypes = [_i, C.POINTER(MfoSystem)]
+        L.mfo_gen_convdiff3d.argtypes = [_i, C.c_double, C.c_double, C.c_double, C.c_uint64, C.POINTER(MfoSystem)]
+        L.mfo_gen_varpoisson3d.argtypes = [_i, C.c_double, C.c_double, C.c_uint64, C.POINTER(MfoSystem)]
+        for f in ("mfo_gen_poisson2d", "mfo_gen_convdiff3d", "mfo_gen_varpoisson3d"):
+            getattr(L, f).restype = _i
+        L.mfo_system_free.argtypes = [C.POINTER(MfoSystem)]
     return _lib
+
+
+class MfoSystem(C.Structure):
+    _fields_ = [("n", _i), ("nnz", _i), ("row_ptr", C.POINTER(C.c_int)), ("col_idx", C.POINTER(C.c_int)),
+                ("val", C.POINTER(C.c_double)), ("b", C.POINTER(C.c_double)), ("xstar", C.POINTER(C.c_double))]
+
+
+class System:
+    """A synthetic workload generated by the oracle (oracle/workloads.c):
+    n, CSR (rp, ci, v), b and x* (None where the workload has none)."""
+
+    def __init__(self, fn, *args):
+        m = MfoSystem()
+        rc = getattr(lib(), fn)(*args, C.byref(m))
+        if rc != 0:
+            raise ValueError(f"{fn}{args}: bad arguments")
+        try:
+            n, nnz = m.n, m.nnz
+            self.n = n
+            self.rp = np.ctypeslib.as_array(m.row_ptr, shape=(n + 1,)).copy()
+            self.ci = np.ctypeslib.as_array(m.col_idx, shape=(nnz,)).copy() if nnz else np.zeros(0, np.int32)
+            self.v = np.ctypeslib.as_array(m.val, shape=(nnz,)).copy() if nnz else np.zeros(0)
+            self.b = np.ctypeslib.as_array(m.b, shape=(n,)).copy()
+            self.xstar = np.ctypeslib.as_array(m.xstar, shape=(n,)).copy() if m.xstar else None
+        finally:
+            lib().mfo_system_free(C.byref(m))
+
+    def csr(self):
+        return self.rp, self.ci, self.v
+
+
+def gen_poisson2d(N):
+    """2D 5-point Laplacian, N x N grid, b = A * ones."""
+    return System("mfo_gen_poisson2d", N)
+
+
+def gen_convdiff3d(N, v=(1.0, 0.5, 0.25), seed=0):
+    """3D 7-point upwind convection-diffusion, N^3 grid, b ~ U[-1, 1]."""
+    return System("mfo_gen_convdiff3d", N, v[0], v[1], v[2], seed)
+
+
+def gen_varpoisson3d(N, klo=1e-3, khi=1e3, seed=1):
+    """3D 7-point variable-coefficient Poisson, N^3 grid, faces logU[klo, khi],
+    b = A x*, x* ~ U[0, 1]."""
+    return System("mfo_gen_varpoisson3d", N, klo, khi, seed)
 
 
 # MLP weight blocks inside the packed weight vector: W1[64][6], b1[64],
@@ -111,6 +162,17 @@ def ref_available():
     return os.path.exists(REF_SO)
 
 
+def ref_tree():
+    """The reference's Performance-Comparison directory the harness was built
+    from (recorded by oracle/Makefile), or None where it is absent."""
+    try:
+        with open(os.path.join(ROOT, "oracle", "_ref", "ref_dir.txt")) as f:
+            d = f.read().strip()
+        return d if os.path.isdir(d) else None
+    except OSError:
+        return None
+
+
 def ref():
     global _ref
     if _ref is None:
@@ -127,6 +189,11 @@ def ref():
                                    C.POINTER(C.POINTER(_i)), C.POINTER(C.POINTER(_i)), C.POINTER(C.POINTER(C.c_double))]
         R.ref_read_mtx.restype = _i
         R.ref_free.argtypes = [_p]
+        R.ref_read_cbd.argtypes = [C.c_char_p, C.POINTER(_i), C.POINTER(_i), C.POINTER(C.c_int64),
+                                   C.POINTER(C.POINTER(C.c_int64)), C.POINTER(C.POINTER(_i)),
+                                   C.POINTER(C.POINTER(C.c_double))]
+        R.ref_read_cbd.restype = _i
+        R.ref_write_cbd.argtypes = [C.c_char_p, _i, _i, C.c_int64, _p, _p, _p]
     return _ref
 
 
@@ -316,3 +383,29 @@ def ref_read_mtx(path):
     for p in (rp, ci, va):
         ref().ref_free(C.cast(p, _p))
     return m.value, n.value, R, CI, V
+
+
+def ref_read_cbd(path):
+    """The reference's binary_read_csr: (rows, cols, row_ptr int64, col, val)."""
+    m, n, nnz = _i(), _i(), C.c_int64()
+    rp = C.POINTER(C.c_int64)()
+    ci = C.POINTER(_i)()
+    va = C.POINTER(C.c_double)()
+    rc = ref().ref_read_cbd(path.encode(), C.byref(m), C.byref(n), C.byref(nnz), C.byref(rp), C.byref(ci),
+                            C.byref(va))
+    if rc != 0:
+        raise OSError(f"binary_read_csr failed on {path}")
+    R = np.ctypeslib.as_array(rp, shape=(m.value + 1,)).copy()
+    CI = np.ctypeslib.as_array(ci, shape=(nnz.value,)).copy()
+    V = np.ctypeslib.as_array(va, shape=(nnz.value,)).copy()
+    for p in (rp, ci, va):
+        ref().ref_free(C.cast(p, _p))
+    return m.value, n.value, R, CI, V
+
+
+def ref_write_cbd(path, m, n, rp, ci, v):
+    """The reference's binary_write_csr of a CSR matrix (row_ptr widened to int64)."""
+    rp64 = np.ascontiguousarray(rp, np.int64)
+    ci = np.ascontiguousarray(ci, np.int32)
+    v = np.ascontiguousarray(v, np.float64)
+    ref().ref_write_cbd(path.encode(), m, n, int(rp64[-1]), _ptr(rp64), _ptr(ci), _ptr(v))

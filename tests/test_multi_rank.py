@@ -91,15 +91,14 @@ def test_reference_arm_under_torchrun_two_ranks():
     """`bench.py --impl reference` launched as the scaling run launches it:
     rank 0 alone prints one JSON line, rank 1 exits 0 without work, and the
     CPU baseline uses every core the process may run on although torchrun
-    sets OMP_NUM_THREADS=1 (short samples keep the test quick)."""
+    sets OMP_NUM_THREADS=1 (a 24^3 grid keeps the test quick)."""
     import subprocess
     import sys
 
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(_free_port()), os.path.join(root, "bench.py"),
-           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "1", "--cpu-sample-iters", "5",
-           "--fp64-iters", "50"]
+           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "1", "--grid", "24"]
     p = subprocess.run(cmd, cwd=root, capture_output=True, text=True, timeout=600)
     assert p.returncode == 0, p.stderr[-2000:]
     lines = [ln for ln in p.stdout.splitlines() if ln.strip()]
