@@ -87,46 +87,20 @@ __device__ __forceinline__ void cursor_next(const TileArgs &A, RowCursor &c) {
     cursor_skip_empty(A, c);
 }
 
-__device__ __forceinline__ int scale_exp(float s) {
-    int e;
-    frexpf(s, &e);
-    return e - 1;  // s = 2^(e-1) for a power of two
+
+// ---- mixed layouts: entry classes, compensation, plane formats -----------
+// Entry class: the tile's precision, except that a diagonal entry (column ==
+// row) of an FP16 / FP8 tile is FP32. A row block's planes are grouped by
+// class (FP64, FP32, FP16, FP8 planes in that order); plane j of a group
+// holds the j-th entry of that class of each of the 16 rows, in the
+// reference's order.
+__device__ __forceinline__ int entry_class(const TileArgs &A, int t, bool is_diag) {
+    const int p = A.prec[t];
+    return (is_diag && p > MF_PREC_FP32) ? MF_PREC_FP32 : p;
 }
 
-// Storage precision and scale of one plane from its entries' tile
-// precisions / scales (warp-wide; lanes without an entry pass prec = -1).
-// Every stored value keeps the exact dequantized value of its tile.
-__device__ void plane_format(int prec, float scale, int &pprec, float &pscale) {
-    const unsigned full = 0xffffffffu;
-    const bool has = prec >= 0;
-    const bool any64 = __any_sync(full, has && prec == MF_PREC_FP64);
-    const bool any32 = __any_sync(full, has && prec == MF_PREC_FP32);
-    const bool any16 = __any_sync(full, has && prec == MF_PREC_FP16);
-    const bool anyl = __any_sync(full, has);
-    // the plane scale is stored as an int8 exponent of a normal float
-    pscale = 1.0f;
-    if (!anyl || any64) {
-        pprec = MF_PREC_FP64;
-        return;
-    }
-    if (any32) {
-        pprec = MF_PREC_FP32;
-        return;
-    }
-    const int e = has ? scale_exp(scale) + 1024 : 1 << 20;
-    const int emin = (int)__reduce_min_sync(full, (unsigned)e);
-    const int emax = (int)__reduce_max_sync(full, has ? (unsigned)e : 0u);
-    if (emin - 1024 < -126 || emax - 1024 > 127) {
-        pprec = MF_PREC_FP32;
-    } else if (emin == emax) {
-        pprec = any16 ? MF_PREC_FP16 : MF_PREC_FP8;
-        pscale = ldexpf(1.0f, emin - 1024);
-    } else if (!any16 && emax - emin <= 7) {
-        pprec = MF_PREC_FP16;
-        pscale = ldexpf(1.0f, emin - 1024);
-    } else {
-        pprec = MF_PREC_FP32;
-    }
+__device__ __forceinline__ bool entry_is_diag(const TileArgs &A, const RowCursor &c, int row) {
+    return A.tile_col[c.t] * 16 + (int)A.col[c.q] == row;
 }
 
 // Dequantized value of entry q of tile t (FP64 tiles: the value itself).
@@ -140,6 +114,93 @@ __device__ __forceinline__ double dequant(const TileArgs &A, int t, int q) {
     if (p == MF_PREC_FP16) return (double)__half2float(__double2half(v * inv)) * s;
     const __nv_fp8_storage_t b = __nv_cvt_double_to_fp8(v * inv, __NV_SATFINITE, __NV_E4M3);
     return (double)__half2float(__half(__nv_cvt_fp8_to_halfraw(b, __NV_E4M3))) * s;
+}
+
+// Value of an entry at its class (a promoted diagonal keeps FP32).
+__device__ __forceinline__ double entry_value(const TileArgs &A, int t, int q, bool is_diag) {
+    if (is_diag && A.prec[t] > MF_PREC_FP32) return (double)__double2float_rn(A.val[q]);
+    return dequant(A, t, q);
+}
+
+__device__ __forceinline__ double class_round(int cls, double v) {
+    return cls == MF_PREC_FP64 ? v : (double)__double2float_rn(v);
+}
+
+// Moves the cursor to the row's next entry of class `cls` (or past the end).
+__device__ __forceinline__ void cursor_seek_class(const TileArgs &A, RowCursor &c, int cls, int row) {
+    while (cursor_valid(c) && entry_class(A, c.t, entry_is_diag(A, c, row)) != cls) cursor_next(A, c);
+}
+
+// Row-sum-preserving compensation of a row (one lane per row): a row with
+// exactly one diagonal entry a_ii > 0, every other entry <= 0 and a diagonal
+// of class FP64 / FP32 stores its diagonal as the class value of
+// a_ii - delta, delta = sum over the other entries in the reference's order
+// of (dequantized - a_ij) in FP64. Writing A as a sum of edge terms
+// (-a_ij)(e_i - e_j)(e_i - e_j)^T plus the diagonal of row sums, the rounding
+// then only moves edge weights, each by at most u_p relative, so that for a
+// symmetric diagonally dominant Z-matrix (1 - u) A <= A~ <= (1 + u) A: the
+// low-precision operator stays positive definite with A's conditioning.
+// Returns true and the diagonal's stored value when the row qualifies.
+__device__ bool row_compensation(const TileArgs &A, RowCursor c, int row, double &diag_value) {
+    int nd = 0;
+    bool z = true;
+    double delta = 0.0, aii = 0.0;
+    int dcls = MF_PREC_FP64;
+    for (; cursor_valid(c); cursor_next(A, c)) {
+        const double a = A.val[c.q];
+        if (entry_is_diag(A, c, row)) {
+            ++nd;
+            aii = a;
+            dcls = entry_class(A, c.t, true);
+        } else {
+            if (!(a <= 0.0)) z = false;
+            delta += entry_value(A, c.t, c.q, false) - a;
+        }
+    }
+    if (nd != 1 || !z || !(aii > 0.0) || dcls > MF_PREC_FP32) return false;
+    diag_value = class_round(dcls, aii - delta);
+    return true;
+}
+
+// Storage format of one plane of class `cls` (warp-wide; lanes without an
+// entry pass has = false). FP64 / FP32 classes store their own type. An
+// FP16 (FP8) class plane is stored as FP16 (FP8) values times a common
+// power-of-two 2^k when every nonzero value / 2^k is an exact normal number
+// of that type, else in the next wider type that holds them exactly (the
+// values carry at most 11 (4) significant bits).
+__device__ void plane_format(int cls, bool has, double v, int &pprec, int &pexp) {
+    const unsigned full = 0xffffffffu;
+    pexp = 0;
+    if (cls <= MF_PREC_FP32) {
+        pprec = cls;
+        return;
+    }
+    const bool nz = has && v != 0.0;
+    const int e = nz ? ilogb(v) : 0;
+    // the largest value's significand (for the FP8 maximum 448 = 1.75 * 2^8)
+    const int emax = (int)__reduce_max_sync(full, nz ? (unsigned)(e + 4096) : 0u) - 4096;
+    const int emin = (int)__reduce_min_sync(full, nz ? (unsigned)(e + 4096) : 0xffffffffu) - 4096;
+    const bool anynz = __any_sync(full, nz);
+    if (!anynz) {
+        pprec = cls;
+        return;
+    }
+    if (cls == MF_PREC_FP8) {
+        const bool big = __any_sync(full, nz && e == emax && fabs(v) > 1.75 * ldexp(1.0, e));
+        const int k = emax - (big ? 7 : 8);
+        if (emin - k >= -6 && k >= -126 && k <= 127) {
+            pprec = MF_PREC_FP8;
+            pexp = k;
+            return;
+        }
+    }
+    const int k = emax - 15;
+    if (emin - k >= -14 && k >= -126 && k <= 127) {
+        pprec = MF_PREC_FP16;
+        pexp = k;
+        return;
+    }
+    pprec = MF_PREC_FP32;
 }
 
 // Power-of-two scale of every FP16 / FP8 tile (1 for the others).
@@ -171,38 +232,53 @@ __global__ void k_tile_scales(int tilenum, const int *tile_off, const double *va
     scale[t] = (float)s;
 }
 
-// Per row block: plane count W and value bytes of the row-sliced block.
-__global__ void k_rb_info(TileArgs A, bool mixed, int *rbW, unsigned *rbvb) {
+// Per row block: plane count W and value bytes of the row-sliced block; in
+// mixed layouts also the bytes of promoted diagonal entries beyond their
+// tile's width (for the algorithmic byte count).
+__global__ void k_rb_info(TileArgs A, bool mixed, int *rbW, unsigned *rbvb, unsigned *rbprom) {
     const int lane = threadIdx.x & 31;
     const int rb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (rb >= A.tilem) return;
+    const int row = rb * 16 + lane;
     RowCursor c;
     cursor_init(A, c, rb, lane < 16 ? lane : 99);
-    int len = 0;
+    int cnt[4] = {0, 0, 0, 0};
+    unsigned prom = 0;
     {
         RowCursor d = c;
         while (lane < 16 && cursor_valid(d)) {
-            ++len;
+            const bool dg = entry_is_diag(A, d, row);
+            const int cl = mixed ? entry_class(A, d.t, dg) : MF_PREC_FP64;
+            ++cnt[cl];
+            if (mixed && dg && A.prec[d.t] > MF_PREC_FP32) prom += 4u - prec_width(A.prec[d.t]);
             cursor_next(A, d);
         }
     }
-    const int W = (int)__reduce_max_sync(0xffffffffu, (unsigned)len);
+    int W = 0;
     unsigned vb = 0;
-    if (!mixed) {
-        vb = 128u * W;
-    } else {
-        for (int k = 0; k < W; ++k) {
-            const bool has = lane < 16 && cursor_valid(c);
-            int pp;
-            float ps;
-            plane_format(has ? (int)A.prec[c.t] : -1, has ? A.scale[c.t] : 1.0f, pp, ps);
+    for (int cl = 0; cl < 4; ++cl) {
+        const int ncl = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt[cl]);
+        W += ncl;
+        if (!mixed) {
+            vb += 128u * ncl;
+            continue;
+        }
+        RowCursor d = c;
+        for (int j = 0; j < ncl; ++j) {
+            if (lane < 16) cursor_seek_class(A, d, cl, row);
+            const bool has = lane < 16 && cursor_valid(d);
+            const double v = has ? entry_value(A, d.t, d.q, entry_is_diag(A, d, row)) : 0.0;
+            int pp, pe;
+            plane_format(cl, has, v, pp, pe);
             vb += 16u * prec_width(pp);
-            if (has) cursor_next(A, c);
+            if (has) cursor_next(A, d);
         }
     }
+    prom = __reduce_add_sync(0xffffffffu, prom);
     if (lane == 0) {
         rbW[rb] = W;
         rbvb[rb] = vb;
+        rbprom[rb] = prom;
     }
 }
 
@@ -282,77 +358,93 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_slabs(const SlabPlan *__r
     for (int j = warp; j < P.nrb; j += FILL_THREADS / 32) {
         const int rb = P.rb0 + j;
         const int W = rbW[rb];
+        const int row = rb * 16 + lane;
         uint8_t *blk = base + s_off[j];
         RowCursor c;
         cursor_init(A, c, rb, lane < 16 ? lane : 99);
-        // row lengths
-        int len = 0;
+        // row lengths, class counts, compensation
+        int len = 0, cnt[4] = {0, 0, 0, 0};
         {
             RowCursor d = c;
             while (lane < 16 && cursor_valid(d)) {
                 ++len;
+                ++cnt[mixed ? entry_class(A, d.t, entry_is_diag(A, d, row)) : MF_PREC_FP64];
                 cursor_next(A, d);
             }
         }
+        double diag_v = 0.0;
+        const bool comp = mixed && lane < 16 && row_compensation(A, c, row, diag_v);
         if (lane < 16) blk[lane] = (uint8_t)len;
         uint64_t pbits = 0;
+        bool fast = true;
         int8_t *sexp = reinterpret_cast<int8_t *>(blk + rb_pinfo_off() + 8);
         uint8_t *idxb = blk + rb_idx_off(W, mixed);
         uint8_t *vals = blk + rb_vals_off(W, mixed, gather);
         uint32_t voff = 0;
-        int prev_t = -1;
-        for (int k = 0; k < W; ++k) {
-            const bool has = lane < 16 && cursor_valid(c);
-            int pp = MF_PREC_FP64;
-            float ps = 1.0f;
-            if (mixed) plane_format(has ? (int)A.prec[c.t] : -1, has ? A.scale[c.t] : 1.0f, pp, ps);
-            if (mixed) {
-                pbits |= (uint64_t)pp << (2 * k);
-                if (lane == 0) sexp[k] = (int8_t)(pp >= MF_PREC_FP16 ? scale_exp(ps) : 0);
-            }
-            if (has) {
-                const int t = c.t;
-                const int q = c.q;
-                const bool start = t != prev_t;
-                prev_t = t;
-                const bool low = mixed && A.prec[t] != MF_PREC_FP64;
-                const int colx = A.tile_col[t];
-                const int cin = A.col[q];
-                if (gather) {
-                    uint32_t id = (uint32_t)(colx * 16 + cin);
-                    if (start) id |= IDX32_START;
-                    if (low) id |= IDX32_LOW;
-                    reinterpret_cast<uint32_t *>(idxb)[k * 16 + lane] = id;
-                } else {
-                    int a = 0, b = P.nseg - 1;
-                    while (a < b) {
-                        const int mid = (a + b) >> 1;
-                        if (segs[P.seg_off + mid] < colx) a = mid + 1; else b = mid;
+        int k = 0;
+        for (int cl = 0; cl < 4; ++cl) {
+            const int ncl = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt[cl]);
+            if (mixed && lane == 0) blk[rb_pinfo_off() + 40 + cl] = (uint8_t)ncl;
+            RowCursor d = c;
+            int prev_t = -1;  // previous entry's tile among this class (FP64 tile starts)
+            for (int jj = 0; jj < ncl; ++jj, ++k) {
+                if (mixed && lane < 16) cursor_seek_class(A, d, cl, row);
+                const bool has = lane < 16 && cursor_valid(d);
+                const bool dg = has && entry_is_diag(A, d, row);
+                double v = 0.0;
+                if (has) v = mixed ? (dg && comp ? diag_v : entry_value(A, d.t, d.q, dg)) : A.val[d.q];
+                int pp = MF_PREC_FP64, pe = 0;
+                if (mixed) {
+                    plane_format(cl, has, v, pp, pe);
+                    pbits |= (uint64_t)pp << (2 * k);
+                    if (lane == 0) sexp[k] = (int8_t)pe;
+                    if (pp != cl) fast = false;
+                }
+                if (has) {
+                    const int t = d.t;
+                    const bool start = t != prev_t;
+                    prev_t = t;
+                    const int colx = A.tile_col[t];
+                    const int cin = A.col[d.q];
+                    if (gather) {
+                        uint32_t id = (uint32_t)(colx * 16 + cin);
+                        if (start && cl == MF_PREC_FP64) id |= IDX32_START;
+                        reinterpret_cast<uint32_t *>(idxb)[k * 16 + lane] = id;
+                    } else {
+                        int a = 0, b = P.nseg - 1;
+                        while (a < b) {
+                            const int mid = (a + b) >> 1;
+                            if (segs[P.seg_off + mid] < colx) a = mid + 1; else b = mid;
+                        }
+                        uint32_t id = (uint32_t)(a * 16 + cin);
+                        if (start && cl == MF_PREC_FP64) id |= IDX16_START;
+                        reinterpret_cast<uint16_t *>(idxb)[k * 16 + lane] = (uint16_t)id;
                     }
-                    uint32_t id = (uint32_t)(a * 16 + cin);
-                    if (start) id |= IDX16_START;
-                    if (low) id |= IDX16_LOW;
-                    reinterpret_cast<uint16_t *>(idxb)[k * 16 + lane] = (uint16_t)id;
+                    uint8_t *pv = vals + voff;
+                    const double sv = ldexp(v, -pe);  // exact: a power-of-two rescaling
+                    if (pp == MF_PREC_FP64) {
+                        reinterpret_cast<double *>(pv)[lane] = v;
+                    } else if (pp == MF_PREC_FP32) {
+                        reinterpret_cast<float *>(pv)[lane] = (float)v;  // exact: v is a class value
+                    } else if (pp == MF_PREC_FP16) {
+                        reinterpret_cast<__half *>(pv)[lane] = __double2half(sv);  // exact
+                    } else {
+                        pv[lane] = (uint8_t)__nv_cvt_double_to_fp8(sv, __NV_SATFINITE, __NV_E4M3);  // exact
+                    }
+                    cursor_next(A, d);
+                } else if (lane < 16) {
+                    // padding entry, value 0 (the zeroed slab): staged rows
+                    // index the zero slot, gather rows carry the padding flag
+                    if (gather) reinterpret_cast<uint32_t *>(idxb)[k * 16 + lane] = IDX32_PAD;
+                    else reinterpret_cast<uint16_t *>(idxb)[k * 16 + lane] = (uint16_t)(XZERO_OFF / (segbytes / 16u));
                 }
-                const double v = mixed ? dequant(A, t, q) : A.val[q];
-                uint8_t *pv = vals + voff;
-                if (pp == MF_PREC_FP64) {
-                    reinterpret_cast<double *>(pv)[lane] = v;
-                } else if (pp == MF_PREC_FP32) {
-                    reinterpret_cast<float *>(pv)[lane] = (float)v;  // exact: v is a dequantized value
-                } else if (pp == MF_PREC_FP16) {
-                    reinterpret_cast<__half *>(pv)[lane] = __double2half(v / (double)ps);  // exact
-                } else {
-                    pv[lane] = (uint8_t)__nv_cvt_double_to_fp8(v / (double)ps, __NV_SATFINITE, __NV_E4M3);
-                }
-                cursor_next(A, c);
-            } else if (lane < 16 && !gather) {
-                // padding entry: value 0 (the zeroed slab) at the zero slot
-                reinterpret_cast<uint16_t *>(idxb)[k * 16 + lane] = (uint16_t)(XZERO_OFF / (segbytes / 16u));
+                voff += 16u * prec_width(pp);
             }
-            voff += 16u * prec_width(pp);
         }
-        if (mixed && lane == 0) *reinterpret_cast<uint64_t *>(blk + rb_pinfo_off()) = pbits;
+        if (mixed && lane == 0) {
+            *reinterpret_cast<uint64_t *>(blk + rb_pinfo_off()) = pbits;
+            blk[rb_pinfo_off() + 44] = fast ? 1 : 0;
+        }
     }
 }
 
@@ -378,8 +470,8 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
     // device: tile scales, row-block plane counts and value bytes
     if (L.prec_dev.alloc(tilenum) || L.scale_dev.alloc(tilenum)) return MF_ERR_NOMEM;
     DevArray<int> d_rbW;
-    DevArray<unsigned> d_rbvb;
-    if (d_rbW.alloc(tilem) || d_rbvb.alloc(tilem)) return MF_ERR_NOMEM;
+    DevArray<unsigned> d_rbvb, d_rbprom;
+    if (d_rbW.alloc(tilem) || d_rbvb.alloc(tilem) || d_rbprom.alloc(tilem)) return MF_ERR_NOMEM;
     if (tilenum > 0) {
         MF_CUDA_TRY(cudaMemcpyAsync(L.prec_dev.p, prec.data(), tilenum, cudaMemcpyHostToDevice, st));
         k_tile_scales<<<(tilenum + 7) / 8, 256, 0, st>>>(tilenum, t->tile_off.p, t->val.p, L.prec_dev.p,
@@ -387,12 +479,13 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
     }
     TileArgs A{t->tile_ptr.p, t->tile_col.p, t->tile_off.p, t->csrptr_off.p, t->ptr.p, t->val.p, t->col.p,
                L.prec_dev.p, L.scale_dev.p, tilem, t->rowA};
-    k_rb_info<<<(tilem + 7) / 8, 256, 0, st>>>(A, mixed, d_rbW.p, d_rbvb.p);
+    k_rb_info<<<(tilem + 7) / 8, 256, 0, st>>>(A, mixed, d_rbW.p, d_rbvb.p, d_rbprom.p);
     MF_CUDA_TRY(cudaGetLastError());
     std::vector<int> rbW(tilem);
-    std::vector<unsigned> rbvb(tilem);
+    std::vector<unsigned> rbvb(tilem), rbprom(tilem);
     MF_CUDA_TRY(cudaMemcpyAsync(rbW.data(), d_rbW.p, sizeof(int) * tilem, cudaMemcpyDeviceToHost, st));
     MF_CUDA_TRY(cudaMemcpyAsync(rbvb.data(), d_rbvb.p, sizeof(unsigned) * tilem, cudaMemcpyDeviceToHost, st));
+    MF_CUDA_TRY(cudaMemcpyAsync(rbprom.data(), d_rbprom.p, sizeof(unsigned) * tilem, cudaMemcpyDeviceToHost, st));
     MF_CUDA_TRY(cudaStreamSynchronize(st));
 
     auto rb_bytes = [&](int rb, bool gather) { return rb_block_bytes(rbW[rb], mixed, gather, rbvb[rb]); };
@@ -647,6 +740,12 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
         alg += tile_alg_bytes(prec[k], tn[k]);
         cnt[prec[k]] += 1;
     }
+    // diagonal entries of FP16 / FP8 tiles are stored in FP32 (oversize row
+    // blocks hold FP64 tiles only)
+    if (mixed)
+        for (const auto &P : plans)
+            if (P.mode != SLAB_OVERSIZE)
+                for (int rb = P.rb0; rb < P.rb0 + P.nrb; ++rb) alg += (double)rbprom[rb];
     // upload and fill
     DevArray<SlabPlan> d_plans;
     DevArray<int> d_slab_cta, d_segs;

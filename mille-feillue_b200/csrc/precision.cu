@@ -6,6 +6,13 @@
 // whose range holds the tile (FP8 also needs a dynamic range <= 2^12);
 // diagonal tiles never go below FP32; otherwise FP64. The levels tighten as
 // the true residual falls (the solver switches at replacement points).
+//
+// Row blocks whose rows are all diagonally dominant Z-rows (one diagonal
+// entry a_ii > 0, every other entry <= 0) are stored with row-sum-preserving
+// compensation (layout.cu): there the rounding of an entry moves only an
+// edge weight of the operator, by at most u_p relative, so its tiles take
+// the lowest precision with u_p <= kCompTau whatever their magnitude (FP16
+// within its range; the diagonal entries themselves stay FP32).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -124,6 +131,61 @@ int tile_features(mf_tiles *t, std::vector<float> &feat, cudaStream_t s) {
 // Unit roundoffs of FP8-E4M3, FP16, FP32.
 static const double kU[4] = {0x1p-53, 0x1p-24, 0x1p-11, 0x1p-4};
 
+// Largest relative edge-weight perturbation accepted for compensated row
+// blocks (the operator then lies within (1 +- u) A): FP16 (u = 4.9e-4)
+// passes, FP8 (u = 6.25e-2) does not (CG with true-residual replacement
+// stalls on the 128^3 variable-coefficient Poisson with every off-diagonal
+// entry in FP8).
+static const double kCompTau = 1e-3;
+
+namespace {
+// 1 for a row block whose rows are all diagonally dominant Z-rows: exactly
+// one diagonal entry, positive, and every other entry <= 0 (one warp per row
+// block, a lane per row).
+__global__ void k_rb_zrows(TileFeatArgs A, uint8_t *zflag) {
+    const int lane = threadIdx.x & 31;
+    const int rb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (rb >= A.tilem) return;
+    const int rl = rb == A.tilem - 1 ? A.rowA - (A.tilem - 1) * 16 : 16;
+    bool ok = true;
+    if (lane < rl) {
+        const int row = rb * 16 + lane;
+        int nd = 0;
+        bool z = true, pos = false;
+        for (int t = A.tile_ptr[rb]; t < A.tile_ptr[rb + 1]; ++t) {
+            const int vo = A.tile_off[t], nk = A.tile_off[t + 1] - vo;
+            const int cc = A.csrptr_off[t];
+            const int q0 = A.bptr[cc + lane], q1 = lane + 1 < rl ? (int)A.bptr[cc + lane + 1] : nk;
+            for (int q = q0; q < q1; ++q) {
+                const double a = A.val[vo + q];
+                if (A.tile_col[t] * 16 + (int)A.col[vo + q] == row) {
+                    ++nd;
+                    pos = a > 0.0;
+                } else if (!(a <= 0.0)) {
+                    z = false;
+                }
+            }
+        }
+        ok = nd == 1 && z && pos;
+    }
+    ok = __all_sync(0xffffffffu, ok);
+    if (lane == 0) zflag[rb] = ok ? 1 : 0;
+}
+}  // namespace
+
+// Per row block: all rows diagonally dominant Z-rows (host copy).
+int rb_zrows(const mf_tiles *t, std::vector<uint8_t> &z, cudaStream_t s) {
+    z.assign(t->tilem, 0);
+    if (t->tilem == 0) return MF_OK;
+    DevArray<uint8_t> d;
+    if (d.alloc(t->tilem)) return MF_ERR_NOMEM;
+    k_rb_zrows<<<(t->tilem + 7) / 8, 256, 0, s>>>(tile_feat_args(t), d.p);
+    MF_CUDA_TRY(cudaGetLastError());
+    MF_CUDA_TRY(cudaMemcpyAsync(z.data(), d.p, t->tilem, cudaMemcpyDeviceToHost, s));
+    MF_CUDA_TRY(cudaStreamSynchronize(s));
+    return MF_OK;
+}
+
 struct RuleThresholds {
     float mag[4];           // largest log10 tile magnitude that passes, per precision
     float range16, range8;  // largest log10 tile range allowed for FP16 / FP8
@@ -182,29 +244,13 @@ uint8_t rule_precision_fast(const float *f, const RuleThresholds &r) {
 }
 
 
-// Row blocks whose tiles are mostly FP32 keep every low-precision tile in
-// FP32: a row block whose planes all hold FP32 runs the lean FP32 loop, and
-// the few FP16 / FP8 tiles would save only a few bytes.
-void promote_minority(const mf_tiles *t, std::vector<uint8_t> &p) {
-    for (int rb = 0; rb < t->tilem; ++rb) {
-        const int t0 = t->h_tile_ptr[rb], t1 = t->h_tile_ptr[rb + 1];
-        int n32 = 0, nsub = 0;
-        for (int k = t0; k < t1; ++k) {
-            n32 += p[k] == MF_PREC_FP32;
-            nsub += p[k] == MF_PREC_FP16 || p[k] == MF_PREC_FP8;
-        }
-        if (nsub > 0 && 2 * nsub < n32 + nsub)
-            for (int k = t0; k < t1; ++k)
-                if (p[k] == MF_PREC_FP16 || p[k] == MF_PREC_FP8) p[k] = MF_PREC_FP32;
-    }
-}
-
 // Level tolerances of the magnitude rule and the relative true residual
 // below which the solver moves to the next level. The tolerance bounds the
 // entry perturbation relative to the Jacobi scale sqrt(a_ii a_jj); it must
 // stay below the smallest eigenvalue of the Jacobi-scaled matrix or the
 // perturbed operator can lose definiteness (a 128^3 variable-coefficient
-// Poisson diverges with FP16 off-diagonal tiles, tau ~ 5e-4).
+// Poisson diverges with uncompensated FP16 off-diagonal tiles, tau ~ 5e-4).
+// Compensated row blocks do not use these levels.
 const double kLevelTau[MF_NLEVELS] = {2e-7, 1e-7, 1e-7};
 const double kLevelSwitch[MF_NLEVELS] = {1e-6, 0.0, 0.0};
 
@@ -237,7 +283,6 @@ int build_mixed_levels(mf_tiles *t, cudaStream_t s) {
         std::vector<uint8_t> prev;
         for (int l = 0; l < nlev; ++l) {
             std::vector<uint8_t> p(pm.begin() + (size_t)l * t->tilenum, pm.begin() + (size_t)(l + 1) * t->tilenum);
-            promote_minority(t, p);
             if (l > 0 && p == prev) break;
             rc = build_layout(t, t->Lmix[l], p, s);
             if (rc) return rc;
@@ -256,14 +301,31 @@ int build_mixed_levels(mf_tiles *t, cudaStream_t s) {
     std::vector<float> feat;
     int rc = tile_features(t, feat, s);
     if (rc) return rc;
+    std::vector<uint8_t> zrb;
+    if ((rc = rb_zrows(t, zrb, s))) return rc;
     const double scale = t->opt.mixed_tau > 0 ? t->opt.mixed_tau : 1.0;
+    // compensated row blocks: the lowest precision with u_p <= kCompTau
+    // (scaled like the level tolerances) whose range holds the tile
+    const RuleThresholds any = rule_thresholds(INFINITY);
+    const bool comp16 = kU[MF_PREC_FP16] <= kCompTau * scale, comp8 = kU[MF_PREC_FP8] <= kCompTau * scale;
+    const bool comp32 = kU[MF_PREC_FP32] <= kCompTau * scale;
     int nl = 0;
     std::vector<uint8_t> prev;
     for (int l = 0; l < MF_NLEVELS; ++l) {
         std::vector<uint8_t> p(t->tilenum);
         const RuleThresholds thr = rule_thresholds(kLevelTau[l] * scale);
-        for (int k = 0; k < t->tilenum; ++k) p[k] = rule_precision_fast(&feat[(size_t)k * 6], thr);
-        promote_minority(t, p);
+        for (int rb = 0; rb < t->tilem; ++rb)
+            for (int k = t->h_tile_ptr[rb]; k < t->h_tile_ptr[rb + 1]; ++k) {
+                const float *f = &feat[(size_t)k * 6];
+                if (zrb[rb]) {
+                    const float f1 = f[1];
+                    p[k] = (comp8 && f1 <= any.range8) ? MF_PREC_FP8
+                           : (comp16 && f1 <= any.range16) ? MF_PREC_FP16
+                           : comp32 ? MF_PREC_FP32 : rule_precision_fast(f, thr);
+                } else {
+                    p[k] = rule_precision_fast(f, thr);
+                }
+            }
         if (l > 0 && p == prev) break;  // identical to the previous level
         rc = build_layout(t, t->Lmix[l], p, s);
         if (rc) return rc;

@@ -92,10 +92,103 @@ __device__ bool wait_bar(uint64_t *bar, uint32_t parity, uint64_t limit_ns) {
 __device__ __forceinline__ float to_f32(double v) { return __double2float_rn(v); }
 __device__ __forceinline__ float to_f32(float v) { return v; }
 
+__device__ __forceinline__ float exp2_int(int e) { return __int_as_float((e + 127) << 23); }  // e in [-126, 127]
+__device__ __forceinline__ float fp8_to_float(uint8_t b) {
+    return __half2float(__half(__nv_cvt_fp8_to_halfraw((__nv_fp8_storage_t)b, __NV_E4M3)));
+}
+
+// Row r of a mixed-layout row block (planes grouped by entry class, see
+// tiles.h). FP64-class entries: sum = 0, sum += x*v, acc += sum at each tile
+// start, exactly blockspmv_cpu's order. The FP32-, FP16- and FP8-class
+// entries: one FP32 accumulator, sumf = fmaf((float)x, v, sumf), group by
+// group in plane order. Returns acc + (double)sumf. Staged rows loop over all
+// planes (padding entries index the zero slot with value 0); gather rows
+// skip the x load of padding entries (PAD flag, value 0).
+template <bool GATHER, typename XT>
+__device__ __forceinline__ double mixed_row(const uint8_t *blk, int W, int r, const XT *xs,
+                                            const XT *__restrict__ xg) {
+    const uint8_t *pi = blk + rb_pinfo_off();
+    const uint32_t cnt = *reinterpret_cast<const uint32_t *>(pi + 40);
+    const int n64 = cnt & 0xffu, n32 = (cnt >> 8) & 0xffu, n16 = (cnt >> 16) & 0xffu, n8 = cnt >> 24;
+    const bool fast = pi[44] != 0;
+    const int8_t *sexp = reinterpret_cast<const int8_t *>(pi + 8);
+    const uint8_t *idxb = blk + rb_idx_off(W, true);
+    const uint8_t *vals = blk + rb_vals_off(W, true, GATHER);
+    auto ld_x = [&](int k, uint32_t &id) -> XT {
+        if constexpr (GATHER) {
+            id = reinterpret_cast<const uint32_t *>(idxb)[k * 16 + r];
+            return (id & IDX32_PAD) ? XT(0) : __ldcg(xg + (id & IDX32_POS));
+        } else {
+            id = reinterpret_cast<const uint16_t *>(idxb)[k * 16 + r];
+            return xs[id & IDX16_POS];
+        }
+    };
+    double acc = 0.0;
+    uint32_t voff = 0;
+    int k = 0;
+    if (n64 > 0) {
+        const double *v = reinterpret_cast<const double *>(vals) + r;
+        double sum = 0.0;
+        for (; k < n64; ++k) {
+            uint32_t id;
+            const double x = (double)ld_x(k, id);
+            if (id & (GATHER ? IDX32_START : IDX16_START)) {
+                acc = dadd(acc, sum);
+                sum = 0.0;
+            }
+            sum = dadd(sum, dmul(x, v[k * 16]));
+        }
+        acc = dadd(acc, sum);
+        voff = 128u * n64;
+    }
+    float sumf = 0.0f;
+    {
+        const float *v = reinterpret_cast<const float *>(vals + voff) + r;
+#pragma unroll 4
+        for (int j = 0; j < n32; ++j) {
+            uint32_t id;
+            const XT x = ld_x(k + j, id);
+            sumf = __fmaf_rn(to_f32(x), v[j * 16], sumf);
+        }
+        k += n32;
+        voff += 64u * n32;
+    }
+    if (fast) {
+        const __half *h = reinterpret_cast<const __half *>(vals + voff) + r;
+#pragma unroll 4
+        for (int j = 0; j < n16; ++j) {
+            uint32_t id;
+            const XT x = ld_x(k + j, id);
+            sumf = __fmaf_rn(to_f32(x), __half2float(h[j * 16]) * exp2_int(sexp[k + j]), sumf);
+        }
+        k += n16;
+        voff += 32u * n16;
+        for (int j = 0; j < n8; ++j) {
+            uint32_t id;
+            const XT x = ld_x(k + j, id);
+            sumf = __fmaf_rn(to_f32(x), fp8_to_float(vals[voff + j * 16 + r]) * exp2_int(sexp[k + j]), sumf);
+        }
+    } else {
+        const uint64_t pbits = *reinterpret_cast<const uint64_t *>(pi);
+        for (; k < W; ++k) {
+            const uint32_t pr = (uint32_t)(pbits >> (2 * k)) & 3u;
+            uint32_t id;
+            const XT x = ld_x(k, id);
+            const float sc = exp2_int(sexp[k]);
+            float v;
+            if (pr == MF_PREC_FP32) v = reinterpret_cast<const float *>(vals + voff)[r];
+            else if (pr == MF_PREC_FP16) v = __half2float(reinterpret_cast<const __half *>(vals + voff)[r]) * sc;
+            else v = fp8_to_float(vals[voff + r]) * sc;
+            sumf = __fmaf_rn(to_f32(x), v, sumf);
+            voff += 128u >> pr;
+        }
+    }
+    return dadd(acc, (double)sumf);
+}
+
 // Sum of row r of row block j of a staged / gather slab (row-sliced planes).
-// FP64 tiles: sum = 0, sum += x*v in order, acc += sum at each tile start,
-// exactly blockspmv_cpu's order. Tiles below FP64 (mixed layouts): the
-// dequantized value in FP32, sumf = fmaf(x, v, sumf), acc += sumf.
+// FP64 layouts: sum = 0, sum += x*v in order, acc += sum at each tile start,
+// exactly blockspmv_cpu's order. Mixed layouts: mixed_row.
 // GB > 1: FP64 gather rows issue GB x loads from L2 before using the first
 // (more gathers in flight, more registers: for kernels with registers to
 // spare; the solver kernels with 128 live registers take GB = 1).
@@ -169,178 +262,65 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
         }
         return dadd(acc, sum);
     }
-    // mixed layouts: packed plane precisions, value offset kept in a register
-    const uint64_t pbits = *reinterpret_cast<const uint64_t *>(blk + rb_pinfo_off());
-    const int8_t *sexp = reinterpret_cast<const int8_t *>(blk + rb_pinfo_off() + 8);
-    const uint8_t *idxb = blk + rb_idx_off(W, true);
-    const uint8_t *vals = blk + rb_vals_off(W, true, gather);
-    uint32_t voff = 0;
-    float sumf = 0.0f;
-    if (KIND == LAYOUT_LOW && W > 0 && W <= 32 && pbits == (0x5555555555555555ull & ((2ull << (2 * W - 1)) - 1ull))) {
-        // every plane of the row block stored in FP32
-        const float *v32 = reinterpret_cast<const float *>(vals);
-        if (!gather) {
-            const uint16_t *idx = reinterpret_cast<const uint16_t *>(idxb);
-#pragma unroll 4
-            for (int k = 0; k < W; ++k) {
-                const uint32_t id = idx[k * 16 + r];
-                const float v = v32[k * 16 + r];
-                const XT x = xstage[id & IDX16_POS];
-                if (id & IDX16_START) {
-                    acc = dadd(acc, (double)sumf);
-                    sumf = 0.0f;
-                }
-                sumf = __fmaf_rn(to_f32(x), v, sumf);
-            }
-        } else {
-            const uint32_t *idx = reinterpret_cast<const uint32_t *>(idxb);
-#pragma unroll 4
-            for (int k = 0; k < len; ++k) {
-                const uint32_t id = idx[k * 16 + r];
-                const float v = v32[k * 16 + r];
-                const XT x = __ldcg(xg + (id & IDX32_POS));
-                if (id & IDX32_START) {
-                    acc = dadd(acc, (double)sumf);
-                    sumf = 0.0f;
-                }
-                sumf = __fmaf_rn(to_f32(x), v, sumf);
-            }
-        }
-        return dadd(acc, (double)sumf);
-    }
-    if (KIND == LAYOUT_LOW) {
-        // every tile below FP64: FP32 products, FP32 tile sums, FP64 row sum.
-        // Branch-free: each lane loads the 32-bit word holding its value
-        // (plane width 4, 2 or 1 bytes) and decodes all three forms.
-        if (!gather) {
-            const uint16_t *idx = reinterpret_cast<const uint16_t *>(idxb);
-#pragma unroll 4
-            for (int k = 0; k < len; ++k) {
-                const uint32_t pr = (uint32_t)(pbits >> (2 * k)) & 3u;
-                const uint32_t wlog = 3u - pr;
-                const uint32_t id = idx[k * 16 + r];
-                const XT x = xstage[id & IDX16_POS];
-                const uint32_t boff = voff + ((uint32_t)r << wlog);
-                const uint32_t wrd = *reinterpret_cast<const uint32_t *>(vals + (boff & ~3u));
-                const uint32_t sh = (boff & 3u) * 8u;
-                const float sc = __int_as_float((sexp[k] + 127) << 23);
-                const float v16 = __half2float(__ushort_as_half((unsigned short)(wrd >> sh)));
-                const float v8 = __half2float(
-                    __half(__nv_cvt_fp8_to_halfraw((__nv_fp8_storage_t)((wrd >> sh) & 0xffu), __NV_E4M3)));
-                const float v = (pr == MF_PREC_FP32 ? __uint_as_float(wrd) : pr == MF_PREC_FP16 ? v16 : v8) * sc;
-                if (id & IDX16_START) {
-                    acc = dadd(acc, (double)sumf);
-                    sumf = 0.0f;
-                }
-                sumf = __fmaf_rn(to_f32(x), v, sumf);
-                voff += 16u << wlog;
-            }
-        } else {
-            const uint32_t *idx = reinterpret_cast<const uint32_t *>(idxb);
-#pragma unroll 4
-            for (int k = 0; k < len; ++k) {
-                const uint32_t pr = (uint32_t)(pbits >> (2 * k)) & 3u;
-                const uint32_t wlog = 3u - pr;
-                const uint32_t id = idx[k * 16 + r];
-                const XT x = __ldcg(xg + (id & IDX32_POS));
-                const uint32_t boff = voff + ((uint32_t)r << wlog);
-                const uint32_t wrd = *reinterpret_cast<const uint32_t *>(vals + (boff & ~3u));
-                const uint32_t sh = (boff & 3u) * 8u;
-                const float sc = __int_as_float((sexp[k] + 127) << 23);
-                const float v16 = __half2float(__ushort_as_half((unsigned short)(wrd >> sh)));
-                const float v8 = __half2float(
-                    __half(__nv_cvt_fp8_to_halfraw((__nv_fp8_storage_t)((wrd >> sh) & 0xffu), __NV_E4M3)));
-                const float v = (pr == MF_PREC_FP32 ? __uint_as_float(wrd) : pr == MF_PREC_FP16 ? v16 : v8) * sc;
-                if (id & IDX32_START) {
-                    acc = dadd(acc, (double)sumf);
-                    sumf = 0.0f;
-                }
-                sumf = __fmaf_rn(to_f32(x), v, sumf);
-                voff += 16u << wlog;
-            }
-        }
-        return dadd(acc, (double)sumf);
-    }
-    // some tiles FP64, some below: each tile sums in its own type
-    bool low = false;
-    for (int k = 0; k < len; ++k) {
-        const uint32_t pr = (uint32_t)(pbits >> (2 * k)) & 3u;
-        double x;
-        bool start, lowk;
-        if (!gather) {
-            const uint32_t id = reinterpret_cast<const uint16_t *>(idxb)[k * 16 + r];
-            x = xstage[id & IDX16_POS];
-            start = id & IDX16_START;
-            lowk = id & IDX16_LOW;
-        } else {
-            const uint32_t id = reinterpret_cast<const uint32_t *>(idxb)[k * 16 + r];
-            x = __ldcg(xg + (id & IDX32_POS));
-            start = id & IDX32_START;
-            lowk = id & IDX32_LOW;
-        }
-        if (start) {
-            acc = dadd(acc, low ? (double)sumf : sum);
-            sum = 0.0;
-            sumf = 0.0f;
-            low = lowk;
-        }
-        const uint8_t *pv = vals + voff;
-        if (low) {
-            float vf;
-            if (pr == MF_PREC_FP64) vf = __double2float_rn(reinterpret_cast<const double *>(pv)[r]);
-            else if (pr == MF_PREC_FP32) vf = reinterpret_cast<const float *>(pv)[r];
-            else {
-                const float sc = __int_as_float((sexp[k] + 127) << 23);
-                if (pr == MF_PREC_FP16) vf = __half2float(reinterpret_cast<const __half *>(pv)[r]) * sc;
-                else vf = __half2float(__half(__nv_cvt_fp8_to_halfraw((__nv_fp8_storage_t)pv[r], __NV_E4M3))) * sc;
-            }
-            sumf = __fmaf_rn(to_f32(x), vf, sumf);
-        } else {
-            sum = dadd(sum, dmul(x, reinterpret_cast<const double *>(pv)[r]));
-        }
-        voff += 16u << (3u - pr);
-    }
-    return dadd(acc, low ? (double)sumf : sum);
+    return gather ? mixed_row<true>(blk, W, r, xstage, xg) : mixed_row<false>(blk, W, r, xstage, xg);
 }
 
-// Two staged row blocks of one half-warp whose W planes are all FP32 and
-// equal in number, interleaved in one loop: two independent load and
-// accumulate chains per lane, each in the order of slab_row (identical
-// results). Returns false (nothing computed) when the pair does not qualify.
-__device__ __forceinline__ bool pair_rows32(const uint8_t *st, int j1, int j2, int r, const float *xs, double &a1,
-                                            double &a2) {
+// Two staged row blocks of one half-warp whose class groups are FP32, FP16
+// and FP8 planes only, equal in number and all stored in their class type,
+// interleaved in one loop: two independent load and accumulate chains per
+// lane, each in the order of mixed_row (identical results). Returns false
+// (nothing computed) when the pair does not qualify.
+__device__ __forceinline__ bool pair_mixed(const uint8_t *st, int j1, int j2, int r, const float *xs, double &a1,
+                                           double &a2) {
     const RbDir *dir = reinterpret_cast<const RbDir *>(st + slab_rbdir_off());
     const RbDir d1 = dir[j1], d2 = dir[j2];
     const int W = (int)(d1.W & 0xffffu);
-    if ((int)(d2.W & 0xffffu) != W || W == 0 || W > 32) return false;
     const uint8_t *b1 = st + d1.off, *b2 = st + d2.off;
-    const uint64_t p1 = *reinterpret_cast<const uint64_t *>(b1 + rb_pinfo_off());
-    const uint64_t p2 = *reinterpret_cast<const uint64_t *>(b2 + rb_pinfo_off());
-    if (p1 != (0x5555555555555555ull & ((2ull << (2 * W - 1)) - 1ull)) || p2 != p1) return false;
+    const uint32_t c1 = *reinterpret_cast<const uint32_t *>(b1 + rb_pinfo_off() + 40);
+    const uint32_t c2 = *reinterpret_cast<const uint32_t *>(b2 + rb_pinfo_off() + 40);
+    const uint32_t f1 = *reinterpret_cast<const uint32_t *>(b1 + rb_pinfo_off() + 44);
+    const uint32_t f2 = *reinterpret_cast<const uint32_t *>(b2 + rb_pinfo_off() + 44);
+    if (c1 != c2 || (c1 & 0xffu) != 0u || (f1 & 0xffu) == 0u || (f2 & 0xffu) == 0u) return false;
+    const int n32 = (c1 >> 8) & 0xffu, n16 = (c1 >> 16) & 0xffu, n8 = c1 >> 24;
     const uint16_t *i1 = reinterpret_cast<const uint16_t *>(b1 + rb_idx_off(W, true)) + r;
     const uint16_t *i2 = reinterpret_cast<const uint16_t *>(b2 + rb_idx_off(W, true)) + r;
-    const float *v1 = reinterpret_cast<const float *>(b1 + rb_vals_off(W, true, false)) + r;
-    const float *v2 = reinterpret_cast<const float *>(b2 + rb_vals_off(W, true, false)) + r;
-    double c1 = 0.0, c2 = 0.0;
+    const int8_t *e1 = reinterpret_cast<const int8_t *>(b1 + rb_pinfo_off() + 8);
+    const int8_t *e2 = reinterpret_cast<const int8_t *>(b2 + rb_pinfo_off() + 8);
+    const uint8_t *v1 = b1 + rb_vals_off(W, true, false);
+    const uint8_t *v2 = b2 + rb_vals_off(W, true, false);
     float s1 = 0.0f, s2 = 0.0f;
+    {
+        const float *w1 = reinterpret_cast<const float *>(v1) + r, *w2 = reinterpret_cast<const float *>(v2) + r;
 #pragma unroll 2
-    for (int k = 0; k < W; ++k) {
-        const uint32_t id1 = i1[k * 16], id2 = i2[k * 16];
-        const float w1 = v1[k * 16], w2 = v2[k * 16];
-        const float x1 = xs[id1 & IDX16_POS], x2 = xs[id2 & IDX16_POS];
-        if (id1 & IDX16_START) {
-            c1 = dadd(c1, (double)s1);
-            s1 = 0.0f;
+        for (int k = 0; k < n32; ++k) {
+            const float x1 = xs[i1[k * 16] & IDX16_POS], x2 = xs[i2[k * 16] & IDX16_POS];
+            s1 = __fmaf_rn(x1, w1[k * 16], s1);
+            s2 = __fmaf_rn(x2, w2[k * 16], s2);
         }
-        if (id2 & IDX16_START) {
-            c2 = dadd(c2, (double)s2);
-            s2 = 0.0f;
-        }
-        s1 = __fmaf_rn(x1, w1, s1);
-        s2 = __fmaf_rn(x2, w2, s2);
     }
-    a1 = dadd(c1, (double)s1);
-    a2 = dadd(c2, (double)s2);
+    int k0 = n32;
+    uint32_t voff = 64u * n32;
+    {
+        const __half *h1 = reinterpret_cast<const __half *>(v1 + voff) + r;
+        const __half *h2 = reinterpret_cast<const __half *>(v2 + voff) + r;
+#pragma unroll 2
+        for (int j = 0; j < n16; ++j) {
+            const int k = k0 + j;
+            const float x1 = xs[i1[k * 16] & IDX16_POS], x2 = xs[i2[k * 16] & IDX16_POS];
+            s1 = __fmaf_rn(x1, __half2float(h1[j * 16]) * exp2_int(e1[k]), s1);
+            s2 = __fmaf_rn(x2, __half2float(h2[j * 16]) * exp2_int(e2[k]), s2);
+        }
+        k0 += n16;
+        voff += 32u * n16;
+    }
+    for (int j = 0; j < n8; ++j) {
+        const int k = k0 + j;
+        const float x1 = xs[i1[k * 16] & IDX16_POS], x2 = xs[i2[k * 16] & IDX16_POS];
+        s1 = __fmaf_rn(x1, fp8_to_float(v1[voff + j * 16 + r]) * exp2_int(e1[k]), s1);
+        s2 = __fmaf_rn(x2, fp8_to_float(v2[voff + j * 16 + r]) * exp2_int(e2[k]), s2);
+    }
+    a1 = (double)s1;
+    a2 = (double)s2;
     return true;
 }
 
@@ -507,9 +487,9 @@ __device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const void *xv,
                 };
                 int jstart = j0;
                 if (MIXED && L.kind == LAYOUT_LOW && h.mode == SLAB_STAGED) {
-                    // all-FP32 row blocks j and j + 2 NWARPS of this half-warp
-                    // computed together; a pair that does not qualify (or a
-                    // lone last row block) goes to the loop below
+                    // row blocks j and j + 2 NWARPS of this half-warp computed
+                    // together; a pair that does not qualify (or a lone last
+                    // row block) goes to the loop below
                     const float *xs = reinterpret_cast<const float *>(st + slab_area);
                     for (; jstart + 2 * NWARPS < h.nrb; jstart += 4 * NWARPS) {
                         const int j2 = jstart + 2 * NWARPS;
@@ -517,7 +497,7 @@ __device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const void *xv,
                         const bool live1 = row1 < L.gt.rowA, live2 = row2 < L.gt.rowA;
                         const PV pv1 = pre_of(jstart, row1, live1), pv2 = pre_of(j2, row2, live2);
                         double a1, a2;
-                        if (!pair_rows32(st, jstart, j2, r, xs, a1, a2)) {
+                        if (!pair_mixed(st, jstart, j2, r, xs, a1, a2)) {
                             a1 = slab_row<LAYOUT_LOW, GB>(st, h, jstart, r, xs, static_cast<const float *>(xv));
                             a2 = slab_row<LAYOUT_LOW, GB>(st, h, j2, r, xs, static_cast<const float *>(xv));
                         }

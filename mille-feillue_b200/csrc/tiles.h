@@ -58,17 +58,25 @@ struct DevArray {
 //   rbdir[nrb + 1]      per row block: byte offset of its block, plane count
 //   row-block blocks    one per row block, "row-sliced planes":
 //     rowlen[16]  (u8)  entries of each of the 16 rows
-//     pinfo             (mixed layouts only, W <= 32) u64 storage precision
-//                       of each plane (2 bits per plane) + int8 exponent of
-//                       each plane's power-of-two scale
+//     pinfo (48 B)      (mixed layouts only, W <= 32) u64 storage precision
+//                       of each plane (2 bits per plane), int8 exponent k
+//                       of each plane's storage scale 2^k (32 B), the plane
+//                       counts of the four class groups (u8 x 4: FP64,
+//                       FP32, FP16, FP8) and a fast flag (u8: every FP16
+//                       class plane stored as FP16, every FP8 one as FP8)
 //     idx[W][16]        u16 x-window position (staged) or u32 column
-//                       (gather) of entry k of row r, with the flags
-//                       TILE_START (first entry of a new tile in this row)
-//                       and LOW (the entry's tile is below FP64)
+//                       (gather) of entry k of row r, with the flag
+//                       TILE_START (first entry of a new FP64 tile in this
+//                       row); padding entries index the stage's zero slot
+//                       (staged) or carry the PAD flag (gather)
 //     vals              plane k holds entry k of the 16 rows: FP64 16x8 B,
 //                       or in mixed layouts FP64/FP32/FP16/FP8 16xwidth B
-// Entry k of row r is the k-th entry of the row in the reference's order:
-// tiles in ascending column, entries of the row inside a tile in CSR order.
+// FP64 layouts: entry k of row r is the k-th entry of the row in the
+// reference's order (tiles in ascending column, entries of the row inside a
+// tile in CSR order). Mixed layouts: the planes are grouped by entry class
+// (the tile's precision; a diagonal entry of an FP16 / FP8 tile is FP32) in
+// the order FP64, FP32, FP16, FP8, and plane j of a group holds the j-th
+// entry of that class of each row, in the reference's order.
 constexpr int STAGES = 4;
 constexpr int MAXRUNS = 24;
 constexpr int XSEG_MAX = 112;      // staged x segments per slab (14 KB of FP64 x)
@@ -84,8 +92,8 @@ constexpr int SLAB_MAX_DEFAULT = 40960;
 constexpr int RB_PER_SLAB_MAX = 60;  // two per consumer half-warp
 constexpr int RB_PER_SLAB_X64 = 30;  // default for layouts staging FP64 x
 constexpr int ISSUE_REC = 16 + MAXRUNS * 8;
-constexpr uint32_t IDX16_START = 0x8000u, IDX16_LOW = 0x4000u, IDX16_POS = 0x3fffu;
-constexpr uint32_t IDX32_START = 0x80000000u, IDX32_LOW = 0x40000000u, IDX32_POS = 0x3fffffffu;
+constexpr uint32_t IDX16_START = 0x8000u, IDX16_POS = 0x3fffu;
+constexpr uint32_t IDX32_START = 0x80000000u, IDX32_PAD = 0x40000000u, IDX32_POS = 0x3fffffffu;
 
 enum { SLAB_STAGED = 0, SLAB_GATHER = 1, SLAB_OVERSIZE = 2 };
 

@@ -581,54 +581,120 @@ double mfo_tile_scale(int prec, double maxabs) {
     return ldexp(1.0, k);
 }
 
+/* Dequantized value of v stored in a tile of precision p with scale s. */
+static double deq_value(int p, double v, double s) {
+    if (p == 0) return v;
+    if (p == 1) return (double)(float)v;
+    if (p == 2) return mfo_fp16_decode(mfo_fp16_encode(v / s)) * s;
+    return mfo_fp8_e4m3_decode(mfo_fp8_e4m3_encode(v / s)) * s;
+}
+
+/* One entry of a row in the reference's order (tiles ascending, CSR order
+ * inside a tile). */
+typedef struct {
+    int col, cls, is_diag;
+    double a, deq;
+} mx_entry;
+
 void mfo_mixed_spmv(const mfo_tiles *t, const unsigned char *prec, const double *x,
                     double *y) {
-    /* Per tile: FP64 tiles sum = 0; sum += x * v; acc += sum. Tiles below
-     * FP64 use the dequantized value v_q (FP32: (float)v; FP16 / FP8:
-     * decode(encode(v / s)) * s with the tile's power-of-two scale s), and
-     * sumf = fmaf((float)x, (float)v_q, sumf); acc += (double)sumf. */
-#pragma omp parallel for schedule(static)
-    for (int rb = 0; rb < t->tilem; ++rb) {
-        int rl = rowlen_of(t, rb);
-        double acc[T16];
-        for (int ri = 0; ri < T16; ++ri) acc[ri] = 0.0;
-        for (int k = t->tile_ptr[rb]; k < t->tile_ptr[rb + 1]; ++k) {
-            const int xo = t->tile_columnidx[k] * T16;
-            const int vo = t->blknnz[k];
-            const int nk = t->blknnz[k + 1] - t->blknnz[k];
-            const unsigned char *bp = t->Blockcsr_Ptr + t->csrptr_offset[k];
-            const int p = prec[k];
-            double maxabs = 0.0;
-            for (int q = 0; q < nk; ++q) {
-                double a = fabs(t->Blockcsr_Val[vo + q]);
-                if (a > maxabs) maxabs = a;
-            }
-            const double scale = mfo_tile_scale(p, maxabs);
+    /* The mixed-precision operator (no reference counterpart; the reference's
+     * own mixed path keeps per-tile-column FP32 / FP16 / int8 copies,
+     * MP/Mille-feuille_CG.cu:452-530).
+     *
+     * Entry class: the tile's precision p_t, except that a diagonal entry
+     * (column == row) of an FP16 / FP8 tile is FP32. Dequantized value:
+     * FP64 v; FP32 (float)v; FP16 / FP8 decode(encode(v / s_t)) * s_t with
+     * the tile's power-of-two scale s_t (mfo_tile_scale of its max |v|).
+     *
+     * Row-sum-preserving compensation: a row with exactly one diagonal entry,
+     * a_ii > 0, every other entry <= 0 and a diagonal of class FP64 or FP32
+     * stores its diagonal as the class value of a_ii - delta_i, where delta_i
+     * = sum over the row's other entries (reference order, FP64) of
+     * (dequantized - a_ij). Writing A = sum_{i<j} (-a_ij) (e_i - e_j)(e_i -
+     * e_j)^T + diag(row sums), the rounding then moves only the edge weights,
+     * each by at most u_p relative, and for a symmetric diagonally dominant
+     * Z-matrix (1 - u) A <= A~ <= (1 + u) A: the operator stays positive
+     * definite with the same conditioning, however small its eigenvalues.
+     *
+     * Row sum: acc = sum over the FP64-class tiles in ascending order of
+     * (sum = 0; sum += x * v in CSR order); sumf = fmaf((float)x, (float)v,
+     * sumf) over the FP32-class entries in reference order, then the
+     * FP16-class ones, then the FP8-class ones; y = acc + (double)sumf. */
+    double *scale = (double *)malloc(sizeof(double) * (size_t)(t->tilenum > 0 ? t->tilenum : 1));
+    for (int k = 0; k < t->tilenum; ++k) {
+        double mx = 0.0;
+        for (int q = t->blknnz[k]; q < t->blknnz[k + 1]; ++q)
+            if (fabs(t->Blockcsr_Val[q]) > mx) mx = fabs(t->Blockcsr_Val[q]);
+        scale[k] = mfo_tile_scale(prec[k], mx);
+    }
+#pragma omp parallel
+    {
+        mx_entry *row = NULL;
+        int cap = 0;
+#pragma omp for schedule(static)
+        for (int rb = 0; rb < t->tilem; ++rb) {
+            const int rl = rowlen_of(t, rb);
             for (int ri = 0; ri < rl; ++ri) {
-                int st = bp[ri];
-                int sp = ri == rl - 1 ? nk : bp[ri + 1];
-                if (p == 0) {
-                    double sum = 0.0;
-                    for (int q = st; q < sp; ++q)
-                        sum += x[xo + t->Tile_csr_Col[vo + q]] * t->Blockcsr_Val[vo + q];
-                    acc[ri] += sum;
-                } else {
-                    float sum = 0.0f;
+                const int grow = rb * T16 + ri;
+                int n = 0;
+                for (int k = t->tile_ptr[rb]; k < t->tile_ptr[rb + 1]; ++k) {
+                    const int vo = t->blknnz[k], nk = t->blknnz[k + 1] - vo;
+                    const unsigned char *bp = t->Blockcsr_Ptr + t->csrptr_offset[k];
+                    const int st = bp[ri], sp = ri == rl - 1 ? nk : bp[ri + 1];
                     for (int q = st; q < sp; ++q) {
-                        double v = t->Blockcsr_Val[vo + q];
-                        double vq;
-                        if (p == 1) vq = (float)v;
-                        else if (p == 2) vq = mfo_fp16_decode(mfo_fp16_encode(v / scale)) * scale;
-                        else vq = mfo_fp8_e4m3_decode(mfo_fp8_e4m3_encode(v / scale)) * scale;
-                        float xf = (float)x[xo + t->Tile_csr_Col[vo + q]];
-                        sum = fmaf(xf, (float)vq, sum);
+                        if (n == cap) {
+                            cap = cap ? 2 * cap : 64;
+                            row = (mx_entry *)realloc(row, sizeof(mx_entry) * (size_t)cap);
+                        }
+                        mx_entry *e = &row[n++];
+                        e->col = t->tile_columnidx[k] * T16 + t->Tile_csr_Col[vo + q];
+                        e->a = t->Blockcsr_Val[vo + q];
+                        e->is_diag = e->col == grow;
+                        e->cls = prec[k];
+                        if (e->is_diag && e->cls > 1) e->cls = 1;
+                        e->deq = deq_value(prec[k], e->a, scale[k]);
+                        if (e->is_diag && prec[k] > 1) e->deq = (double)(float)e->a;
                     }
-                    acc[ri] += (double)sum;
                 }
+                /* compensation */
+                int nd = 0, zrow = 1, di = -1;
+                for (int q = 0; q < n; ++q) {
+                    if (row[q].is_diag) { ++nd; di = q; }
+                    else if (!(row[q].a <= 0.0)) zrow = 0;
+                }
+                if (nd == 1 && zrow && row[di].a > 0.0) {
+                    double delta = 0.0;
+                    for (int q = 0; q < n; ++q)
+                        if (!row[q].is_diag) delta += row[q].deq - row[q].a;
+                    const double dv = row[di].a - delta;
+                    row[di].deq = row[di].cls == 0 ? dv : (double)(float)dv;
+                }
+                /* FP64 class: per-tile sums in tile order (entries of one tile
+                 * are contiguous in reference order) */
+                double acc = 0.0, sum = 0.0;
+                int cur_tile_col = -1;
+                for (int q = 0; q < n; ++q) {
+                    if (row[q].cls != 0) continue;
+                    const int tcol = row[q].col / T16;
+                    if (tcol != cur_tile_col) {
+                        if (cur_tile_col >= 0) acc += sum;
+                        sum = 0.0;
+                        cur_tile_col = tcol;
+                    }
+                    sum += x[row[q].col] * row[q].deq;
+                }
+                if (cur_tile_col >= 0) acc += sum;
+                float sumf = 0.0f;
+                for (int c = 1; c <= 3; ++c)
+                    for (int q = 0; q < n; ++q)
+                        if (row[q].cls == c) sumf = fmaf((float)x[row[q].col], (float)row[q].deq, sumf);
+                y[grow] = acc + (double)sumf;
             }
         }
-        for (int ri = 0; ri < rl; ++ri) y[rb * T16 + ri] = acc[ri];
+        free(row);
     }
+    free(scale);
 }
 
 /* ---- MLP oracle (6 -> 64 -> 64 -> 4, ReLU, softmax cross-entropy) ---- */

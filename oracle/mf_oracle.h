@@ -87,9 +87,11 @@ double mfo_fp16_decode(uint16_t h);
 double mfo_tile_scale(int prec, double maxabs);
 
 /* Mixed-precision tiled SpMV: tile t stored at prec[t] (0 fp64, 1 fp32,
- * 2 fp16, 3 fp8) with scale 2^e; low-precision tiles multiply their
- * dequantized values in FP32 with fmaf accumulation in CSR order, then add
- * the FP32 tile sum to the FP64 row total. */
+ * 2 fp16, 3 fp8) with a power-of-two scale for fp16 / fp8; diagonal entries
+ * never below fp32; the diagonal of a diagonally dominant Z-row absorbs its
+ * row's rounding (row sums preserved); FP64-class entries summed per tile in
+ * FP64, the others in one FP32 accumulator by class (fp32, fp16, fp8). The
+ * full definition is in mf_oracle.c. */
 void mfo_mixed_spmv(const mfo_tiles *t, const unsigned char *prec, const double *x,
                     double *y);
 

@@ -87,3 +87,19 @@ def test_mixed_bicgstab_reaches_fp64_tolerance(mf, maker, growth):
     # both meet the 1e-10 residual; their difference is bounded by the
     # condition number times that, not by the rounding of either
     assert np.linalg.norm(xm - x64) / np.linalg.norm(x64) < 1e-5
+
+
+def test_c3_mixed_layout_is_fp16_and_keeps_fp64_iterations(mf):
+    """The headline matrix (diagonally dominant Z-matrix) is stored with
+    row-sum-preserving FP16 tiles (diagonal entries FP32): the CG keeps the
+    FP64 iteration count within a few percent and the FP64 true residual."""
+    A = mf.Matrix.varpoisson3d(128)
+    t = mf.Tiles(A, mf.options(precision_mode=mf.MODE_MIXED_RULE))
+    x64, r64 = t.solve_cg(A.b(), tol=1e-10, maxiter=40000, opts=mf.options())
+    xm, rm = t.solve_cg(A.b(), tol=1e-10, maxiter=40000)
+    assert rm["status"] == 0 and rm["rel_residual_true"] <= 1e-10, rm
+    assert rm["tile_frac"][2] > 0.99, rm["tile_frac"]
+    assert rm["iterations"] <= 1.05 * r64["iterations"], (rm["iterations"], r64["iterations"])
+    assert np.linalg.norm(xm - x64) / np.linalg.norm(x64) < 1e-6
+    # the layout moves fewer bytes than an all-FP32 one would (FP16 values)
+    assert rm["spmv_bytes_level"][0] < 0.8 * 113.5e6

@@ -206,3 +206,51 @@ def test_oracle_jacobi_pcg_solves_and_beats_cg_on_contrast(O):
     assert rel_p <= 1e-10
     assert np.linalg.norm(b - M @ x_p) / np.linalg.norm(b) <= 2e-10
     assert it_p < 0.5 * it_c, (it_p, it_c)
+
+
+def test_mixed_operator_preserves_row_sums(O):
+    """Row-sum-preserving compensation: with every tile in FP16 (diagonal
+    entries promoted to FP32), A~ 1 equals A 1 up to the FP32 rounding of
+    the diagonal and of the row's FP32 accumulation; without it the FP16
+    rounding of the off-diagonals (relative 4.9e-4) would show."""
+    S = O.gen_varpoisson3d(12)
+    rp, ci, v = S.csr()
+    o = O.OracleTiles(S.n, S.n, rp, ci, v)
+    prec = np.full(o.sizes["tilenum"], 2, np.uint8)
+    ones = np.ones(S.n)
+    y = o.mixed_spmv(prec, ones)
+    rows = np.repeat(np.arange(S.n), np.diff(rp))
+    rowsum = np.bincount(rows, weights=v, minlength=S.n)
+    absum = np.bincount(rows, weights=np.abs(v), minlength=S.n)
+    err = np.abs(y - rowsum)
+    assert np.all(err <= 16 * 2.0 ** -24 * absum), (err / absum).max()
+    # the compensated diagonal is what carries it: the off-diagonal FP16
+    # rounding alone is orders of magnitude larger than the error left
+    off = ci != rows
+    h = v[off].astype(np.float16).astype(np.float64)  # the tile scales are powers of two
+    assert np.abs(h - v[off]).max() > 100 * err.max()
+
+
+def test_mixed_operator_keeps_non_z_rows_uncompensated(O):
+    """A row with a positive off-diagonal entry keeps its diagonal's plain
+    class value: A~ 1 then differs from A 1 by the off-diagonals' rounding."""
+    n = 64
+    rp = np.arange(0, 3 * n + 1, 3, dtype=np.int32)[: n + 1]
+    ci, v = [], []
+    for i in range(n):
+        cols = sorted({i, (i + 1) % n, (i + 7) % n})
+        while len(cols) < 3:
+            cols.append((cols[-1] + 1) % n)
+        for c in cols:
+            ci.append(c)
+            v.append(10.0 if c == i else 0.1 + 0.001 * (i % 13))  # positive off-diagonals
+    ci = np.array(ci, np.int32)
+    v = np.array(v)
+    o = O.OracleTiles(n, n, rp, ci, v)
+    prec = np.full(o.sizes["tilenum"], 2, np.uint8)
+    y = o.mixed_spmv(prec, np.ones(n))
+    rows = np.repeat(np.arange(n), 3)
+    # compensation would make y equal the FP64 row sums to FP32 accuracy;
+    # rows that are not Z-rows keep the FP16 rounding of their off-diagonals
+    rs = np.bincount(rows, weights=v, minlength=n)
+    assert np.max(np.abs(y - rs)) > 4 * 2.0 ** -24 * np.max(np.abs(rs))
