@@ -538,7 +538,7 @@ def multi_rhs_arm(args, rank, local):
             "speedup_vs_single_rhs": single_ms / multi_ms}
 
 
-def batch_arm(args, world, rank, local, dist):
+def batch_arm(args, world, rank, local, dist, steps=None, warmup=None):
     """512 random SPD systems, n log-uniform in [1e3, 2e5] (seed 2), FP64 CG
     to 1e-10: one persistent launch (CUDA-graph replay) against one
     single-system launch per system. With N ranks the systems are split by
@@ -562,7 +562,9 @@ def batch_arm(args, world, rank, local, dist):
     b = np.concatenate([m.b() for m in mats])
     bd = torch.tensor(b, device=f"cuda:{dev}")
     xd = torch.zeros_like(bd)
-    for _ in range(args.warmup):
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
+    for _ in range(warmup):
         B.solve_cg_dev(bd.data_ptr(), xd.data_ptr(), TOL, 10000)
     torch.cuda.synchronize()
     _barrier(dist)
@@ -571,13 +573,13 @@ def batch_arm(args, world, rank, local, dist):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
-    for _ in range(args.steps):
+    for _ in range(steps):
         B.solve_cg_dev(bd.data_ptr(), xd.data_ptr(), TOL, 10000)
     e1.record()
     torch.cuda.synchronize()
     _barrier(dist)
     clk = clocks.stop()
-    ms = _max_over_ranks(dist, e0.elapsed_time(e1) / args.steps)
+    ms = _max_over_ranks(dist, e0.elapsed_time(e1) / steps)
     it, st, rel = B.results()
     each_ms = None
     if not args.no_each:
@@ -589,7 +591,7 @@ def batch_arm(args, world, rank, local, dist):
         return None
     return {
         "metric": "batched solve time to 1e-10 (512 SPD systems)", "value": ms, "unit": "ms", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+        "steps": steps, "warmup": warmup, "ms_per_step": ms, "higher_is_better": False,
         "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "batch512_spd n~logU[1e3,2e5] seed 2, CG to 1e-10", "systems": len(mats),
                    "rows_rank0": inf["rows"], "nnz_rank0": inf["nnz"], "grid": inf["grid"],
@@ -600,8 +602,34 @@ def batch_arm(args, world, rank, local, dist):
         "one_launch_per_system_ms": each_ms,
         "speedup_vs_one_launch_per_system": (each_ms / ms) if each_ms else None,
         "clocks": clk, "gen_s": gen_s, "encode_s": enc_s,
-        "gpu_launches": args.steps * 3,
+        "gpu_launches": steps * 3,
     }
+
+
+def _extra_legs(args, world, rank, local, dist, out):
+    """The north star's two other workloads, measured in the default run
+    beside the headline: the batched 512-system launch against one launch
+    per system (systems split over the ranks), and CG on 16 right-hand sides
+    against 16 single solves (rank 0 of a one-GPU run)."""
+    if args.no_extra:
+        return
+    try:
+        bat = batch_arm(args, world, rank, local, dist, steps=3, warmup=1)
+    except Exception as e:  # the headline stands without it
+        bat = {"unavailable": f"{type(e).__name__}: {e}"}
+    if rank == 0 and out is not None:
+        keep = ("value", "unit", "n_gpus", "steps", "warmup", "config", "iterations_min_max", "all_converged",
+                "max_rel_residual", "one_launch_per_system_ms", "speedup_vs_one_launch_per_system", "clocks",
+                "encode_s", "unavailable")
+        out["batch512"] = {k: bat[k] for k in keep if bat and k in bat}
+    if rank == 0 and world == 1 and out is not None:
+        try:
+            m = multi_rhs_arm(args, rank, local)
+            out["multi16"] = {k: m[k] for k in ("value", "unit", "config", "iterations_min_max", "max_rel_residual",
+                                                "single_rhs_total_ms", "single_iterations_min_max",
+                                                "speedup_vs_single_rhs")}
+        except Exception as e:
+            out["multi16"] = {"unavailable": f"{type(e).__name__}: {e}"}
 
 
 def profile_case(args):
@@ -702,6 +730,7 @@ def main():
                          "smaller only for quick checks)")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the batch512 / multi16 legs of the default run")
     ap.add_argument("--workload", default="poisson128",
                     choices=["poisson128", "batch", "vs_cusparse", "multi16", "profile"])
     # --workload profile: one kernel on a fixed case, for profilers (profile_case)
@@ -742,6 +771,7 @@ def main():
             print(json.dumps(out))
         return
     out = gpu_arm(args, world, rank, local, dist)
+    _extra_legs(args, world, rank, local, dist, out)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # one whole oracle solve (about 10 s of CPU work)
         a2 = argparse.Namespace(**vars(args))

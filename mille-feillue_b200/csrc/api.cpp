@@ -196,6 +196,7 @@ int mf_memory_report(const mf_tiles *t, mf_memory_cost *r) {
                dev_bytes(t->block_signal) + dev_bytes(t->blockrowid_new) + dev_bytes(t->blockcsr_ptr_new) +
                dev_bytes(t->diag) + layout_dev_bytes(t->L64);
     for (int l = 0; l < MF_NLEVELS; ++l) d += layout_dev_bytes(t->Lmix[l]);
+    d += layout_dev_bytes(t->Lbicg);
     r->workspace_bytes = dev_bytes(t->ws) + dev_bytes(t->sync) + dev_bytes(t->xpad) + dev_bytes(t->x32buf) +
                          dev_bytes(t->trace);
     r->device_bytes = d + r->workspace_bytes;
@@ -273,6 +274,7 @@ int mf_tiles_set_precisions(mf_tiles *t, const unsigned char *prec) {
     int rc = build_layout(t, t->Lmix[0], p, 0);
     if (rc) return rc;
     for (int l = 1; l < MF_NLEVELS; ++l) t->Lmix[l].built = false;
+    t->Lbicg.built = false;
     t->nlevels = 1;
     t->level_switch[0] = 0.0;
     t->mixed_ready = true;
@@ -471,20 +473,38 @@ static int solve_dev_once(mf_tiles *t, int kind, const double *b_dev, double *x_
         t->trace_iters = ti;
     }
     const bool mixed = (kind == 0 || kind == 1) && opt.precision_mode != MF_MODE_FP64 && t->mixed_ready;
+    const Layout *lv[MF_NLEVELS] = {nullptr, nullptr, nullptr};  // the mixed levels this solve runs
     if (mixed) {
         int nl = 1;
-        for (int l = 0; l < t->nlevels; ++l) {
-            if (!t->Lmix[l].built) break;
+        auto add_level = [&](const Layout &L, double rel) {
+            lv[nl - 1] = &L;
             LayoutArgs &a = P.lay[nl];
-            a.slabs = t->Lmix[l].slabs.p;
-            a.head = t->Lmix[l].head.p;
-            a.cta_slab = t->Lmix[l].cta_slab.p;
-            a.cta_rb = t->Lmix[l].cta_rb.p;
-            a.cta_dep = t->Lmix[l].cta_dep.p;
-            a.kind = t->Lmix[l].kind;
-            a.x32 = t->Lmix[l].x32 ? 1 : 0;
-            P.level_rel[nl] = t->level_switch[l];
+            a.slabs = L.slabs.p;
+            a.head = L.head.p;
+            a.cta_slab = L.cta_slab.p;
+            a.cta_rb = L.cta_rb.p;
+            a.cta_dep = L.cta_dep.p;
+            a.kind = L.kind;
+            a.x32 = L.x32 ? 1 : 0;
+            P.level_rel[nl] = rel;
             ++nl;
+        };
+        bool below32 = false;
+        for (int l = 0; l < t->nlevels && t->Lmix[l].built; ++l)
+            for (auto p : t->Lmix[l].prec) below32 = below32 || p > MF_PREC_FP32;
+        if (kind == 1 && below32) {
+            if (!t->Lbicg.built) {
+                std::vector<uint8_t> p32(t->Lmix[0].prec);
+                for (auto &p : p32)
+                    if (p > MF_PREC_FP32) p = MF_PREC_FP32;
+                if ((rc = build_layout(t, t->Lbicg, p32, 0)) != MF_OK) return rc;
+            }
+            add_level(t->Lbicg, 0.0);
+        } else {
+            for (int l = 0; l < t->nlevels; ++l) {
+                if (!t->Lmix[l].built) break;
+                add_level(t->Lmix[l], t->level_switch[l]);
+            }
         }
         P.nlay = nl;
         P.start_layout = 1;
@@ -559,14 +579,15 @@ static int solve_dev_once(mf_tiles *t, int kind, const double *b_dev, double *x_
     R.time_ms = ms;
     R.spmv_bytes_fp64 = t->L64.alg_bytes;
     const Layout *Lf = &t->L64;
-    if (mixed && dr.final_layout >= 1 && t->Lmix[dr.final_layout - 1].built) Lf = &t->Lmix[dr.final_layout - 1];
+    if (mixed && dr.final_layout >= 1 && dr.final_layout <= MF_NLEVELS && lv[dr.final_layout - 1])
+        Lf = lv[dr.final_layout - 1];
     R.spmv_bytes = Lf->alg_bytes;
     for (int p = 0; p < 4; ++p) R.tile_frac[p] = Lf->tile_frac[p];
     R.iters_fp64 = dr.it_layout[0];
     R.fell_back_fp64 = kind <= 1 ? dr.pad : 0;
     for (int l = 0; l < 3; ++l) {
         R.iters_level[l] = dr.it_layout[l + 1];
-        R.spmv_bytes_level[l] = (mixed && t->Lmix[l].built) ? t->Lmix[l].alg_bytes : 0.0;
+        R.spmv_bytes_level[l] = (mixed && lv[l]) ? lv[l]->alg_bytes : 0.0;
     }
     {
         // per iteration: CG one SpMV + 56 n, PCG + 16 n for 1/a_ii, BiCGSTAB
@@ -673,7 +694,7 @@ int mf_tiles_autotune(mf_tiles *t, int reps, mf_tune_result *out) {
     MF_CUDA_TRY(cudaSetDevice(t->opt.device));
     std::memset(out, 0, sizeof *out);
     static const int kSlab[] = {24576, 32768, 40960};
-    static const int kRb[] = {16, 30, 60};
+    static const int kRb[] = {16, 30, 60, 120};
     double best = 1e30;
     int bsb = 0, brb = 0;
     for (int sb : kSlab)
@@ -686,7 +707,7 @@ int mf_tiles_autotune(mf_tiles *t, int reps, mf_tune_result *out) {
             out->cand_slab_bytes[k] = sb;
             out->cand_rb_per_slab[k] = rb;
             out->cand_ms[k] = ms;
-            if (sb == SLAB_MAX_DEFAULT && rb == (t->opt.precision_mode != MF_MODE_FP64 ? RB_PER_SLAB_MAX
+            if (sb == SLAB_MAX_DEFAULT && rb == (t->opt.precision_mode != MF_MODE_FP64 ? RB_PER_SLAB_X32
                                                                                         : RB_PER_SLAB_X64))
                 out->ms_default = ms;
             if (ms < best) {

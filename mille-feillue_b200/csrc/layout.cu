@@ -185,16 +185,19 @@ __device__ void plane_format(int cls, bool has, double v, int &pprec, int &pexp)
         pprec = cls;
         return;
     }
+    // scale 1 when the values fit as they are (the SpMV then skips the
+    // multiply), else the largest value at the top of the type's range
     if (cls == MF_PREC_FP8) {
         const bool big = __any_sync(full, nz && e == emax && fabs(v) > 1.75 * ldexp(1.0, e));
-        const int k = emax - (big ? 7 : 8);
+        const int top = big ? 7 : 8;
+        const int k = (emax <= top && emin >= -6) ? 0 : emax - top;
         if (emin - k >= -6 && k >= -126 && k <= 127) {
             pprec = MF_PREC_FP8;
             pexp = k;
             return;
         }
     }
-    const int k = emax - 15;
+    const int k = (emax <= 15 && emin >= -14) ? 0 : emax - 15;
     if (emin - k >= -14 && k >= -126 && k <= 127) {
         pprec = MF_PREC_FP16;
         pexp = k;
@@ -235,7 +238,7 @@ __global__ void k_tile_scales(int tilenum, const int *tile_off, const double *va
 // Per row block: plane count W and value bytes of the row-sliced block; in
 // mixed layouts also the bytes of promoted diagonal entries beyond their
 // tile's width (for the algorithmic byte count).
-__global__ void k_rb_info(TileArgs A, bool mixed, int *rbW, unsigned *rbvb, unsigned *rbprom) {
+__global__ void k_rb_info(TileArgs A, bool mixed, int *rbW, unsigned *rbvb, unsigned *rbprom, uint8_t *rbaff) {
     const int lane = threadIdx.x & 31;
     const int rb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (rb >= A.tilem) return;
@@ -256,6 +259,7 @@ __global__ void k_rb_info(TileArgs A, bool mixed, int *rbW, unsigned *rbvb, unsi
     }
     int W = 0;
     unsigned vb = 0;
+    bool aff = mixed && c.rl == 16;  // affine: see tiles.h
     for (int cl = 0; cl < 4; ++cl) {
         const int ncl = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt[cl]);
         W += ncl;
@@ -263,6 +267,7 @@ __global__ void k_rb_info(TileArgs A, bool mixed, int *rbW, unsigned *rbvb, unsi
             vb += 128u * ncl;
             continue;
         }
+        if (cl == MF_PREC_FP64 && ncl > 0) aff = false;
         RowCursor d = c;
         for (int j = 0; j < ncl; ++j) {
             if (lane < 16) cursor_seek_class(A, d, cl, row);
@@ -271,6 +276,13 @@ __global__ void k_rb_info(TileArgs A, bool mixed, int *rbW, unsigned *rbvb, unsi
             int pp, pe;
             plane_format(cl, has, v, pp, pe);
             vb += 16u * prec_width(pp);
+            // every row has an entry here, at the same offset from its row
+            const int off = has ? A.tile_col[d.t] * 16 + (int)A.col[d.q] - row : 0;
+            const unsigned full = 0xffffffffu;
+            const bool all16 = __popc(__ballot_sync(full, has)) == 16;
+            const int omin = (int)__reduce_min_sync(full, lane < 16 ? (unsigned)(off + (1 << 30)) : 0xffffffffu);
+            const int omax = (int)__reduce_max_sync(full, lane < 16 ? (unsigned)(off + (1 << 30)) : 0u);
+            if (!all16 || omin != omax) aff = false;
             if (has) cursor_next(A, d);
         }
     }
@@ -279,6 +291,7 @@ __global__ void k_rb_info(TileArgs A, bool mixed, int *rbW, unsigned *rbvb, unsi
         rbW[rb] = W;
         rbvb[rb] = vb;
         rbprom[rb] = prom;
+        rbaff[rb] = aff ? 1 : 0;
     }
 }
 
@@ -290,8 +303,9 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_slabs(const SlabPlan *__r
                                                              const int *__restrict__ segs,
                                                              const XRun *__restrict__ runs, TileArgs A,
                                                              const int *__restrict__ rbW,
-                                                             const unsigned *__restrict__ rbvb, bool mixed,
-                                                             uint32_t segbytes, uint8_t *slabs) {
+                                                             const unsigned *__restrict__ rbvb,
+                                                             const uint8_t *__restrict__ rbaff, bool mixed,
+                                                             uint32_t segbytes, uint32_t zpos, uint8_t *slabs) {
     __shared__ uint32_t s_off[RB_PER_SLAB_MAX + 1];
     const int s = blockIdx.x;
     const SlabPlan P = plans[s];
@@ -346,7 +360,7 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_slabs(const SlabPlan *__r
                     if (lo < P.nseg && sg[lo] == P.rb0 + j) dslot = (uint32_t)lo + 1u;
                 }
                 dir[j].W = (uint32_t)W | (dslot << 16);
-                off += rb_block_bytes(W, mixed, gather, rbvb[P.rb0 + j]);
+                off += rb_block_bytes(W, mixed, gather, rbvb[P.rb0 + j], rbaff[P.rb0 + j] != 0);
             }
             dir[P.nrb].off = off;
             dir[P.nrb].W = 0;
@@ -374,17 +388,19 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_slabs(const SlabPlan *__r
         }
         double diag_v = 0.0;
         const bool comp = mixed && lane < 16 && row_compensation(A, c, row, diag_v);
-        if (lane < 16) blk[lane] = (uint8_t)len;
+        const bool aff = mixed && !gather && rbaff[rb] != 0;
+        if (!mixed && lane < 16) blk[lane] = (uint8_t)len;
         uint64_t pbits = 0;
-        bool fast = true;
-        int8_t *sexp = reinterpret_cast<int8_t *>(blk + rb_pinfo_off() + 8);
-        uint8_t *idxb = blk + rb_idx_off(W, mixed);
-        uint8_t *vals = blk + rb_vals_off(W, mixed, gather);
+        bool fast = true, unscaled = true;
+        int8_t *sexp = reinterpret_cast<int8_t *>(blk + rbm_sexp_off());
+        uint16_t *bases = reinterpret_cast<uint16_t *>(blk + rbm_base_off(W));
+        uint8_t *idxb = blk + (mixed ? rbm_idx_off(W, aff) : rb_idx_off());
+        uint8_t *vals = blk + (mixed ? rbm_vals_off(W, gather, aff) : rb_vals_off(W, gather));
         uint32_t voff = 0;
         int k = 0;
         for (int cl = 0; cl < 4; ++cl) {
             const int ncl = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt[cl]);
-            if (mixed && lane == 0) blk[rb_pinfo_off() + 40 + cl] = (uint8_t)ncl;
+            if (mixed && lane == 0) blk[cl] = (uint8_t)ncl;
             RowCursor d = c;
             int prev_t = -1;  // previous entry's tile among this class (FP64 tile starts)
             for (int jj = 0; jj < ncl; ++jj, ++k) {
@@ -399,6 +415,7 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_slabs(const SlabPlan *__r
                     pbits |= (uint64_t)pp << (2 * k);
                     if (lane == 0) sexp[k] = (int8_t)pe;
                     if (pp != cl) fast = false;
+                    if (pe != 0) unscaled = false;
                 }
                 if (has) {
                     const int t = d.t;
@@ -417,8 +434,12 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_slabs(const SlabPlan *__r
                             if (segs[P.seg_off + mid] < colx) a = mid + 1; else b = mid;
                         }
                         uint32_t id = (uint32_t)(a * 16 + cin);
-                        if (start && cl == MF_PREC_FP64) id |= IDX16_START;
-                        reinterpret_cast<uint16_t *>(idxb)[k * 16 + lane] = (uint16_t)id;
+                        if (aff) {
+                            if (lane == 0) bases[k] = (uint16_t)id;  // entry of row r at bases[k] + r
+                        } else {
+                            if (start && cl == MF_PREC_FP64) id |= IDX16_START;
+                            reinterpret_cast<uint16_t *>(idxb)[k * 16 + lane] = (uint16_t)id;
+                        }
                     }
                     uint8_t *pv = vals + voff;
                     const double sv = ldexp(v, -pe);  // exact: a power-of-two rescaling
@@ -436,14 +457,14 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_slabs(const SlabPlan *__r
                     // padding entry, value 0 (the zeroed slab): staged rows
                     // index the zero slot, gather rows carry the padding flag
                     if (gather) reinterpret_cast<uint32_t *>(idxb)[k * 16 + lane] = IDX32_PAD;
-                    else reinterpret_cast<uint16_t *>(idxb)[k * 16 + lane] = (uint16_t)(XZERO_OFF / (segbytes / 16u));
+                    else reinterpret_cast<uint16_t *>(idxb)[k * 16 + lane] = (uint16_t)zpos;
                 }
                 voff += 16u * prec_width(pp);
             }
         }
         if (mixed && lane == 0) {
-            *reinterpret_cast<uint64_t *>(blk + rb_pinfo_off()) = pbits;
-            blk[rb_pinfo_off() + 44] = fast ? 1 : 0;
+            *reinterpret_cast<uint64_t *>(blk + 8) = pbits;
+            blk[4] = (uint8_t)((fast ? RBF_FAST : 0) | (aff ? RBF_AFFINE : 0) | (fast && unscaled ? RBF_UNSCALED : 0));
         }
     }
 }
@@ -455,6 +476,8 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
     const int tilem = t->tilem, tilenum = t->tilenum;
     const int G = t->G;
     const int slab_max = t->opt.slab_bytes > 0 ? t->opt.slab_bytes : SLAB_MAX_DEFAULT;
+    const int slab_area = (slab_max + 127) & ~127;  // the solver kernels' slab area (solver.h)
+    int slab_lim = slab_max;                         // largest slab of this layout
     const auto &tp = t->h_tile_ptr;
     const auto &tc = t->h_tile_col;
     const auto &tn = t->h_tile_nnz;
@@ -471,7 +494,9 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
     if (L.prec_dev.alloc(tilenum) || L.scale_dev.alloc(tilenum)) return MF_ERR_NOMEM;
     DevArray<int> d_rbW;
     DevArray<unsigned> d_rbvb, d_rbprom;
-    if (d_rbW.alloc(tilem) || d_rbvb.alloc(tilem) || d_rbprom.alloc(tilem)) return MF_ERR_NOMEM;
+    DevArray<uint8_t> d_rbaff;
+    if (d_rbW.alloc(tilem) || d_rbvb.alloc(tilem) || d_rbprom.alloc(tilem) || d_rbaff.alloc(tilem))
+        return MF_ERR_NOMEM;
     if (tilenum > 0) {
         MF_CUDA_TRY(cudaMemcpyAsync(L.prec_dev.p, prec.data(), tilenum, cudaMemcpyHostToDevice, st));
         k_tile_scales<<<(tilenum + 7) / 8, 256, 0, st>>>(tilenum, t->tile_off.p, t->val.p, L.prec_dev.p,
@@ -479,16 +504,20 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
     }
     TileArgs A{t->tile_ptr.p, t->tile_col.p, t->tile_off.p, t->csrptr_off.p, t->ptr.p, t->val.p, t->col.p,
                L.prec_dev.p, L.scale_dev.p, tilem, t->rowA};
-    k_rb_info<<<(tilem + 7) / 8, 256, 0, st>>>(A, mixed, d_rbW.p, d_rbvb.p, d_rbprom.p);
+    k_rb_info<<<(tilem + 7) / 8, 256, 0, st>>>(A, mixed, d_rbW.p, d_rbvb.p, d_rbprom.p, d_rbaff.p);
     MF_CUDA_TRY(cudaGetLastError());
     std::vector<int> rbW(tilem);
     std::vector<unsigned> rbvb(tilem), rbprom(tilem);
+    std::vector<uint8_t> rbaff(tilem);
     MF_CUDA_TRY(cudaMemcpyAsync(rbW.data(), d_rbW.p, sizeof(int) * tilem, cudaMemcpyDeviceToHost, st));
     MF_CUDA_TRY(cudaMemcpyAsync(rbvb.data(), d_rbvb.p, sizeof(unsigned) * tilem, cudaMemcpyDeviceToHost, st));
     MF_CUDA_TRY(cudaMemcpyAsync(rbprom.data(), d_rbprom.p, sizeof(unsigned) * tilem, cudaMemcpyDeviceToHost, st));
+    MF_CUDA_TRY(cudaMemcpyAsync(rbaff.data(), d_rbaff.p, tilem, cudaMemcpyDeviceToHost, st));
     MF_CUDA_TRY(cudaStreamSynchronize(st));
 
-    auto rb_bytes = [&](int rb, bool gather) { return rb_block_bytes(rbW[rb], mixed, gather, rbvb[rb]); };
+    auto rb_bytes = [&](int rb, bool gather) {
+        return rb_block_bytes(rbW[rb], mixed, gather, rbvb[rb], rbaff[rb] != 0);
+    };
     const int maxw = mixed ? MAXW_MIXED : MAXW;
     // CTA ranges of equal cost, computed once per matrix and shared by every
     // layout so that all layouts give each CTA the same rows
@@ -559,7 +588,7 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
                 for (int k = tp[rb]; k < tp[rb + 1]; ++k) seg_add(tc[k]);
                 const bool staged0 = (int)members.size() <= xseg_max && seg_runs <= MAXRUNS;
                 const uint32_t tot0 = slab_blocks_off(1) + rb_bytes(rb, !staged0);
-                if (tot0 > (uint32_t)slab_max || rbW[rb] > maxw) {
+                if (tot0 > (uint32_t)slab_lim || rbW[rb] > maxw) {
                     P.mode = SLAB_OVERSIZE;
                     P.nrb = 1;
                     P.ntiles = tp[rb + 1] - tp[rb];
@@ -577,7 +606,7 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
                     while (nx < cta_rb[g + 1] && P.nrb < rbps) {
                         if (rbW[nx] > maxw) break;
                         const uint32_t bx = rb_bytes(nx, !staged);
-                        if (slab_blocks_off(P.nrb + 1) + body + bx > (uint32_t)slab_max) break;
+                        if (slab_blocks_off(P.nrb + 1) + body + bx > (uint32_t)slab_lim) break;
                         if (staged) {
                             const size_t n0 = members.size();
                             for (int k = tp[nx]; k < tp[nx + 1]; ++k) seg_add(tc[k]);
@@ -615,10 +644,11 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
         }
     };
     for (;;) {
-        xseg_max = x32 ? XSEG_MAX32 : XSEG_MAX;
+        xseg_max = x32 ? xseg_max32(slab_area) : XSEG_MAX;
+        slab_lim = x32 ? x_off_of(slab_area, true) : slab_max;
         segbytes = x32 ? 64u : 128u;
         rbps = t->opt.rb_per_slab > 0 ? std::min(t->opt.rb_per_slab, RB_PER_SLAB_MAX)
-                                      : (x32 ? RB_PER_SLAB_MAX : RB_PER_SLAB_X64);
+                                      : (x32 ? RB_PER_SLAB_X32 : RB_PER_SLAB_X64);
         const unsigned hw = std::thread::hardware_concurrency();
         const int nth = tilem >= 16384 ? std::max(1, std::min({16, (int)(hw ? hw : 1), G})) : 1;
         std::vector<Part> parts(nth);
@@ -768,7 +798,8 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
         MF_CUDA_TRY(cudaMemcpyAsync(d_runs.p, run_all.data(), sizeof(XRun) * run_all.size(), cudaMemcpyHostToDevice, st));
     if (ns > 0)
         k_fill_slabs<<<ns, FILL_THREADS, 0, st>>>(d_plans.p, d_slab_cta.p, L.cta_slab.p, d_segs.p, d_runs.p, A,
-                                                 d_rbW.p, d_rbvb.p, mixed, segbytes, L.slabs.p);
+                                                 d_rbW.p, d_rbvb.p, d_rbaff.p, mixed, segbytes,
+                                                 zero_pos_of(slab_area, x32), L.slabs.p);
     MF_CUDA_TRY(cudaGetLastError());
     MF_CUDA_TRY(cudaStreamSynchronize(st));
     L.prec.swap(prec);

@@ -257,6 +257,7 @@ const double kLevelSwitch[MF_NLEVELS] = {1e-6, 0.0, 0.0};
 int build_mixed_levels(mf_tiles *t, cudaStream_t s) {
     const int mode = t->opt.precision_mode;
     for (int l = 0; l < MF_NLEVELS; ++l) t->Lmix[l].built = false;
+    t->Lbicg.built = false;
     if (mode == MF_MODE_FIXED) {
         if (t->opt.fixed_precision < MF_PREC_FP64 || t->opt.fixed_precision > MF_PREC_FP8) return MF_ERR_ARG;
         std::vector<uint8_t> p(t->tilenum, (uint8_t)t->opt.fixed_precision);

@@ -60,11 +60,11 @@ __device__ void set_error(const KParams &P, uint32_t code, uint32_t site) { set_
 // Thread 0: issue the bulk copies of one slab (x runs first, slab last: the
 // issue record may live inside the stage the slab overwrites).
 // An x segment is 16 entries: 128 bytes of FP64 x, 64 bytes of FP32 x.
-__device__ void issue_slab(Smem &S, uint8_t *stage, int slab_area, int k, uint32_t off16, uint32_t bytes,
+__device__ void issue_slab(Smem &S, uint8_t *stage, int xoff, int k, uint32_t off16, uint32_t bytes,
                            uint32_t xbytes, int nruns, const XRun *runs, const uint8_t *slabs,
                            const uint8_t *xv, uint32_t segb, uint64_t pol_m, uint64_t pol_v) {
     mbar_arrive_expect_tx(&S.full[k], bytes + xbytes);
-    uint8_t *xarea = stage + slab_area;
+    uint8_t *xarea = stage + xoff;
     for (int q = 0; q < nruns; ++q) {
         const XRun r = runs[q];
         bulk_g2s(xarea + (size_t)r.slot0 * segb, xv + (size_t)r.seg0 * segb, (uint32_t)r.nseg * segb, &S.full[k],
@@ -97,6 +97,92 @@ __device__ __forceinline__ float fp8_to_float(uint8_t b) {
     return __half2float(__half(__nv_cvt_fp8_to_halfraw((__nv_fp8_storage_t)b, __NV_E4M3)));
 }
 
+// x-window position source of a staged mixed row block, one instruction
+// stream for both kinds: plane k of lane r sits at (p[k * stride] & POS) +
+// add, with p = base, stride 1, add = r for affine blocks and p = idx + r,
+// stride 16, add 0 otherwise (two half-warps of a warp may hold one of each
+// without diverging).
+struct PosSrc {
+    const uint16_t *p;
+    uint32_t stride, add;
+    __device__ __forceinline__ uint32_t operator()(int k) const {
+        return ((uint32_t)p[(uint32_t)k * stride] & IDX16_POS) + add;
+    }
+};
+__device__ __forceinline__ PosSrc pos_src(const uint8_t *blk, int W, int r, uint32_t flags) {
+    PosSrc s;
+    if (flags & RBF_AFFINE) {
+        s.p = reinterpret_cast<const uint16_t *>(blk + rbm_base_off(W));
+        s.stride = 1u;
+        s.add = (uint32_t)r;
+    } else {
+        s.p = reinterpret_cast<const uint16_t *>(blk + rbm_idx_off(W, false)) + r;
+        s.stride = 16u;
+        s.add = 0u;
+    }
+    return s;
+}
+
+// Class-group loops of a mixed row block (FP32, FP16, FP8 classes, each
+// plane stored in its class type): sumf = fmaf((float)x, v, sumf) plane by
+// plane from plane k on. UNSC: every scale is 1.
+template <bool UNSC, typename XT>
+__device__ __forceinline__ float low_groups(const uint8_t *vals, int k, int n32, int n16, int n8, int r,
+                                            const int8_t *sexp, const XT *xs, const PosSrc &pos, float sumf) {
+    const float *v32 = reinterpret_cast<const float *>(vals) + r;
+#pragma unroll 4
+    for (int j = 0; j < n32; ++j) sumf = __fmaf_rn(to_f32(xs[pos(k + j)]), v32[j * 16], sumf);
+    k += n32;
+    const __half *h = reinterpret_cast<const __half *>(vals + 64u * n32) + r;
+#pragma unroll 4
+    for (int j = 0; j < n16; ++j) {
+        const float v = __half2float(h[j * 16]);
+        sumf = __fmaf_rn(to_f32(xs[pos(k + j)]), UNSC ? v : v * exp2_int(sexp[k + j]), sumf);
+    }
+    k += n16;
+    const uint8_t *b8 = vals + 64u * n32 + 32u * n16 + r;
+    for (int j = 0; j < n8; ++j) {
+        const float v = fp8_to_float(b8[j * 16]);
+        sumf = __fmaf_rn(to_f32(xs[pos(k + j)]), UNSC ? v : v * exp2_int(sexp[k + j]), sumf);
+    }
+    return sumf;
+}
+
+// Two staged row blocks, each with one FP32-class and N16 FP16-class planes
+// (all stored in their class type), fully unrolled so that a lane issues
+// all position, x and value loads of both rows before the first FMA: the row
+// sums of mixed_row, in the same order. UNSC: every scale is 1.
+template <int N16, bool UNSC>
+__device__ __forceinline__ void rows2_fixed(const uint8_t *b1, const uint8_t *b2, uint32_t f1, uint32_t f2, int r,
+                                            const float *xs, float &s1, float &s2) {
+    constexpr int NW = 1 + N16;
+    const PosSrc p1 = pos_src(b1, NW, r, f1), p2 = pos_src(b2, NW, r, f2);
+    const uint8_t *v1 = b1 + rbm_vals_off(NW, false, (f1 & RBF_AFFINE) != 0);
+    const uint8_t *v2 = b2 + rbm_vals_off(NW, false, (f2 & RBF_AFFINE) != 0);
+    const int8_t *e1 = reinterpret_cast<const int8_t *>(b1 + rbm_sexp_off());
+    const int8_t *e2 = reinterpret_cast<const int8_t *>(b2 + rbm_sexp_off());
+    float x1[NW], x2[NW], w1[NW], w2[NW];
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+        x1[k] = xs[p1(k)];
+        x2[k] = xs[p2(k)];
+    }
+    w1[0] = reinterpret_cast<const float *>(v1)[r];
+    w2[0] = reinterpret_cast<const float *>(v2)[r];
+#pragma unroll
+    for (int j = 0; j < N16; ++j) {
+        const float h1 = __half2float(reinterpret_cast<const __half *>(v1 + 64u)[j * 16 + r]);
+        const float h2 = __half2float(reinterpret_cast<const __half *>(v2 + 64u)[j * 16 + r]);
+        w1[1 + j] = UNSC ? h1 : h1 * exp2_int(e1[1 + j]);
+        w2[1 + j] = UNSC ? h2 : h2 * exp2_int(e2[1 + j]);
+    }
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+        s1 = __fmaf_rn(x1[k], w1[k], s1);
+        s2 = __fmaf_rn(x2[k], w2[k], s2);
+    }
+}
+
 // Row r of a mixed-layout row block (planes grouped by entry class, see
 // tiles.h). FP64-class entries: sum = 0, sum += x*v, acc += sum at each tile
 // start, exactly blockspmv_cpu's order. The FP32-, FP16- and FP8-class
@@ -107,18 +193,23 @@ __device__ __forceinline__ float fp8_to_float(uint8_t b) {
 template <bool GATHER, typename XT>
 __device__ __forceinline__ double mixed_row(const uint8_t *blk, int W, int r, const XT *xs,
                                             const XT *__restrict__ xg) {
-    const uint8_t *pi = blk + rb_pinfo_off();
-    const uint32_t cnt = *reinterpret_cast<const uint32_t *>(pi + 40);
+    const uint32_t cnt = *reinterpret_cast<const uint32_t *>(blk);
+    const uint32_t flags = blk[4];
     const int n64 = cnt & 0xffu, n32 = (cnt >> 8) & 0xffu, n16 = (cnt >> 16) & 0xffu, n8 = cnt >> 24;
-    const bool fast = pi[44] != 0;
-    const int8_t *sexp = reinterpret_cast<const int8_t *>(pi + 8);
-    const uint8_t *idxb = blk + rb_idx_off(W, true);
-    const uint8_t *vals = blk + rb_vals_off(W, true, GATHER);
+    const int8_t *sexp = reinterpret_cast<const int8_t *>(blk + rbm_sexp_off());
+    const bool aff = !GATHER && (flags & RBF_AFFINE);
+    const uint8_t *idxb = blk + rbm_idx_off(W, aff);
+    const uint8_t *vals = blk + rbm_vals_off(W, GATHER, aff);
+    const uint16_t *base = reinterpret_cast<const uint16_t *>(blk + rbm_base_off(W));
     auto ld_x = [&](int k, uint32_t &id) -> XT {
         if constexpr (GATHER) {
             id = reinterpret_cast<const uint32_t *>(idxb)[k * 16 + r];
             return (id & IDX32_PAD) ? XT(0) : __ldcg(xg + (id & IDX32_POS));
         } else {
+            if (aff) {
+                id = (uint32_t)base[k] + (uint32_t)r;
+                return xs[id];
+            }
             id = reinterpret_cast<const uint16_t *>(idxb)[k * 16 + r];
             return xs[id & IDX16_POS];
         }
@@ -142,34 +233,38 @@ __device__ __forceinline__ double mixed_row(const uint8_t *blk, int W, int r, co
         voff = 128u * n64;
     }
     float sumf = 0.0f;
-    {
-        const float *v = reinterpret_cast<const float *>(vals + voff) + r;
-#pragma unroll 4
-        for (int j = 0; j < n32; ++j) {
-            uint32_t id;
-            const XT x = ld_x(k + j, id);
-            sumf = __fmaf_rn(to_f32(x), v[j * 16], sumf);
-        }
-        k += n32;
-        voff += 64u * n32;
-    }
-    if (fast) {
-        const __half *h = reinterpret_cast<const __half *>(vals + voff) + r;
-#pragma unroll 4
-        for (int j = 0; j < n16; ++j) {
-            uint32_t id;
-            const XT x = ld_x(k + j, id);
-            sumf = __fmaf_rn(to_f32(x), __half2float(h[j * 16]) * exp2_int(sexp[k + j]), sumf);
-        }
-        k += n16;
-        voff += 32u * n16;
-        for (int j = 0; j < n8; ++j) {
-            uint32_t id;
-            const XT x = ld_x(k + j, id);
-            sumf = __fmaf_rn(to_f32(x), fp8_to_float(vals[voff + j * 16 + r]) * exp2_int(sexp[k + j]), sumf);
+    if (flags & RBF_FAST) {
+        if constexpr (GATHER) {
+            // gather rows: x from L2; padding entries (PAD) read as 0
+            const float *v32 = reinterpret_cast<const float *>(vals + voff) + r;
+            for (int j = 0; j < n32; ++j) {
+                uint32_t id;
+                const XT x = ld_x(k + j, id);
+                sumf = __fmaf_rn(to_f32(x), v32[j * 16], sumf);
+            }
+            k += n32;
+            voff += 64u * n32;
+            const __half *h = reinterpret_cast<const __half *>(vals + voff) + r;
+            for (int j = 0; j < n16; ++j) {
+                uint32_t id;
+                const XT x = ld_x(k + j, id);
+                sumf = __fmaf_rn(to_f32(x), __half2float(h[j * 16]) * exp2_int(sexp[k + j]), sumf);
+            }
+            k += n16;
+            voff += 32u * n16;
+            for (int j = 0; j < n8; ++j) {
+                uint32_t id;
+                const XT x = ld_x(k + j, id);
+                sumf = __fmaf_rn(to_f32(x), fp8_to_float(vals[voff + j * 16 + r]) * exp2_int(sexp[k + j]), sumf);
+            }
+        } else {
+            const PosSrc pos = pos_src(blk, W, r, flags);
+            sumf = (flags & RBF_UNSCALED) ? low_groups<true>(vals + voff, k, n32, n16, n8, r, sexp, xs, pos, sumf)
+                                          : low_groups<false>(vals + voff, k, n32, n16, n8, r, sexp, xs, pos, sumf);
         }
     } else {
-        const uint64_t pbits = *reinterpret_cast<const uint64_t *>(pi);
+        // some FP16 / FP8 class plane stored wider: decode plane by plane
+        const uint64_t pbits = *reinterpret_cast<const uint64_t *>(blk + 8);
         for (; k < W; ++k) {
             const uint32_t pr = (uint32_t)(pbits >> (2 * k)) & 3u;
             uint32_t id;
@@ -202,12 +297,12 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
     const bool gather = h.mode == SLAB_GATHER;
     double acc = 0.0, sum = 0.0;
     if (KIND == LAYOUT_FP64) {
-        const double *vals = reinterpret_cast<const double *>(blk + rb_vals_off(W, false, gather));
+        const double *vals = reinterpret_cast<const double *>(blk + rb_vals_off(W, gather));
         if (!gather) {
             // all W planes: padding entries add x(zero slot) * 0 = +0 to a sum
             // that is never -0, which leaves it unchanged; the trip count is
             // the same for the 16 lanes of the row block
-            const uint16_t *idx = reinterpret_cast<const uint16_t *>(blk + rb_idx_off(W, false));
+            const uint16_t *idx = reinterpret_cast<const uint16_t *>(blk + rb_idx_off());
 #pragma unroll 4
             for (int k = 0; k < W; ++k) {
                 const uint32_t id = idx[k * 16 + r];
@@ -220,7 +315,7 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
                 sum = dadd(sum, dmul(x, v));
             }
         } else if (GB == 1) {
-            const uint32_t *idx = reinterpret_cast<const uint32_t *>(blk + rb_idx_off(W, false));
+            const uint32_t *idx = reinterpret_cast<const uint32_t *>(blk + rb_idx_off());
 #pragma unroll 4
             for (int k = 0; k < len; ++k) {
                 const uint32_t id = idx[k * 16 + r];
@@ -235,7 +330,7 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
         } else {
             // x comes from L2 entry by entry: issue GB loads before the
             // first is used so that a lane keeps GB gathers in flight
-            const uint32_t *idx = reinterpret_cast<const uint32_t *>(blk + rb_idx_off(W, false));
+            const uint32_t *idx = reinterpret_cast<const uint32_t *>(blk + rb_idx_off());
             for (int k0 = 0; k0 < len; k0 += GB) {
                 uint32_t id[GB];
                 double v[GB];
@@ -265,60 +360,73 @@ __device__ __forceinline__ double slab_row(const uint8_t *st, const SlabHeader &
     return gather ? mixed_row<true>(blk, W, r, xstage, xg) : mixed_row<false>(blk, W, r, xstage, xg);
 }
 
-// Two staged row blocks of one half-warp whose class groups are FP32, FP16
-// and FP8 planes only, equal in number and all stored in their class type,
-// interleaved in one loop: two independent load and accumulate chains per
-// lane, each in the order of mixed_row (identical results). Returns false
+// Two staged row blocks of one half-warp without FP64-class planes, all
+// planes stored in their class type, with equal class groups and scale
+// flags, interleaved in one loop: two independent load and accumulate chains
+// per lane, each in the order of mixed_row (identical results). Returns false
 // (nothing computed) when the pair does not qualify.
+template <bool UNSC>
+__device__ __forceinline__ void pair_groups(const uint8_t *b1, const uint8_t *b2, int W, uint32_t f1, uint32_t f2,
+                                            int n32, int n16, int n8, int r, const float *xs, float &s1, float &s2) {
+    const PosSrc p1 = pos_src(b1, W, r, f1), p2 = pos_src(b2, W, r, f2);
+    const int8_t *e1 = reinterpret_cast<const int8_t *>(b1 + rbm_sexp_off());
+    const int8_t *e2 = reinterpret_cast<const int8_t *>(b2 + rbm_sexp_off());
+    const uint8_t *v1 = b1 + rbm_vals_off(W, false, f1 & RBF_AFFINE), *v2 = b2 + rbm_vals_off(W, false, f2 & RBF_AFFINE);
+    {
+        const float *w1 = reinterpret_cast<const float *>(v1) + r, *w2 = reinterpret_cast<const float *>(v2) + r;
+#pragma unroll 2
+        for (int k = 0; k < n32; ++k) {
+            s1 = __fmaf_rn(xs[p1(k)], w1[k * 16], s1);
+            s2 = __fmaf_rn(xs[p2(k)], w2[k * 16], s2);
+        }
+    }
+    const int k0 = n32;
+    const __half *h1 = reinterpret_cast<const __half *>(v1 + 64u * n32) + r;
+    const __half *h2 = reinterpret_cast<const __half *>(v2 + 64u * n32) + r;
+#pragma unroll 2
+    for (int j = 0; j < n16; ++j) {
+        const int k = k0 + j;
+        const float a1 = __half2float(h1[j * 16]), a2 = __half2float(h2[j * 16]);
+        s1 = __fmaf_rn(xs[p1(k)], UNSC ? a1 : a1 * exp2_int(e1[k]), s1);
+        s2 = __fmaf_rn(xs[p2(k)], UNSC ? a2 : a2 * exp2_int(e2[k]), s2);
+    }
+    const int k1 = n32 + n16;
+    const uint32_t o8 = 64u * n32 + 32u * n16 + r;
+    for (int j = 0; j < n8; ++j) {
+        const int k = k1 + j;
+        const float a1 = fp8_to_float(v1[o8 + j * 16]), a2 = fp8_to_float(v2[o8 + j * 16]);
+        s1 = __fmaf_rn(xs[p1(k)], UNSC ? a1 : a1 * exp2_int(e1[k]), s1);
+        s2 = __fmaf_rn(xs[p2(k)], UNSC ? a2 : a2 * exp2_int(e2[k]), s2);
+    }
+}
+
 __device__ __forceinline__ bool pair_mixed(const uint8_t *st, int j1, int j2, int r, const float *xs, double &a1,
                                            double &a2) {
     const RbDir *dir = reinterpret_cast<const RbDir *>(st + slab_rbdir_off());
     const RbDir d1 = dir[j1], d2 = dir[j2];
     const int W = (int)(d1.W & 0xffffu);
     const uint8_t *b1 = st + d1.off, *b2 = st + d2.off;
-    const uint32_t c1 = *reinterpret_cast<const uint32_t *>(b1 + rb_pinfo_off() + 40);
-    const uint32_t c2 = *reinterpret_cast<const uint32_t *>(b2 + rb_pinfo_off() + 40);
-    const uint32_t f1 = *reinterpret_cast<const uint32_t *>(b1 + rb_pinfo_off() + 44);
-    const uint32_t f2 = *reinterpret_cast<const uint32_t *>(b2 + rb_pinfo_off() + 44);
-    if (c1 != c2 || (c1 & 0xffu) != 0u || (f1 & 0xffu) == 0u || (f2 & 0xffu) == 0u) return false;
+    const uint32_t c1 = *reinterpret_cast<const uint32_t *>(b1), c2 = *reinterpret_cast<const uint32_t *>(b2);
+    const uint32_t f1 = b1[4], f2 = b2[4];
+    if (c1 != c2 || (c1 & 0xffu) != 0u || ((f1 ^ f2) & RBF_UNSCALED) || !(f1 & f2 & RBF_FAST)) return false;
     const int n32 = (c1 >> 8) & 0xffu, n16 = (c1 >> 16) & 0xffu, n8 = c1 >> 24;
-    const uint16_t *i1 = reinterpret_cast<const uint16_t *>(b1 + rb_idx_off(W, true)) + r;
-    const uint16_t *i2 = reinterpret_cast<const uint16_t *>(b2 + rb_idx_off(W, true)) + r;
-    const int8_t *e1 = reinterpret_cast<const int8_t *>(b1 + rb_pinfo_off() + 8);
-    const int8_t *e2 = reinterpret_cast<const int8_t *>(b2 + rb_pinfo_off() + 8);
-    const uint8_t *v1 = b1 + rb_vals_off(W, true, false);
-    const uint8_t *v2 = b2 + rb_vals_off(W, true, false);
     float s1 = 0.0f, s2 = 0.0f;
-    {
-        const float *w1 = reinterpret_cast<const float *>(v1) + r, *w2 = reinterpret_cast<const float *>(v2) + r;
-#pragma unroll 2
-        for (int k = 0; k < n32; ++k) {
-            const float x1 = xs[i1[k * 16] & IDX16_POS], x2 = xs[i2[k * 16] & IDX16_POS];
-            s1 = __fmaf_rn(x1, w1[k * 16], s1);
-            s2 = __fmaf_rn(x2, w2[k * 16], s2);
+    if (n8 == 0 && n32 == 1 && (n16 == 6 || n16 == 4)) {
+        // the 3D 7-point / 2D 5-point stencil shapes, fully unrolled
+        const bool u = (f1 & RBF_UNSCALED) != 0;
+        if (n16 == 6) {
+            if (u) rows2_fixed<6, true>(b1, b2, f1, f2, r, xs, s1, s2);
+            else rows2_fixed<6, false>(b1, b2, f1, f2, r, xs, s1, s2);
+        } else {
+            if (u) rows2_fixed<4, true>(b1, b2, f1, f2, r, xs, s1, s2);
+            else rows2_fixed<4, false>(b1, b2, f1, f2, r, xs, s1, s2);
         }
+        a1 = (double)s1;
+        a2 = (double)s2;
+        return true;
     }
-    int k0 = n32;
-    uint32_t voff = 64u * n32;
-    {
-        const __half *h1 = reinterpret_cast<const __half *>(v1 + voff) + r;
-        const __half *h2 = reinterpret_cast<const __half *>(v2 + voff) + r;
-#pragma unroll 2
-        for (int j = 0; j < n16; ++j) {
-            const int k = k0 + j;
-            const float x1 = xs[i1[k * 16] & IDX16_POS], x2 = xs[i2[k * 16] & IDX16_POS];
-            s1 = __fmaf_rn(x1, __half2float(h1[j * 16]) * exp2_int(e1[k]), s1);
-            s2 = __fmaf_rn(x2, __half2float(h2[j * 16]) * exp2_int(e2[k]), s2);
-        }
-        k0 += n16;
-        voff += 32u * n16;
-    }
-    for (int j = 0; j < n8; ++j) {
-        const int k = k0 + j;
-        const float x1 = xs[i1[k * 16] & IDX16_POS], x2 = xs[i2[k * 16] & IDX16_POS];
-        s1 = __fmaf_rn(x1, fp8_to_float(v1[voff + j * 16 + r]) * exp2_int(e1[k]), s1);
-        s2 = __fmaf_rn(x2, fp8_to_float(v2[voff + j * 16 + r]) * exp2_int(e2[k]), s2);
-    }
+    if (f1 & RBF_UNSCALED) pair_groups<true>(b1, b2, W, f1, f2, n32, n16, n8, r, xs, s1, s2);
+    else pair_groups<false>(b1, b2, W, f1, f2, n32, n16, n8, r, xs, s1, s2);
     a1 = (double)s1;
     a2 = (double)s2;
     return true;
@@ -376,7 +484,7 @@ __device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const void *xv,
                              Pipe &pp, Epi &epi) {
     const int ns = L.ns;
     const int stride = C.stage_stride;
-    const int slab_area = C.slab_area;
+    const int xoff = x_off_of(C.slab_area, L.x32 != 0);  // the layout's x window in a stage
     const int tid = threadIdx.x;
     const int w = tid >> 5, lane = tid & 31;
     const int half = lane >> 4, r = lane & 15;
@@ -427,12 +535,12 @@ __device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const void *xv,
                     const uint32_t segb = L.x32 ? 64u : 128u;
                     for (int q = 0; q < nruns; ++q) {
                         const XRun rr = runs[q];
-                        bulk_g2s(st + slab_area + (size_t)rr.slot0 * segb,
+                        bulk_g2s(st + xoff + (size_t)rr.slot0 * segb,
                                  static_cast<const uint8_t *>(xv) + (size_t)rr.seg0 * segb, (uint32_t)rr.nseg * segb,
                                  &S.full[k], pv);
                     }
                 } else {
-                    issue_slab(S, st, slab_area, k, off16, bytes, xbytes, nruns, runs, L.slabs,
+                    issue_slab(S, st, xoff, k, off16, bytes, xbytes, nruns, runs, L.slabs,
                                static_cast<const uint8_t *>(xv), L.x32 ? 64u : 128u, pm, pv);
                     S.res_tag[k] = keep ? (uint8_t)(L.site + 1) : (uint8_t)0;
                 }
@@ -467,7 +575,7 @@ __device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const void *xv,
                 int j0 = 2 * w + half - base;
                 if (j0 < 0) j0 += 2 * NWARPS;
                 base = (base + h.nrb) % (2 * NWARPS);
-                const double *xsg = reinterpret_cast<const double *>(st + slab_area);
+                const double *xsg = reinterpret_cast<const double *>(st + xoff);
                 using PV = decltype(epi.pre(0));
                 // the pre-loaded value keeps its own type until the epilogue:
                 // a conversion here would wait for the load before the row's
@@ -490,7 +598,7 @@ __device__ bool cta_spmv_src(const SpmvSrc &L, const PipeCfg &C, const void *xv,
                     // row blocks j and j + 2 NWARPS of this half-warp computed
                     // together; a pair that does not qualify (or a lone last
                     // row block) goes to the loop below
-                    const float *xs = reinterpret_cast<const float *>(st + slab_area);
+                    const float *xs = reinterpret_cast<const float *>(st + xoff);
                     for (; jstart + 2 * NWARPS < h.nrb; jstart += 4 * NWARPS) {
                         const int j2 = jstart + 2 * NWARPS;
                         const int row1 = (h.rb0 + jstart) * 16 + r, row2 = (h.rb0 + j2) * 16 + r;
@@ -1156,7 +1264,12 @@ int launch_jacobi_inv(int n, int npad, const double *diag, double *minv, cudaStr
 // solve stops.
 //   p = r + beta p;  s = w + beta s;  x += alpha p;  r -= alpha s;
 //   w = A r;  gamma = r.r;  delta = w.r;
-//   beta = gamma / gamma_old;  alpha = gamma / (delta - beta gamma / alpha_old)
+//   beta = gamma / gamma_old;  alpha = gamma / (delta + 2 beta r.s + beta^2 p.s)
+// with r.s and p.s (the previous s and p) summed in the vector pass (or, for
+// r.s, after a replacement) and reduced with gamma and delta: the textbook
+// delta - beta gamma / alpha_old assumes r orthogonal to the previous
+// direction, which each replacement breaks by the low-precision operator's
+// gap to A.
 struct EpiW {  // w = A r (FP32), gamma += r*r, delta += w*r
     static constexpr bool kUsesX = false;
     const double *r;
@@ -1175,8 +1288,10 @@ struct EpiW {  // w = A r (FP32), gamma += r*r, delta += w*r
 __global__ void __launch_bounds__(NTHREADS, 1) k_cgcg(KParams P) {
     extern __shared__ __align__(128) uint8_t dyn[];
     __shared__ Smem S;
+    __shared__ double s_wpart[2][NWARPS + 1];  // the warps' shares of r.s and p.s
     kernel_setup(P, S, P.nlay);
     const int g = blockIdx.x, tid = threadIdx.x;
+    const int lane = tid & 31, wid = tid >> 5;
     Pipe pp;
     uint32_t phase = 0;
     const uint64_t vpol = policy_evict_last();
@@ -1204,6 +1319,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cgcg(KParams P) {
             stf2_hint(sv32 + 2 * MF_PI(u), make_float2(0.f, 0.f), vpol);
         }
     })
+    if (lane == 0) s_wpart[0][wid] = s_wpart[1][wid] = 0.0;
     double v1[1] = {bbp}, o1[1];
     if (!grid_sum<1>(P, S, v1, o1, phase)) return;
     const double bb = o1[0];
@@ -1213,7 +1329,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cgcg(KParams P) {
     publish(P, ep);
     int it = 0, status = MF_OK, repl = 0, switches = 0, fellback = 0;
     int it_lay[KMAX_LAYOUTS] = {0, 0, 0, 0};
-    double gamma_old = 0.0, alpha_old = 1.0, rel = 1.0, rr_best = 1e300, gam = 0.0;
+    double gamma_old = 0.0, rel = 1.0, rr_best = 1e300, gam = 0.0;
     bool first = true, pending = false;
     const bool fixed = P.fixed_iterations > 0;
     const int maxit = fixed ? P.fixed_iterations : P.maxiter;
@@ -1223,6 +1339,21 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cgcg(KParams P) {
             if (!wait_deps(P, S, lay64, ep)) return;
             EpiResidual32 e2{b, r, r32, 0.0, vpol};
             if (!cta_spmv<false>(P, lay64, x, S, dyn, pp, e2)) return;
+            // r.s of the replaced r with the current s (p.s is unchanged)
+            double rsl = 0.0;
+            MF_PAIRS(2, vlo, vhi, {
+                double2 rv[_vb];
+                float2 sw[_vb];
+#pragma unroll
+                MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                    rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+                    sw[u] = ldf2_hint(sv32 + 2 * MF_PI(u), vpol);
+                }
+#pragma unroll
+                MF_FOR_VB if (MF_LIVE(u, vhi)) rsl += rv[u].x * (double)sw[u].x + rv[u].y * (double)sw[u].y;
+            })
+            for (int o = 16; o > 0; o >>= 1) rsl += __shfl_xor_sync(0xffffffffu, rsl, o);
+            if (lane == 0) s_wpart[0][wid] = rsl;
             double a1[1] = {e2.rr}, c1[1];
             if (!grid_sum<1>(P, S, a1, c1, phase)) return;
             ++repl;
@@ -1257,11 +1388,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cgcg(KParams P) {
         else ok = cta_spmv<false>(P, lay64, r, S, dyn, pp, ew);
         if (!ok) return;
         MF_TRACE(it, 2);
-        double a2[2] = {ew.g, ew.dl}, c2[2];
-        if (!grid_sum<2>(P, S, a2, c2, phase)) return;
+        double a2[4] = {ew.g, ew.dl, lane == 0 ? s_wpart[0][wid] : 0.0, lane == 0 ? s_wpart[1][wid] : 0.0}, c2[4];
+        if (!grid_sum<4>(P, S, a2, c2, phase)) return;
         MF_TRACE(it, 3);
         gam = c2[0];
-        const double delta = c2[1];
+        const double delta = c2[1], rs_old = c2[2], ps_old = c2[3];
         rel = bnorm > 0 ? sqrt(gam) / bnorm : 0.0;
         if (!fixed && rel <= tol) {
             pending = true;  // confirm with the FP64 true residual
@@ -1274,12 +1405,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cgcg(KParams P) {
             first = false;
         } else {
             beta = gam / gamma_old;
-            alpha = gam / (delta - beta * gam / alpha_old);
+            alpha = gam / (delta + beta * (2.0 * rs_old + beta * ps_old));  // p.A p, as in cgcg_tm_body
         }
         if (!isfinite(alpha) || !isfinite(beta) || alpha == 0.0) {
             status = MF_ERR_BREAKDOWN;
             break;
         }
+        double rsn = 0.0, psn = 0.0;
         MF_PAIRS(4, vlo, vhi, {
             double2 rv[_vb], xv[_vb];
             float2 pw[_vb], sw[_vb], ww[_vb];
@@ -1308,10 +1440,19 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cgcg(KParams P) {
                 st2_hint(x + 2 * MF_PI(u), xo, vpol);
                 st2_hint(r + 2 * MF_PI(u), ro, vpol);
                 stf2_hint(r32 + 2 * MF_PI(u), make_float2(__double2float_rn(ro.x), __double2float_rn(ro.y)), vpol);
+                rsn += ro.x * (double)sf.x + ro.y * (double)sf.y;
+                psn += (double)pf.x * (double)sf.x + (double)pf.y * (double)sf.y;
             }
         })
+        for (int o = 16; o > 0; o >>= 1) {
+            rsn += __shfl_xor_sync(0xffffffffu, rsn, o);
+            psn += __shfl_xor_sync(0xffffffffu, psn, o);
+        }
+        if (lane == 0) {
+            s_wpart[0][wid] = rsn;
+            s_wpart[1][wid] = psn;
+        }
         gamma_old = gam;
-        alpha_old = alpha;
         MF_TRACE(it, 4);
         MF_TRACE(it, 5);
         ++it;
@@ -1481,8 +1622,8 @@ __device__ void tm_upd_issue(Smem &S, uint8_t *dyn, const float *pv, const float
 // thread's share of the new r.r.
 __device__ double tm_update_smem(const TmemRows &T, double alpha, double beta, const float *sp,
                                               const float *ss, const float *sw, float *pv, float *sv, float *r32,
-                                              double *rg, uint64_t pol) {
-    double rr = 0.0;
+                                              double *rg, uint64_t pol, double &rs_out, double &ps_out) {
+    double rr = 0.0, rs = 0.0, ps = 0.0;
     const float bf = (float)beta;
     for (int k = T.k0; k < T.nblk; k += 4 * TM_CB) {
         uint32_t t[TM_CB][16];
@@ -1508,7 +1649,7 @@ __device__ double tm_update_smem(const TmemRows &T, double alpha, double beta, c
                 const float sin_[4] = {sf.x, sf.y, sf.z, sf.w};
                 const float win[4] = {wf.x, wf.y, wf.z, wf.w};
                 float pn[4], sn[4], rn[4];
-                double rsq = 0.0;
+                double rsq = 0.0, rsd = 0.0, psd = 0.0;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     double xv = tm_x(t[u], j), rv = tm_r(t[u], j);
@@ -1519,6 +1660,8 @@ __device__ double tm_update_smem(const TmemRows &T, double alpha, double beta, c
                     tm_set(t[u], j, xv, rv);
                     rn[j] = __double2float_rn(rv);
                     rsq += rv * rv;
+                    rsd += rv * (double)sn[j];
+                    psd += (double)pn[j] * (double)sn[j];
                 }
                 tmem_st16_wait(T.addr(kk), t[u]);
                 if (live) {
@@ -1531,15 +1674,19 @@ __device__ double tm_update_smem(const TmemRows &T, double alpha, double beta, c
                         st2_hint(rg + row + 2, make_double2(tm_r(t[u], 2), tm_r(t[u], 3)), pol);
                     }
                     rr += rsq;
+                    rs += rsd;
+                    ps += psd;
                 }
             }
         }
     }
+    rs_out = rs;
+    ps_out = ps;
     return rr;
 }
 
 __device__ __forceinline__ void cgcg_tm_body(const KParams &P, Smem &S, uint8_t *dyn, const volatile uint32_t *s_tmem,
-                                             volatile double *s_gpart) {
+                                             volatile double *s_gpart, volatile double (*s_wpart)[NWARPS + 1]) {
     const int g = blockIdx.x, tid = threadIdx.x;
     Pipe pp;
     uint32_t phase = 0;
@@ -1573,8 +1720,11 @@ __device__ __forceinline__ void cgcg_tm_body(const KParams &P, Smem &S, uint8_t 
         }
     })
     // this thread's share of r.r, carried to the next reduction in shared
-    // memory (not in a register across the SpMV)
+    // memory (not in a register across the SpMV); the warps' shares of r.s
+    // and p.s (p = s = 0 before the first iteration) likewise
     s_gpart[tid] = tm_load(tm_rows(P, s_tmem), x, r, vpol);
+    const int lane = tid & 31, wid = tid >> 5;
+    if (lane == 0) s_wpart[0][wid] = s_wpart[1][wid] = 0.0;
     double v1[1] = {bbp}, o1[1];
     if (!grid_sum<1>(P, S, v1, o1, phase)) return;
     const double bb = o1[0];
@@ -1584,7 +1734,7 @@ __device__ __forceinline__ void cgcg_tm_body(const KParams &P, Smem &S, uint8_t 
     publish(P, ep);
     int it = 0, status = MF_OK, repl = 0, switches = 0, fellback = 0;
     int it_lay[KMAX_LAYOUTS] = {0, 0, 0, 0};
-    double gamma_old = 0.0, alpha_old = 1.0, rel = 1.0, rr_best = 1e300, gam = 0.0;
+    double gamma_old = 0.0, rel = 1.0, rr_best = 1e300, gam = 0.0;
     bool first = true, pending = false;
     const bool fixed = P.fixed_iterations > 0;
     const int maxit = fixed ? P.fixed_iterations : P.maxiter;
@@ -1601,6 +1751,22 @@ __device__ __forceinline__ void cgcg_tm_body(const KParams &P, Smem &S, uint8_t 
             if (!cta_spmv<false>(P, lay64, x, S, dyn, pp, e2)) return;
             const double gl = tm_load(tm_rows(P, s_tmem), nullptr, r, vpol);
             s_gpart[tid] = gl;
+            // r.s of the replaced r with the current s (the next step's
+            // p.A p needs it; p.s is unchanged)
+            double rsl = 0.0;
+            MF_PAIRS(2, vlo, vhi, {
+                double2 rv[_vb];
+                float2 sv[_vb];
+#pragma unroll
+                MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                    rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+                    sv[u] = *reinterpret_cast<const float2 *>(sv32 + 2 * MF_PI(u));
+                }
+#pragma unroll
+                MF_FOR_VB if (MF_LIVE(u, vhi)) rsl += rv[u].x * (double)sv[u].x + rv[u].y * (double)sv[u].y;
+            })
+            for (int o = 16; o > 0; o >>= 1) rsl += __shfl_xor_sync(0xffffffffu, rsl, o);
+            if (lane == 0) s_wpart[0][wid] = rsl;
             double a1[1] = {gl}, c1[1];
             if (!grid_sum<1>(P, S, a1, c1, phase)) return;
             ++repl;
@@ -1641,8 +1807,9 @@ __device__ __forceinline__ void cgcg_tm_body(const KParams &P, Smem &S, uint8_t 
         fence_proxy_async_global();
         __syncthreads();
         if (tid == 0) tm_upd_issue(S, dyn, pv32, sv32, wv32, vlo, vhi - vlo, vpol);
-        double a2[2] = {s_gpart[tid], ew.dl}, c2[2];
-        const bool red_ok = grid_sum<2>(P, S, a2, c2, phase);
+        double a2[4] = {s_gpart[tid], ew.dl, lane == 0 ? s_wpart[0][wid] : 0.0, lane == 0 ? s_wpart[1][wid] : 0.0},
+               c2[4];
+        const bool red_ok = grid_sum<4>(P, S, a2, c2, phase);
         // no path leaves with the copies in flight
         if (!wait_bar(&S.upd, uph, P.limit_ns)) {
             set_error(P, (uint32_t)MF_ERR_TIMEOUT, 30);
@@ -1652,13 +1819,19 @@ __device__ __forceinline__ void cgcg_tm_body(const KParams &P, Smem &S, uint8_t 
         if (!red_ok) return;
         MF_TRACE(it, 3);
         gam = c2[0];
-        const double delta = c2[1];
+        const double delta = c2[1], rs_old = c2[2], ps_old = c2[3];
         rel = bnorm > 0 ? sqrt(gam) / bnorm : 0.0;
         if (!fixed && rel <= tol) {
             pending = true;  // confirm with the FP64 true residual
             zero_slots(dyn, P.stage_stride, P.slab_area);  // the copies overwrote them
             continue;
         }
+        // p = r + beta p_old, s = w + beta s_old: p.A p = p.s = r.w + 2 beta
+        // r.s_old + beta^2 p_old.s_old (A symmetric). Summed from its parts
+        // rather than taken as delta - beta gamma / alpha_old, which assumes
+        // the orthogonality of r to the previous direction: a true-residual
+        // replacement breaks that by the gap between the low-precision
+        // operator and A.
         double alpha, beta;
         if (first) {
             beta = 0.0;
@@ -1666,17 +1839,25 @@ __device__ __forceinline__ void cgcg_tm_body(const KParams &P, Smem &S, uint8_t 
             first = false;
         } else {
             beta = gam / gamma_old;
-            alpha = gam / (delta - beta * gam / alpha_old);
+            alpha = gam / (delta + beta * (2.0 * rs_old + beta * ps_old));
         }
         if (!isfinite(alpha) || !isfinite(beta) || alpha == 0.0) {
             status = MF_ERR_BREAKDOWN;
             break;
         }
         const float *sp = reinterpret_cast<const float *>(dyn);
+        double rsn, psn;
         s_gpart[tid] = tm_update_smem(tm_rows(P, s_tmem), alpha, beta, sp, sp + (vhi - vlo), sp + 2 * (vhi - vlo),
-                                      pv32, sv32, r32, lay == lay64 ? r : nullptr, vpol);
+                                      pv32, sv32, r32, lay == lay64 ? r : nullptr, vpol, rsn, psn);
+        for (int o = 16; o > 0; o >>= 1) {
+            rsn += __shfl_xor_sync(0xffffffffu, rsn, o);
+            psn += __shfl_xor_sync(0xffffffffu, psn, o);
+        }
+        if (lane == 0) {
+            s_wpart[0][wid] = rsn;
+            s_wpart[1][wid] = psn;
+        }
         gamma_old = gam;
-        alpha_old = alpha;
         MF_TRACE(it, 4);
         MF_TRACE(it, 5);
         ++it;
@@ -1710,13 +1891,14 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cgcg_tm(KParams P) {
     __shared__ Smem S;
     __shared__ uint32_t s_tmem;
     __shared__ double s_gpart[NTHREADS];
+    __shared__ double s_wpart[2][NWARPS + 1];
     kernel_setup(P, S, P.nlay);
     const int w = threadIdx.x >> 5;
     if (w == 0) tmem_alloc512(&s_tmem);
     tcgen05_fence_before_sync();
     __syncthreads();
     tcgen05_fence_after_sync();
-    cgcg_tm_body(P, S, dyn, &s_tmem, s_gpart);
+    cgcg_tm_body(P, S, dyn, &s_tmem, s_gpart, s_wpart);
     tcgen05_fence_before_sync();
     __syncthreads();
     tcgen05_fence_after_sync();

@@ -56,40 +56,65 @@ struct DevArray {
 //   runs[MAXRUNS]       x-segment runs to stage for the slab that the CTA
 //                       consumes STAGES slabs later (issue record)
 //   rbdir[nrb + 1]      per row block: byte offset of its block, plane count
-//   row-block blocks    one per row block, "row-sliced planes":
+//   row-block blocks    one per row block, "row-sliced planes".
+//   FP64 layouts:
 //     rowlen[16]  (u8)  entries of each of the 16 rows
-//     pinfo (48 B)      (mixed layouts only, W <= 32) u64 storage precision
-//                       of each plane (2 bits per plane), int8 exponent k
-//                       of each plane's storage scale 2^k (32 B), the plane
-//                       counts of the four class groups (u8 x 4: FP64,
-//                       FP32, FP16, FP8) and a fast flag (u8: every FP16
-//                       class plane stored as FP16, every FP8 one as FP8)
 //     idx[W][16]        u16 x-window position (staged) or u32 column
 //                       (gather) of entry k of row r, with the flag
-//                       TILE_START (first entry of a new FP64 tile in this
-//                       row); padding entries index the stage's zero slot
-//                       (staged) or carry the PAD flag (gather)
-//     vals              plane k holds entry k of the 16 rows: FP64 16x8 B,
-//                       or in mixed layouts FP64/FP32/FP16/FP8 16xwidth B
-// FP64 layouts: entry k of row r is the k-th entry of the row in the
-// reference's order (tiles in ascending column, entries of the row inside a
-// tile in CSR order). Mixed layouts: the planes are grouped by entry class
-// (the tile's precision; a diagonal entry of an FP16 / FP8 tile is FP32) in
-// the order FP64, FP32, FP16, FP8, and plane j of a group holds the j-th
-// entry of that class of each row, in the reference's order.
+//                       TILE_START (first entry of a new tile in this row)
+//     vals[W][16]       FP64; plane k holds entry k of the 16 rows, in the
+//                       reference's order (tiles in ascending column,
+//                       entries of the row inside a tile in CSR order)
+//   Mixed layouts (W <= 32): the planes are grouped by entry class (the
+//   tile's precision; a diagonal entry of an FP16 / FP8 tile is FP32) in the
+//   order FP64, FP32, FP16, FP8; plane j of a group holds the j-th entry of
+//   that class of each row, in the reference's order.
+//     head (16 B)       u8 plane counts of the four groups, u8 flags
+//                       (RBF_*), 3 B pad, u64 storage precision of each
+//                       plane (2 bits per plane)
+//     sexp[W]           int8 exponent k of each plane's storage scale 2^k
+//                       (padded to 16 B)
+//     base[W]           (affine blocks in staged slabs only) u16 x-window
+//                       position of row 0's entry of each plane: entry k of
+//                       row r sits at base[k] + r, and no idx is stored
+//     idx[W][16]        (other blocks) as in FP64 layouts; TILE_START only
+//                       in FP64-class planes; padding entries index the
+//                       stage's zero slot (staged) or carry PAD (gather)
+//     vals              FP64/FP32/FP16/FP8 planes of 16 x width bytes
+// A row block is affine when it has 16 rows, no FP64-class entry, and in
+// every plane the column of row r's entry is (its row + a constant): its x
+// positions then follow from the plane's base in any staged slab (the
+// segments of those columns are consecutive, hence in consecutive slots).
 constexpr int STAGES = 4;
 constexpr int MAXRUNS = 24;
 constexpr int XSEG_MAX = 112;      // staged x segments per slab (14 KB of FP64 x)
-constexpr int XSEG_MAX32 = 224;    // the same 14 KB holding FP32 x
 // Byte offset, inside a stage's x window, of 16 zero bytes that no copy
 // writes. The padding entries of staged planes (plane k >= the row's length)
 // index it with value 0, so a loop over all W planes of a row block adds
 // 0 * 0 for them whatever x holds.
 constexpr uint32_t XZERO_OFF = XSEG_MAX * 128;
+// Layouts staging FP32 x (every tile below FP64) move XEXTRA32 bytes of each
+// stage from the slab area to the x window, when the slab area is large
+// enough: their slabs are small (FP16 values), and the slab count, not its
+// bytes, sets the ring's pace, so a wider x window (more row blocks per
+// slab) is what they need. The window then ends at the same zero slot.
+constexpr int XEXTRA32 = 6144;
+__host__ __device__ inline int x32_extra(int slab_area) { return slab_area >= 4 * XEXTRA32 ? XEXTRA32 : 0; }
+// Start of the x window in a stage, and the x-window position of the zero
+// slot (the index of padding entries), for a layout staging FP32 or FP64 x.
+__host__ __device__ inline int x_off_of(int slab_area, bool x32) {
+    return x32 ? slab_area - x32_extra(slab_area) : slab_area;
+}
+__host__ __device__ inline uint32_t zero_pos_of(int slab_area, bool x32) {
+    return x32 ? (XZERO_OFF + (uint32_t)x32_extra(slab_area)) / 4u : XZERO_OFF / 8u;
+}
+// Staged x segments per slab of an FP32-x layout (64-byte segments).
+__host__ __device__ inline int xseg_max32(int slab_area) { return (int)(XZERO_OFF + x32_extra(slab_area)) / 64; }
 constexpr int MAXW = 255;          // planes per row block (rowlen is u8)
 constexpr int MAXW_MIXED = 32;     // planes per row block in mixed layouts
 constexpr int SLAB_MAX_DEFAULT = 40960;
-constexpr int RB_PER_SLAB_MAX = 60;  // two per consumer half-warp
+constexpr int RB_PER_SLAB_MAX = 120;  // four per consumer half-warp (a tuner candidate)
+constexpr int RB_PER_SLAB_X32 = 60;   // default for layouts staging FP32 x
 constexpr int RB_PER_SLAB_X64 = 30;  // default for layouts staging FP64 x
 constexpr int ISSUE_REC = 16 + MAXRUNS * 8;
 constexpr uint32_t IDX16_START = 0x8000u, IDX16_POS = 0x3fffu;
@@ -133,14 +158,28 @@ __host__ __device__ inline uint32_t align8u(uint32_t v) { return (v + 7u) & ~7u;
 __host__ __device__ inline uint32_t slab_rbdir_off() { return align16u(SLAB_HDR + 8u * MAXRUNS); }
 __host__ __device__ inline uint32_t slab_blocks_off(int nrb) { return align16u(slab_rbdir_off() + 8u * (nrb + 1)); }
 
-// Offsets inside one row-block block.
-__host__ __device__ inline uint32_t rb_pinfo_off() { return 16u; }
-__host__ __device__ inline uint32_t rb_idx_off(int W, bool mixed) { return mixed ? 16u + 48u : 16u; }
-__host__ __device__ inline uint32_t rb_vals_off(int W, bool mixed, bool gather) {
-    return align16u(rb_idx_off(W, mixed) + (uint32_t)W * 16u * (gather ? 4u : 2u));
+// Offsets inside one FP64 row-block block.
+__host__ __device__ inline uint32_t rb_idx_off() { return 16u; }
+__host__ __device__ inline uint32_t rb_vals_off(int W, bool gather) {
+    return align16u(rb_idx_off() + (uint32_t)W * 16u * (gather ? 4u : 2u));
 }
-__host__ __device__ inline uint32_t rb_block_bytes(int W, bool mixed, bool gather, uint32_t valbytes) {
-    return align16u(rb_vals_off(W, mixed, gather) + valbytes);
+// Offsets inside one mixed row-block block (aff: stored affine, which needs
+// a staged slab).
+enum { RBF_FAST = 1, RBF_AFFINE = 2, RBF_UNSCALED = 4 };
+// RBF_FAST: every FP16-class plane stored as FP16 and every FP8-class one
+// as FP8; RBF_UNSCALED: besides, every such plane's scale is 1.
+__host__ __device__ inline uint32_t rbm_sexp_off() { return 16u; }
+__host__ __device__ inline uint32_t rbm_base_off(int W) { return 16u + align16u((uint32_t)W); }
+__host__ __device__ inline uint32_t rbm_idx_off(int W, bool aff) {
+    return rbm_base_off(W) + (aff ? align16u(2u * (uint32_t)W) : 0u);
+}
+__host__ __device__ inline uint32_t rbm_vals_off(int W, bool gather, bool aff) {
+    const bool a = aff && !gather;
+    return align16u(rbm_idx_off(W, a) + (a ? 0u : (uint32_t)W * 16u * (gather ? 4u : 2u)));
+}
+__host__ __device__ inline uint32_t rb_block_bytes(int W, bool mixed, bool gather, uint32_t valbytes,
+                                                   bool aff = false) {
+    return mixed ? align16u(rbm_vals_off(W, gather, aff) + valbytes) : align16u(rb_vals_off(W, gather) + valbytes);
 }
 __host__ __device__ inline uint32_t prec_width(int prec) {
     return prec == MF_PREC_FP64 ? 8u : prec == MF_PREC_FP32 ? 4u : prec == MF_PREC_FP16 ? 2u : 1u;
@@ -197,6 +236,11 @@ struct mf_tiles {
     // solver layouts
     mf::Layout L64;
     mf::Layout Lmix[MF_NLEVELS];
+    // BiCGSTAB's mixed layout, built on its first mixed solve when the
+    // levels hold FP16 / FP8 tiles: those tiles raised to FP32 (the
+    // replacement-window argument that makes compensated FP16 safe for CG
+    // does not carry over to BiCGSTAB, whose iterations then grow ~2x)
+    mf::Layout Lbicg;
     bool mixed_ready = false;
     int nlevels = 0;                        // mixed levels built
     double level_switch[MF_NLEVELS] = {0};  // relative residual to leave level l

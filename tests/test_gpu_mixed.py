@@ -24,9 +24,32 @@ def test_rule_layout_spmv_bitexact(mf, O):
         assert np.array_equal(yd.cpu().numpy(), o.mixed_spmv(p, x))
 
 
+def test_random_low_precisions_bitexact(mf, O):
+    """Every tile at a random precision below FP64 (FP32 / FP16 / FP8 class
+    groups in one row block) on matrices whose row blocks keep their tiles."""
+    import torch
+
+    for A in (mf.Matrix.poisson2d(80), mf.Matrix.varpoisson3d(20)):
+        n = A.n
+        rp, ci, v = A.csr()
+        t = mf.Tiles(A)
+        p = np.random.default_rng(3).integers(1, 4, t.info()["tilenum"]).astype(np.uint8)
+        t.set_precisions(p)
+        pe, _ = t.precisions()
+        assert np.array_equal(pe, p)
+        x = np.random.default_rng(4).standard_normal(n)
+        xd = torch.tensor(x, device="cuda")
+        yd = torch.zeros(n, dtype=torch.float64, device="cuda")
+        t.spmv_level_dev(0, xd.data_ptr(), yd.data_ptr())
+        assert np.array_equal(yd.cpu().numpy(), O.OracleTiles(n, n, rp, ci, v).mixed_spmv(p, x))
+
+
 def test_random_per_tile_precisions_bitexact(mf, O):
     """Planes whose entries come from tiles of different precisions / scales
-    are stored at a common width without changing any dequantized value."""
+    are stored at a common width without changing any dequantized value.
+    A row block whose class groups need more than 32 planes in all is
+    computed in FP64 from the tile arrays (its tiles report FP64), so the
+    oracle takes the precisions the layout reports."""
     import torch
 
     A = mf.Matrix.spd_random(8000, 6)
@@ -36,12 +59,16 @@ def test_random_per_tile_precisions_bitexact(mf, O):
     tn = t.info()["tilenum"]
     p = np.random.default_rng(1).integers(0, 4, tn).astype(np.uint8)
     t.set_precisions(p)
+    pe, _ = t.precisions()
+    assert np.all((pe == p) | (pe == 0)) and np.mean(pe == p) > 0.5
     o = O.OracleTiles(n, n, rp, ci, v)
     x = np.random.default_rng(2).standard_normal(n)
     xd = torch.tensor(x, device="cuda")
     yd = torch.zeros(n, dtype=torch.float64, device="cuda")
     t.spmv_level_dev(0, xd.data_ptr(), yd.data_ptr())
-    assert np.array_equal(yd.cpu().numpy(), o.mixed_spmv(p, x))
+    y, yo = yd.cpu().numpy(), o.mixed_spmv(pe, x)
+    bad = np.flatnonzero(y != yo)
+    assert bad.size == 0, (bad[:8], y[bad[:4]], yo[bad[:4]])
 
 
 @pytest.mark.parametrize("N", [24, 48])
@@ -68,12 +95,13 @@ def test_mixed_cg_full_size_varpoisson_128(mf):
     assert np.linalg.norm(xm - xs) / np.linalg.norm(xs) < 1e-4
 
 
-@pytest.mark.parametrize("maker,growth", [("convdiff3d_24", 1.3), ("varpoisson3d_24", 1.6)])
+@pytest.mark.parametrize("maker,growth", [("convdiff3d_24", 1.3), ("varpoisson3d_24", 1.7)])
 def test_mixed_bicgstab_reaches_fp64_tolerance(mf, maker, growth):
     """BiCGSTAB on the low-precision layouts (FP64 vectors, dots and periodic
     true-residual replacement) reaches the FP64 true residual. On the
     contrast-1e6 Poisson (scaled condition ~1e8 at 24^3) the FP32 operator
-    costs BiCGSTAB about 1.5x the FP64 iterations, CG only a few percent."""
+    costs BiCGSTAB about 1.6x the FP64 iterations, CG only a few percent.
+    BiCGSTAB runs FP32 tiles where the CG levels hold FP16 ones."""
     kind, size = maker.rsplit("_", 1)
     A = mf.Matrix.convdiff3d(int(size)) if kind == "convdiff3d" else mf.Matrix.varpoisson3d(int(size))
     b = A.b()
