@@ -91,9 +91,7 @@ int encode_dev_impl(int n, int ncols, int nnz, const int *rp, const int *ci, con
     int rc;
     MF_CUDA_TRY(cudaSetDevice(t->opt.device));
     t->device = t->opt.device;
-    cudaDeviceProp prop;
-    MF_CUDA_TRY(cudaGetDeviceProperties(&prop, t->device));
-    t->nsm = prop.multiProcessorCount;
+    MF_CUDA_TRY(cudaDeviceGetAttribute(&t->nsm, cudaDevAttrMultiProcessorCount, t->device));
     if ((rc = kernel_config(t, &t->G)) != MF_OK) { delete t; return rc; }
     if (G_force > 0) t->G = G_force;
     cudaStream_t s = 0;

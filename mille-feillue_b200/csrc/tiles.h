@@ -21,10 +21,31 @@
 
 namespace mf {
 
+// Device buffers come from the current device's stream-ordered memory pool,
+// kept warm (its release threshold is raised once per device): a handle
+// encoded, solved and freed again and again reuses the same memory instead
+// of mapping and unmapping hundreds of MB per call. Each allocation is made
+// usable by every stream before it returns, and each free first waits for
+// the device, as a plain cudaFree would, because the batched and multi-RHS
+// solvers run on streams of their own.
+inline bool pool_ready(int dev) {
+    static bool ready[64] = {};
+    if (dev < 0 || dev >= 64) return false;
+    if (!ready[dev]) {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return false;
+        uint64_t keep = UINT64_MAX;
+        if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) return false;
+        ready[dev] = true;
+    }
+    return true;
+}
+
 template <class T>
 struct DevArray {
     T *p = nullptr;
     size_t n = 0;
+    bool pooled = false;
     DevArray() = default;
     DevArray(const DevArray &) = delete;
     DevArray &operator=(const DevArray &) = delete;
@@ -32,9 +53,15 @@ struct DevArray {
     int alloc(size_t count) {
         release();
         if (count == 0) count = 1;
-        if (cudaMalloc((void **)&p, count * sizeof(T)) != cudaSuccess) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        pooled = pool_ready(dev);
+        const cudaError_t e = pooled ? cudaMallocAsync((void **)&p, count * sizeof(T), 0)
+                                     : cudaMalloc((void **)&p, count * sizeof(T));
+        if (e != cudaSuccess || (pooled && cudaStreamSynchronize(0) != cudaSuccess)) {
+            if (e == cudaSuccess) release();
             p = nullptr;
-            set_last_error("cudaMalloc failed");
+            set_last_error("device allocation failed");
             return MF_ERR_NOMEM;
         }
         n = count;
@@ -42,9 +69,17 @@ struct DevArray {
     }
     int zero(cudaStream_t s = 0) { return cudaMemsetAsync(p, 0, n * sizeof(T), s) == cudaSuccess ? MF_OK : MF_ERR_CUDA; }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            if (pooled) {
+                cudaDeviceSynchronize();
+                cudaFreeAsync(p, 0);
+            } else {
+                cudaFree(p);
+            }
+        }
         p = nullptr;
         n = 0;
+        pooled = false;
     }
 };
 
