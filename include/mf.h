@@ -271,6 +271,14 @@ int mf_solve_bicgstab_dev(mf_tiles *t, const double *b_dev, double *x_dev,
 int mf_solve_cg_dev_noalloc(mf_tiles *t, const double *b_dev, double *x_dev,
                             double tol, int maxiter, const mf_options *opt,
                             mf_result *res);
+/* Self-check of the slab planner (no counterpart in the reference; the
+ * reference's two-pointer split, Mille-feuille_CG_NVIDIA.cu:4216-4484, is
+ * host code). Layouts are planned on the GPU; while the check is on (on = 1;
+ * on = -1 only reads the counters), every layout built is planned again by
+ * the host planner and each plan, segment and run is compared. Returns the
+ * previous setting; *checked = layouts compared, *mismatches = differences
+ * found since the check was last switched. Process-wide, not thread-safe. */
+int mf_check_planner(int on, long long *checked, long long *mismatches);
 /* Phase timestamps (ns, %globaltimer of CTA 0) of the last traced CG solve:
  * out[8*i + s] for iteration i, slot s = 0 iteration start, 1 halo ready,
  * 2 SpMV done, 3 alpha known, 4 r updated, 5 beta known, 6 x / d published.

@@ -125,6 +125,7 @@ EXPORTED = [
     "mf_solve_cg_dev_noalloc", "mf_mlp_set_weights", "mf_mlp_get_weights", "mf_tiles_features",
     "mf_tiles_select_mlp", "mf_mlp_forward_dev", "mf_mlp_grad_dev", "mf_mlp_train_dev", "mf_solve_pcg",
     "mf_solve_pcg_dev", "mf_memory_report", "mf_tiles_autotune", "mf_solve_cg_multi", "mf_solve_cg_multi_dev",
+    "mf_check_planner",
 ]
 MLP_WEIGHTS = 4868
 MLP_WEIGHTS_PATH = os.path.join(_HERE, "mlp_weights.bin")
@@ -180,6 +181,8 @@ def lib():
               "mf_solve_cg_dev_noalloc"):
         getattr(L, f).argtypes = [_p, _p, _p, _d, _i, C.POINTER(MfOptions), C.POINTER(MfResult)]
     L.mf_true_residual.argtypes = [_p, _p, _p, C.POINTER(_d)]
+    L.mf_check_planner.argtypes = [_i, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+    L.mf_check_planner.restype = _i
     L.mf_memory_report.argtypes = [_p, C.POINTER(MfMemoryReport)]
     L.mf_tiles_autotune.argtypes = [_p, _i, C.POINTER(MfTuneResult)]
     L.mf_solve_cg_multi.argtypes = [C.POINTER(MfCsr), _i, _p, _p, _d, _i, _p, _p, C.POINTER(_d)]
@@ -359,6 +362,14 @@ class Matrix:
                 self.h = None
         except Exception:
             pass
+
+
+def check_planner(on=None):
+    """Switches the GPU slab planner's self-check (every layout built is also
+    planned on the host and compared) and returns (checked, mismatches)."""
+    c, m = C.c_longlong(), C.c_longlong()
+    lib().mf_check_planner(-1 if on is None else int(bool(on)), C.byref(c), C.byref(m))
+    return c.value, m.value
 
 
 def batch_sizes(count=512, lo=1000, hi=200000, seed=2):

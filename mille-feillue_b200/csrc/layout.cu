@@ -469,7 +469,461 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_slabs(const SlabPlan *__r
     }
 }
 
+
+// ---- GPU slab planner ---------------------------------------------------------
+// Plans every CTA's slabs on the device with the same greedy rules as the
+// host planner (check_plans): one warp per CTA range. The lanes first copy
+// the range's row-block data and tile columns into shared memory (when they
+// fit; else they are read from global memory), then walk the row blocks
+// together: a row block's tile columns enter the slab's x-segment set (a
+// linear-probing hash set in shared memory) 32 at a time, a row block that
+// does not fit is taken out again as a whole (removals are always of the
+// latest inserts, so emptying their slots keeps the set consistent), and the
+// warp sorts each staged slab's segments to form its runs. The plans, segments and runs go
+// to CTA-local scratch (at most one slab per row block, one segment and one
+// run per tile), with per-CTA counts; k_plan_compact then places them.
+struct PlanArgs {
+    const int *tile_ptr, *tile_col, *cta_rb, *rbW;
+    const unsigned *rbvb;
+    const uint8_t *rbaff;
+    int tilen, mixed, xseg_max, slab_lim, rbps, maxw;
+};
+struct PlanCounts {  // per CTA
+    int nslabs, nsegs, nruns, ngather, nover, pad;
+    unsigned long long bytes;
+    int cmin, cmax;  // smallest / largest tile column of the range (-1 when it has no tiles)
+};
+struct PlanScratch {  // CTA g: plans from cta_rb[g], segments and runs from tile_ptr[cta_rb[g]]
+    SlabPlan *plans;  // off16 holds the CTA-local byte offset; seg_off / run_off are CTA-local
+    int *segs;
+    XRun *runs;
+    uint8_t *over_rb;
+};
+
+constexpr int PLAN_HASH = 1024;    // > 2 * (the largest x window in segments + 1)
+constexpr int PLAN_MEM = 512;      // members kept: fewer than xseg_max + 33 (a batch of 32 past it at most)
+constexpr int PLAN_PRE_RB = 2048;  // row blocks of a CTA range prefetched into shared memory
+constexpr int PLAN_PRE_T = 6144;   // tile columns prefetched
+constexpr size_t PLAN_DYN_SMEM = (size_t)(PLAN_PRE_RB + 1) * 4 + (size_t)PLAN_PRE_RB * 9 + (size_t)PLAN_PRE_T * 4;
+
+__global__ void __launch_bounds__(32) k_plan(PlanArgs A, PlanCounts *cnt, PlanScratch O) {
+    extern __shared__ __align__(16) uint8_t pdyn[];
+    __shared__ int hkey[PLAN_HASH];
+    __shared__ int mem[PLAN_MEM], mslot[PLAN_MEM], sorted[PLAN_MEM];
+    const unsigned full = 0xffffffffu;
+    const int g = blockIdx.x, lane = threadIdx.x;
+    for (int i = lane; i < PLAN_HASH; i += 32) hkey[i] = -1;
+    const int lo = A.cta_rb[g], hi = A.cta_rb[g + 1];
+    const int t0 = A.tile_ptr[lo], t1 = A.tile_ptr[hi];
+    // the range's data in shared memory when it fits
+    const bool pre_rb = hi - lo <= PLAN_PRE_RB, pre_t = t1 - t0 <= PLAN_PRE_T;
+    int *s_tp = reinterpret_cast<int *>(pdyn);
+    int *s_w = s_tp + PLAN_PRE_RB + 1;
+    unsigned *s_vb = reinterpret_cast<unsigned *>(s_w + PLAN_PRE_RB);
+    int *s_tc = reinterpret_cast<int *>(s_vb + PLAN_PRE_RB);
+    uint8_t *s_aff = reinterpret_cast<uint8_t *>(s_tc + PLAN_PRE_T);
+    if (pre_rb) {
+        for (int i = lane; i <= hi - lo; i += 32) s_tp[i] = A.tile_ptr[lo + i];
+        for (int i = lane; i < hi - lo; i += 32) {
+            s_w[i] = A.rbW[lo + i];
+            s_vb[i] = A.rbvb[lo + i];
+            s_aff[i] = A.rbaff[lo + i];
+        }
+    }
+    if (pre_t)
+        for (int i = lane; i < t1 - t0; i += 32) s_tc[i] = A.tile_col[t0 + i];
+    __syncwarp();
+    auto TP = [&](int rb) { return pre_rb ? s_tp[rb - lo] : A.tile_ptr[rb]; };
+    auto TC = [&](int k) { return pre_t ? s_tc[k - t0] : A.tile_col[k]; };
+    auto RW = [&](int rb) { return pre_rb ? s_w[rb - lo] : A.rbW[rb]; };
+    const bool mixed = A.mixed != 0;
+    auto rb_bytes = [&](int rb, bool gather) {
+        const unsigned vb = pre_rb ? s_vb[rb - lo] : A.rbvb[rb];
+        const bool af = (pre_rb ? s_aff[rb - lo] : A.rbaff[rb]) != 0;
+        return rb_block_bytes(RW(rb), mixed, gather, vb, af);
+    };
+    auto find = [&](int key) -> bool {
+        if (key < 0 || key >= A.tilen) return false;
+        for (uint32_t h = ((uint32_t)key * 2654435761u) & (PLAN_HASH - 1);; h = (h + 1) & (PLAN_HASH - 1)) {
+            const int v = hkey[h];
+            if (v == key) return true;
+            if (v < 0) return false;
+        }
+    };
+    // The slab's segment set: n members (mem[0..n), in batches) and its run
+    // count, both uniform across the warp. add_rb adds a row block's tile
+    // columns 32 at a time: with S the members before the batch and N its new
+    // keys, runs grows by sum over N of 1 - [k-1 in S or N] - [k+1 in S].
+    // Past xseg_max members the set stops growing (the slab cannot be staged:
+    // only that fact is used, as by the host planner).
+    int n = 0, runs = 0;
+    auto add_rb = [&](int rb) {
+        const int k0 = TP(rb), k1 = TP(rb + 1);
+        for (int base = k0; base < k1 && n <= A.xseg_max; base += 32) {
+            const int k = base + lane;
+            const bool has = k < k1;
+            const int key = has ? TC(k) : -1;
+            const bool isnew = has && !find(key);
+            const bool left_s = isnew && find(key - 1), right_s = isnew && find(key + 1);
+            const int nk = isnew ? key : -2;
+            bool left_n = false;
+            for (int j = 0; j < 32; ++j) left_n |= __shfl_sync(full, nk, j) == key - 1 && isnew;
+            const int d = isnew ? 1 - ((left_s || left_n) ? 1 : 0) - (right_s ? 1 : 0) : 0;
+            const unsigned bal = __ballot_sync(full, isnew);
+            if (isnew) {
+                uint32_t h = ((uint32_t)key * 2654435761u) & (PLAN_HASH - 1);
+                while (atomicCAS(&hkey[h], -1, key) != -1) h = (h + 1) & (PLAN_HASH - 1);
+                const int pos = n + __popc(bal & ((1u << lane) - 1u));
+                mem[pos] = key;
+                mslot[pos] = (int)h;
+            }
+            int dsum = d;
+            for (int o = 16; o > 0; o >>= 1) dsum += __shfl_xor_sync(full, dsum, o);
+            n += __popc(bal);
+            runs += dsum;
+            __syncwarp();
+        }
+    };
+    auto clear_to = [&](int n0) {  // removes the members past n0 (whole batches)
+        for (int i = n0 + lane; i < n; i += 32) hkey[mslot[i]] = -1;
+        __syncwarp();
+        n = n0;
+    };
+    SlabPlan *plans = O.plans + lo;
+    int *segs = O.segs + t0;
+    XRun *rout = O.runs + t0;
+    int slab = 0, segpos = 0, runpos = 0, ngather = 0, nover = 0;
+    unsigned long long bytepos = 0;
+    int rb = lo;
+    while (rb < hi) {
+        const int rb0 = rb;
+        int nrb = 1, mode;
+        const int ntiles0 = TP(rb + 1) - TP(rb);
+        int ntiles = ntiles0;
+        uint32_t bytes;
+        add_rb(rb);
+        const bool staged0 = n <= A.xseg_max && runs <= MAXRUNS;
+        const uint32_t tot0 = slab_blocks_off(1) + rb_bytes(rb, !staged0);
+        bool staged = false;
+        if (tot0 > (uint32_t)A.slab_lim || RW(rb) > A.maxw) {
+            mode = SLAB_OVERSIZE;
+            bytes = slab_blocks_off(0);
+            ++nover;
+            if (lane == 0) O.over_rb[rb] = 1;
+        } else {
+            staged = staged0;
+            mode = staged ? SLAB_STAGED : SLAB_GATHER;
+            uint32_t body = rb_bytes(rb, !staged);
+            int nx = rb + 1;
+            while (nx < hi && nrb < A.rbps) {
+                if (RW(nx) > A.maxw) break;
+                const uint32_t bx = rb_bytes(nx, !staged);
+                if (slab_blocks_off(nrb + 1) + body + bx > (uint32_t)A.slab_lim) break;
+                if (staged) {
+                    const int n0 = n, r0 = runs;
+                    add_rb(nx);
+                    if (n > A.xseg_max || runs > MAXRUNS) {
+                        clear_to(n0);
+                        runs = r0;
+                        break;
+                    }
+                }
+                nrb += 1;
+                ntiles += TP(nx + 1) - TP(nx);
+                body += bx;
+                ++nx;
+            }
+            bytes = slab_blocks_off(nrb) + body;
+            if (!staged) ++ngather;
+        }
+        // ---- staged slabs: sort the segments (bitonic), write them and their runs
+        int nseg = 0, nruns = 0;
+        if (staged) {
+            int m = 1;
+            while (m < n) m <<= 1;
+            for (int i = lane; i < m; i += 32) sorted[i] = i < n ? mem[i] : 0x7fffffff;
+            __syncwarp();
+            for (int k = 2; k <= m; k <<= 1)
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    for (int i = lane; i < m; i += 32) {
+                        const int l = i ^ j;
+                        if (l > i) {
+                            const int a = sorted[i], b = sorted[l];
+                            if ((a > b) == ((i & k) == 0)) {
+                                sorted[i] = b;
+                                sorted[l] = a;
+                            }
+                        }
+                    }
+                    __syncwarp();
+                }
+            nseg = n;
+            for (int i = lane; i < n; i += 32) segs[segpos + i] = sorted[i];
+            if (lane == 0) {
+                for (int i = 0; i < n; ++i) {
+                    if (i == 0 || sorted[i] != sorted[i - 1] + 1) rout[runpos + nruns++] = XRun{sorted[i], 0, (uint16_t)i};
+                    rout[runpos + nruns - 1].nseg++;
+                }
+            }
+            nruns = __shfl_sync(full, nruns, 0);
+        }
+        if (lane == 0) {
+            SlabPlan P;
+            P.rb0 = rb0;
+            P.nrb = nrb;
+            P.ntiles = ntiles;
+            P.mode = mode;
+            P.bytes = bytes;
+            P.off16 = (uint32_t)bytepos;  // CTA-local byte offset until compaction
+            P.seg_off = staged ? segpos : 0;
+            P.nseg = nseg;
+            P.run_off = staged ? runpos : 0;
+            P.nruns = nruns;
+            plans[slab] = P;
+        }
+        bytepos += bytes;
+        rb = rb0 + nrb;
+        clear_to(0);
+        runs = 0;
+        segpos += nseg;
+        runpos += nruns;
+        ++slab;
+    }
+    // the range's smallest / largest tile column (its x dependencies)
+    int cmin = 0x7fffffff, cmax = -1;
+    for (int k = t0 + lane; k < t1; k += 32) {
+        const int c = TC(k);
+        cmin = min(cmin, c);
+        cmax = max(cmax, c);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        cmin = min(cmin, __shfl_xor_sync(full, cmin, o));
+        cmax = max(cmax, __shfl_xor_sync(full, cmax, o));
+    }
+    if (lane == 0) {
+        PlanCounts c;
+        c.nslabs = slab;
+        c.nsegs = segpos;
+        c.nruns = runpos;
+        c.ngather = ngather;
+        c.nover = nover;
+        c.pad = 0;
+        c.bytes = bytepos;
+        c.cmin = cmax < 0 ? -1 : cmin;
+        c.cmax = cmax;
+        cnt[g] = c;
+    }
+}
+
+// Layout tallies over the tiles, one thread per row block: tiles per
+// precision, algorithmic bytes (integers, so the sum is exact and
+// deterministic), and whether a row block outside the oversize ones holds an
+// FP64 tile. out: [0..3] tile counts, [4] bytes, [5] any FP64 tile.
+__global__ void k_layout_tally(const int *tile_ptr, const int *tile_off, const uint8_t *prec, const uint8_t *over_rb,
+                               const unsigned *rbprom, int tilem, int mixed, unsigned long long *out) {
+    const int rb = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long c[4] = {0, 0, 0, 0}, bytes = 0, any64 = 0;
+    if (rb < tilem) {
+        const bool ov = over_rb[rb] != 0;
+        for (int k = tile_ptr[rb]; k < tile_ptr[rb + 1]; ++k) {
+            const int p = prec[k];
+            const unsigned long long nnz = (unsigned long long)(tile_off[k + 1] - tile_off[k]);
+            ++c[p];
+            bytes += nnz * (prec_width(p) + 1u) + 8u + (p == MF_PREC_FP8 ? 4u : 0u);
+            if (!ov && p == MF_PREC_FP64) any64 = 1;
+        }
+        if (mixed && !ov) bytes += rbprom[rb];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        for (int q = 0; q < 4; ++q) c[q] += __shfl_xor_sync(0xffffffffu, c[q], o);
+        bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+        any64 |= __shfl_xor_sync(0xffffffffu, any64, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        for (int q = 0; q < 4; ++q)
+            if (c[q]) atomicAdd(&out[q], c[q]);
+        if (bytes) atomicAdd(&out[4], bytes);
+        if (any64) atomicOr(&out[5], 1ull);
+    }
+}
+
+// Places CTA g's plans, segments and runs at the offsets of the counts'
+// prefix sums (slab_base, seg_base, run_base, byte_base per CTA).
+__global__ void k_plan_compact(const int *cta_rb, const int *tile_ptr, const PlanCounts *cnt, PlanScratch S,
+                               const int *slab_base, const int *seg_base, const int *run_base,
+                               const unsigned long long *byte_base, SlabPlan *plans, int *segs, XRun *runs,
+                               int *slab_cta) {
+    const int g = blockIdx.x;
+    const int lo = cta_rb[g], t0 = tile_ptr[lo];
+    const PlanCounts c = cnt[g];
+    for (int i = threadIdx.x; i < c.nslabs; i += blockDim.x) {
+        SlabPlan P = S.plans[lo + i];
+        P.off16 = (uint32_t)((byte_base[g] + P.off16) / 16);
+        if (P.mode == SLAB_STAGED) {
+            P.seg_off += seg_base[g];
+            P.run_off += run_base[g];
+        }
+        plans[slab_base[g] + i] = P;
+        slab_cta[slab_base[g] + i] = g;
+    }
+    for (int i = threadIdx.x; i < c.nsegs; i += blockDim.x) segs[seg_base[g] + i] = S.segs[t0 + i];
+    for (int i = threadIdx.x; i < c.nruns; i += blockDim.x) runs[run_base[g] + i] = S.runs[t0 + i];
+}
+
+// Issue records of the first STAGES slabs of every CTA (one thread per record).
+__global__ void k_heads(const SlabPlan *__restrict__ plans, const XRun *__restrict__ runs, const int *cta_slab,
+                        int G, uint32_t segbytes, uint8_t *head) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= G * STAGES) return;
+    const int g = q / STAGES, k = q % STAGES;
+    uint32_t *rec = reinterpret_cast<uint32_t *>(head + (size_t)q * ISSUE_REC);
+    for (int i = 0; i < ISSUE_REC / 4; ++i) rec[i] = 0;
+    const int s = cta_slab[g] + k;
+    if (s >= cta_slab[g + 1]) return;
+    const SlabPlan P = plans[s];
+    rec[0] = P.off16;
+    rec[1] = P.bytes;
+    rec[2] = P.mode == SLAB_STAGED ? (uint32_t)P.nseg * segbytes : 0u;
+    rec[3] = P.mode == SLAB_STAGED ? (uint32_t)P.nruns : 0u;
+    if (P.mode == SLAB_STAGED) {
+        XRun *dst = reinterpret_cast<XRun *>(rec + 4);
+        for (int i = 0; i < P.nruns; ++i) dst[i] = runs[P.run_off + i];
+    }
+}
+
 }  // namespace
+
+// ---- planner check ------------------------------------------------------------
+// The host planner (the reference for the GPU planner k_plan): the same
+// greedy rules, one CTA range after another. Used only when the planner
+// check is on, to compare every plan, segment and run with the GPU's.
+static bool g_planner_check = false;
+static long long g_planner_checked = 0, g_planner_mismatch = 0;
+bool planner_check_on() { return g_planner_check; }
+
+int check_plans(mf_tiles *t, int G, const std::vector<int> &cta_rb, const std::vector<int> &rbW,
+                const std::vector<unsigned> &rbvb, const std::vector<uint8_t> &rbaff, bool mixed, bool x32,
+                int xseg_max, int slab_lim, int rbps, int maxw, const std::vector<int> &cta_slab_gpu, int ns,
+                int nsegs, int nruns, const DevArray<SlabPlan> &d_plans, const DevArray<int> &d_slab_cta,
+                const DevArray<int> &d_segs, const DevArray<XRun> &d_runs, cudaStream_t st) {
+    const auto &tp = t->h_tile_ptr;
+    const auto &tc = t->h_tile_col;
+    auto rb_bytes = [&](int rb, bool gather) {
+        return rb_block_bytes(rbW[rb], mixed, gather, rbvb[rb], rbaff[rb] != 0);
+    };
+    std::vector<SlabPlan> plans;
+    std::vector<int> segs, slab_cta, cta_slab(G + 1, 0);
+    std::vector<XRun> runs;
+    std::vector<uint8_t> inseg((size_t)t->tilen + 2, 0);
+    std::vector<int> members, cur;
+    int seg_runs = 0;
+    auto seg_add = [&](int s) {
+        if (inseg[s + 1]) return;
+        inseg[s + 1] = 1;
+        members.push_back(s);
+        seg_runs += 1 - inseg[s] - inseg[s + 2];
+    };
+    auto seg_drop_to = [&](size_t n) {
+        while (members.size() > n) {
+            const int s = members.back();
+            members.pop_back();
+            inseg[s + 1] = 0;
+            seg_runs -= 1 - inseg[s] - inseg[s + 2];
+        }
+    };
+    uint64_t off = 0;
+    for (int g = 0; g < G; ++g) {
+        cta_slab[g] = (int)plans.size();
+        int rb = cta_rb[g];
+        while (rb < cta_rb[g + 1]) {
+            SlabPlan P;
+            std::memset(&P, 0, sizeof P);
+            P.rb0 = rb;
+            for (int k = tp[rb]; k < tp[rb + 1]; ++k) seg_add(tc[k]);
+            const bool staged0 = (int)members.size() <= xseg_max && seg_runs <= MAXRUNS;
+            const uint32_t tot0 = slab_blocks_off(1) + rb_bytes(rb, !staged0);
+            if (tot0 > (uint32_t)slab_lim || rbW[rb] > maxw) {
+                P.mode = SLAB_OVERSIZE;
+                P.nrb = 1;
+                P.ntiles = tp[rb + 1] - tp[rb];
+                P.bytes = slab_blocks_off(0);
+                rb += 1;
+            } else {
+                const bool staged = staged0;
+                P.mode = staged ? SLAB_STAGED : SLAB_GATHER;
+                P.nrb = 1;
+                P.ntiles = tp[rb + 1] - tp[rb];
+                uint32_t body = rb_bytes(rb, !staged);
+                int nx = rb + 1;
+                while (nx < cta_rb[g + 1] && P.nrb < rbps) {
+                    if (rbW[nx] > maxw) break;
+                    const uint32_t bx = rb_bytes(nx, !staged);
+                    if (slab_blocks_off(P.nrb + 1) + body + bx > (uint32_t)slab_lim) break;
+                    if (staged) {
+                        const size_t n0 = members.size();
+                        for (int k = tp[nx]; k < tp[nx + 1]; ++k) seg_add(tc[k]);
+                        if ((int)members.size() > xseg_max || seg_runs > MAXRUNS) {
+                            seg_drop_to(n0);
+                            break;
+                        }
+                    }
+                    P.nrb += 1;
+                    P.ntiles += tp[nx + 1] - tp[nx];
+                    body += bx;
+                    ++nx;
+                }
+                P.bytes = slab_blocks_off(P.nrb) + body;
+                rb = nx;
+            }
+            if (P.mode == SLAB_STAGED) {
+                cur.assign(members.begin(), members.end());
+                std::sort(cur.begin(), cur.end());
+                P.seg_off = (int)segs.size();
+                P.nseg = (int)cur.size();
+                segs.insert(segs.end(), cur.begin(), cur.end());
+                P.run_off = (int)runs.size();
+                for (size_t i = 0; i < cur.size(); ++i) {
+                    if (i == 0 || cur[i] != cur[i - 1] + 1) runs.push_back(XRun{cur[i], 0, (uint16_t)i});
+                    runs.back().nseg++;
+                }
+                P.nruns = (int)runs.size() - P.run_off;
+            }
+            P.off16 = (uint32_t)(off / 16);
+            off += P.bytes;
+            seg_drop_to(0);
+            plans.push_back(P);
+            slab_cta.push_back(g);
+        }
+    }
+    cta_slab[G] = (int)plans.size();
+    long long bad = 0;
+    if ((int)plans.size() != ns || (int)segs.size() != nsegs || (int)runs.size() != nruns || cta_slab != cta_slab_gpu) {
+        bad = 1;
+    } else {
+        std::vector<SlabPlan> gp(ns);
+        std::vector<int> gs(nsegs), gsc(ns);
+        std::vector<XRun> gr(nruns);
+        if (ns) MF_CUDA_TRY(cudaMemcpyAsync(gp.data(), d_plans.p, sizeof(SlabPlan) * ns, cudaMemcpyDeviceToHost, st));
+        if (ns) MF_CUDA_TRY(cudaMemcpyAsync(gsc.data(), d_slab_cta.p, sizeof(int) * ns, cudaMemcpyDeviceToHost, st));
+        if (nsegs) MF_CUDA_TRY(cudaMemcpyAsync(gs.data(), d_segs.p, sizeof(int) * nsegs, cudaMemcpyDeviceToHost, st));
+        if (nruns) MF_CUDA_TRY(cudaMemcpyAsync(gr.data(), d_runs.p, sizeof(XRun) * nruns, cudaMemcpyDeviceToHost, st));
+        MF_CUDA_TRY(cudaStreamSynchronize(st));
+        for (int i = 0; i < ns; ++i) {
+            const SlabPlan &a = plans[i], &b = gp[i];
+            if (a.rb0 != b.rb0 || a.nrb != b.nrb || a.ntiles != b.ntiles || a.mode != b.mode || a.bytes != b.bytes ||
+                a.off16 != b.off16 || a.nseg != b.nseg || a.nruns != b.nruns ||
+                (a.mode == SLAB_STAGED && (a.seg_off != b.seg_off || a.run_off != b.run_off)))
+                ++bad;
+        }
+        if (gsc != slab_cta || gs != segs) ++bad;
+        for (int i = 0; i < nruns; ++i)
+            if (gr[i].seg0 != runs[i].seg0 || gr[i].nseg != runs[i].nseg || gr[i].slot0 != runs[i].slot0) ++bad;
+    }
+    (void)x32;
+    ++g_planner_checked;
+    g_planner_mismatch += bad;
+    return MF_OK;
+}
 
 int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cudaStream_t st) {
     auto t_start = std::chrono::steady_clock::now();
@@ -479,8 +933,6 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
     const int slab_area = (slab_max + 127) & ~127;  // the solver kernels' slab area (solver.h)
     int slab_lim = slab_max;                         // largest slab of this layout
     const auto &tp = t->h_tile_ptr;
-    const auto &tc = t->h_tile_col;
-    const auto &tn = t->h_tile_nnz;
     std::vector<uint8_t> prec(prec_in);
     if ((int)prec.size() != tilenum) prec.assign(tilenum, MF_PREC_FP64);
     bool mixed = false;
@@ -507,11 +959,10 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
     k_rb_info<<<(tilem + 7) / 8, 256, 0, st>>>(A, mixed, d_rbW.p, d_rbvb.p, d_rbprom.p, d_rbaff.p);
     MF_CUDA_TRY(cudaGetLastError());
     std::vector<int> rbW(tilem);
-    std::vector<unsigned> rbvb(tilem), rbprom(tilem);
+    std::vector<unsigned> rbvb(tilem);
     std::vector<uint8_t> rbaff(tilem);
     MF_CUDA_TRY(cudaMemcpyAsync(rbW.data(), d_rbW.p, sizeof(int) * tilem, cudaMemcpyDeviceToHost, st));
     MF_CUDA_TRY(cudaMemcpyAsync(rbvb.data(), d_rbvb.p, sizeof(unsigned) * tilem, cudaMemcpyDeviceToHost, st));
-    MF_CUDA_TRY(cudaMemcpyAsync(rbprom.data(), d_rbprom.p, sizeof(unsigned) * tilem, cudaMemcpyDeviceToHost, st));
     MF_CUDA_TRY(cudaMemcpyAsync(rbaff.data(), d_rbaff.p, tilem, cudaMemcpyDeviceToHost, st));
     MF_CUDA_TRY(cudaStreamSynchronize(st));
 
@@ -542,200 +993,115 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
     // layout is planned again with FP64 x.
     bool x32 = mixed;
     for (size_t k = 0; k < prec.size() && x32; ++k) x32 = prec[k] != MF_PREC_FP64;
-    // slabs: the CTAs' row-block ranges are planned independently (on up to
-    // 16 host threads for large matrices) and concatenated in CTA order
-    std::vector<SlabPlan> plans;
-    std::vector<int> seg_all;
-    std::vector<XRun> run_all;
-    std::vector<int> slab_cta;
-    std::vector<int> cta_slab(G + 1, 0);
-    struct Part {  // one thread's CTAs
-        std::vector<SlabPlan> plans;
-        std::vector<int> segs, nslab;
-        std::vector<XRun> runs;
-        int n_gather = 0, n_over = 0;
-    };
+    // slabs: planned on the GPU (k_plan into CTA-local scratch, counts,
+    // k_plan_compact). With the planner check on (mf_check_planner), the host
+    // planner plans the same layout and every plan, segment and run is
+    // compared.
     int n_gather = 0, n_over = 0, xseg_max = XSEG_MAX, rbps = RB_PER_SLAB_X64;
     uint32_t segbytes = 128u;
-    auto plan_ctas = [&](int g0, int g1, Part &out) {
-        // x segments (tile columns) of the slab being planned, kept
-        // incrementally since a row block adds only a few: membership (offset
-        // by one so that s - 1 and s + 1 are always addressable), the members
-        // in insertion order, and the number of runs of consecutive segments
-        std::vector<uint8_t> inseg((size_t)t->tilen + 2, 0);
-        std::vector<int> members, cur;
-        int seg_runs = 0;
-        auto seg_add = [&](int s) {
-            if (inseg[s + 1]) return;
-            inseg[s + 1] = 1;
-            members.push_back(s);
-            seg_runs += 1 - inseg[s] - inseg[s + 2];
-        };
-        auto seg_drop_to = [&](size_t n) {  // undo the adds past the first n, newest first
-            while (members.size() > n) {
-                const int s = members.back();
-                members.pop_back();
-                inseg[s + 1] = 0;
-                seg_runs -= 1 - inseg[s] - inseg[s + 2];
-            }
-        };
-        for (int g = g0; g < g1; ++g) {
-            const size_t first = out.plans.size();
-            int rb = cta_rb[g];
-            while (rb < cta_rb[g + 1]) {
-                SlabPlan P{};
-                P.rb0 = rb;
-                for (int k = tp[rb]; k < tp[rb + 1]; ++k) seg_add(tc[k]);
-                const bool staged0 = (int)members.size() <= xseg_max && seg_runs <= MAXRUNS;
-                const uint32_t tot0 = slab_blocks_off(1) + rb_bytes(rb, !staged0);
-                if (tot0 > (uint32_t)slab_lim || rbW[rb] > maxw) {
-                    P.mode = SLAB_OVERSIZE;
-                    P.nrb = 1;
-                    P.ntiles = tp[rb + 1] - tp[rb];
-                    P.bytes = slab_blocks_off(0);
-                    for (int k = tp[rb]; k < tp[rb + 1]; ++k) prec[k] = MF_PREC_FP64;  // this CTA's tiles only
-                    ++out.n_over;
-                    rb += 1;
-                } else {
-                    const bool staged = staged0;
-                    P.mode = staged ? SLAB_STAGED : SLAB_GATHER;
-                    P.nrb = 1;
-                    P.ntiles = tp[rb + 1] - tp[rb];
-                    uint32_t body = rb_bytes(rb, !staged);
-                    int nx = rb + 1;
-                    while (nx < cta_rb[g + 1] && P.nrb < rbps) {
-                        if (rbW[nx] > maxw) break;
-                        const uint32_t bx = rb_bytes(nx, !staged);
-                        if (slab_blocks_off(P.nrb + 1) + body + bx > (uint32_t)slab_lim) break;
-                        if (staged) {
-                            const size_t n0 = members.size();
-                            for (int k = tp[nx]; k < tp[nx + 1]; ++k) seg_add(tc[k]);
-                            if ((int)members.size() > xseg_max || seg_runs > MAXRUNS) {
-                                seg_drop_to(n0);
-                                break;
-                            }
-                        }
-                        P.nrb += 1;
-                        P.ntiles += tp[nx + 1] - tp[nx];
-                        body += bx;
-                        ++nx;
-                    }
-                    P.bytes = slab_blocks_off(P.nrb) + body;
-                    if (!staged) ++out.n_gather;
-                    rb = nx;
-                }
-                if (P.mode == SLAB_STAGED) {
-                    cur.assign(members.begin(), members.end());
-                    std::sort(cur.begin(), cur.end());
-                    P.seg_off = (int)out.segs.size();  // within this part; offset at the merge
-                    P.nseg = (int)cur.size();
-                    out.segs.insert(out.segs.end(), cur.begin(), cur.end());
-                    P.run_off = (int)out.runs.size();
-                    for (size_t i = 0; i < cur.size(); ++i) {
-                        if (i == 0 || cur[i] != cur[i - 1] + 1) out.runs.push_back(XRun{cur[i], 0, (uint16_t)i});
-                        out.runs.back().nseg++;
-                    }
-                    P.nruns = (int)out.runs.size() - P.run_off;
-                }
-                seg_drop_to(0);
-                out.plans.push_back(P);
-            }
-            out.nslab.push_back((int)(out.plans.size() - first));
-        }
-    };
+    DevArray<int> d_cta_rb, d_sb, d_gb, d_rbase;
+    DevArray<unsigned long long> d_bb;
+    DevArray<PlanCounts> d_cnt;
+    DevArray<SlabPlan> d_plans, sc_plans;
+    DevArray<int> d_slab_cta, d_segs, sc_segs;
+    DevArray<XRun> d_runs, sc_runs;
+    DevArray<uint8_t> d_over;
+    if (d_cta_rb.alloc(G + 1) || d_cnt.alloc(G) || d_sb.alloc(G) || d_gb.alloc(G) || d_rbase.alloc(G) ||
+        d_bb.alloc(G) || d_over.alloc(tilem) || sc_plans.alloc(tilem) || sc_segs.alloc(tilenum) ||
+        sc_runs.alloc(tilenum))
+        return MF_ERR_NOMEM;
+    MF_CUDA_TRY(cudaMemcpyAsync(d_cta_rb.p, cta_rb.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice, st));
+    static bool plan_smem_set = false;
+    if (!plan_smem_set) {
+        MF_CUDA_TRY(cudaFuncSetAttribute(k_plan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PLAN_DYN_SMEM));
+        plan_smem_set = true;
+    }
+    std::vector<int> cta_slab(G + 1, 0);
+    std::vector<PlanCounts> hcnt;
+    uint64_t off = 0;
+    int ns = 0, nsegs = 0, nruns = 0;
     for (;;) {
         xseg_max = x32 ? xseg_max32(slab_area) : XSEG_MAX;
-        slab_lim = x32 ? x_off_of(slab_area, true) : slab_max;
         segbytes = x32 ? 64u : 128u;
         rbps = t->opt.rb_per_slab > 0 ? std::min(t->opt.rb_per_slab, RB_PER_SLAB_MAX)
                                       : (x32 ? RB_PER_SLAB_X32 : RB_PER_SLAB_X64);
-        const unsigned hw = std::thread::hardware_concurrency();
-        const int nth = tilem >= 16384 ? std::max(1, std::min({16, (int)(hw ? hw : 1), G})) : 1;
-        std::vector<Part> parts(nth);
-        if (nth == 1) {
-            plan_ctas(0, G, parts[0]);
-        } else {
-            std::vector<std::thread> th;
-            for (int i = 0; i < nth; ++i)
-                th.emplace_back(plan_ctas, (int)((long long)G * i / nth), (int)((long long)G * (i + 1) / nth),
-                                std::ref(parts[i]));
-            for (auto &x : th) x.join();
-        }
-        plans.clear();
-        seg_all.clear();
-        run_all.clear();
-        slab_cta.clear();
-        cta_slab.assign(G + 1, 0);
+        slab_lim = x32 ? x_off_of(slab_area, true) : slab_max;
+        const PlanArgs pa{t->tile_ptr.p, t->tile_col.p, d_cta_rb.p, d_rbW.p, d_rbvb.p, d_rbaff.p, t->tilen,
+                          mixed ? 1 : 0, xseg_max, slab_lim, rbps, maxw};
+        MF_CUDA_TRY(cudaMemsetAsync(d_over.p, 0, tilem, st));
+        k_plan<<<G, 32, PLAN_DYN_SMEM, st>>>(pa, d_cnt.p, PlanScratch{sc_plans.p, sc_segs.p, sc_runs.p, d_over.p});
+        MF_CUDA_TRY(cudaGetLastError());
+        hcnt.assign(G, PlanCounts{});
+        std::vector<PlanCounts> &hc = hcnt;
+        MF_CUDA_TRY(cudaMemcpyAsync(hc.data(), d_cnt.p, sizeof(PlanCounts) * G, cudaMemcpyDeviceToHost, st));
+        MF_CUDA_TRY(cudaStreamSynchronize(st));
+        std::vector<int> sb(G), gb(G), rbase(G);
+        std::vector<unsigned long long> bb(G);
+        ns = nsegs = nruns = 0;
+        off = 0;
         n_gather = n_over = 0;
-        int g = 0;
-        for (auto &pt : parts) {
-            const int soff = (int)seg_all.size(), roff = (int)run_all.size();
-            size_t k = 0;
-            for (int cnt : pt.nslab) {
-                cta_slab[g] = (int)plans.size();
-                for (int j = 0; j < cnt; ++j, ++k) {
-                    SlabPlan P = pt.plans[k];
-                    if (P.mode == SLAB_STAGED) {
-                        P.seg_off += soff;
-                        P.run_off += roff;
-                    }
-                    plans.push_back(P);
-                    slab_cta.push_back(g);
-                }
-                ++g;
-            }
-            seg_all.insert(seg_all.end(), pt.segs.begin(), pt.segs.end());
-            run_all.insert(run_all.end(), pt.runs.begin(), pt.runs.end());
-            n_gather += pt.n_gather;
-            n_over += pt.n_over;
+        for (int g = 0; g < G; ++g) {
+            cta_slab[g] = sb[g] = ns;
+            gb[g] = nsegs;
+            rbase[g] = nruns;
+            bb[g] = off;
+            ns += hc[g].nslabs;
+            nsegs += hc[g].nsegs;
+            nruns += hc[g].nruns;
+            off += hc[g].bytes;
+            n_gather += hc[g].ngather;
+            n_over += hc[g].nover;
         }
-        cta_slab[G] = (int)plans.size();
-        if (x32 && n_over > 0) {
+        cta_slab[G] = ns;
+        if (x32 && n_over > 0) {  // planned again with FP64 x
             x32 = false;
-            prec = prec_in;
-            if ((int)prec.size() != tilenum) prec.assign(tilenum, MF_PREC_FP64);
             continue;
         }
+        if (d_plans.alloc(ns) || d_slab_cta.alloc(ns) || d_segs.alloc(nsegs) || d_runs.alloc(nruns))
+            return MF_ERR_NOMEM;
+        MF_CUDA_TRY(cudaMemcpyAsync(d_sb.p, sb.data(), sizeof(int) * G, cudaMemcpyHostToDevice, st));
+        MF_CUDA_TRY(cudaMemcpyAsync(d_gb.p, gb.data(), sizeof(int) * G, cudaMemcpyHostToDevice, st));
+        MF_CUDA_TRY(cudaMemcpyAsync(d_rbase.p, rbase.data(), sizeof(int) * G, cudaMemcpyHostToDevice, st));
+        MF_CUDA_TRY(cudaMemcpyAsync(d_bb.p, bb.data(), sizeof(unsigned long long) * G, cudaMemcpyHostToDevice, st));
+        k_plan_compact<<<G, 128, 0, st>>>(d_cta_rb.p, t->tile_ptr.p, d_cnt.p,
+                                           PlanScratch{sc_plans.p, sc_segs.p, sc_runs.p, d_over.p}, d_sb.p, d_gb.p,
+                                           d_rbase.p, d_bb.p, d_plans.p, d_segs.p, d_runs.p, d_slab_cta.p);
+        MF_CUDA_TRY(cudaGetLastError());
         break;
-    }
-    const int ns = (int)plans.size();
-    uint64_t off = 0;
-    for (auto &P : plans) {
-        P.off16 = (uint32_t)(off / 16);
-        off += P.bytes;
     }
     if (off / 16 > 0xffffffffull) {
         set_last_error("slab layout exceeds 64 GiB");
         return MF_ERR_UNSUPPORTED;
     }
     // oversize row blocks are computed in FP64 from the tile arrays
-    if (n_over > 0 && tilenum > 0) {
-        MF_CUDA_TRY(cudaMemcpyAsync(L.prec_dev.p, prec.data(), tilenum, cudaMemcpyHostToDevice, st));
-        k_tile_scales<<<(tilenum + 7) / 8, 256, 0, st>>>(tilenum, t->tile_off.p, t->val.p, L.prec_dev.p,
-                                                        L.scale_dev.p);
+    std::vector<uint8_t> over(tilem, 0);
+    if (n_over > 0) {
+        MF_CUDA_TRY(cudaMemcpyAsync(over.data(), d_over.p, tilem, cudaMemcpyDeviceToHost, st));
+        MF_CUDA_TRY(cudaStreamSynchronize(st));
+        for (int rb = 0; rb < tilem; ++rb)
+            if (over[rb])
+                for (int k = tp[rb]; k < tp[rb + 1]; ++k) prec[k] = MF_PREC_FP64;
+        if (tilenum > 0) {
+            MF_CUDA_TRY(cudaMemcpyAsync(L.prec_dev.p, prec.data(), tilenum, cudaMemcpyHostToDevice, st));
+            k_tile_scales<<<(tilenum + 7) / 8, 256, 0, st>>>(tilenum, t->tile_off.p, t->val.p, L.prec_dev.p,
+                                                            L.scale_dev.p);
+        }
+    }
+    if (planner_check_on()) {
+        const int rc = check_plans(t, G, cta_rb, rbW, rbvb, rbaff, mixed, x32, xseg_max, slab_lim, rbps, maxw,
+                                   cta_slab, ns, nsegs, nruns, d_plans, d_slab_cta, d_segs, d_runs, st);
+        if (rc) return rc;
     }
     // issue records of the first STAGES slabs of every CTA
-    std::vector<uint8_t> head((size_t)G * STAGES * ISSUE_REC, 0);
-    for (int g = 0; g < G; ++g)
-        for (int k = 0; k < STAGES; ++k) {
-            const int s = cta_slab[g] + k;
-            uint32_t *rec = reinterpret_cast<uint32_t *>(&head[((size_t)g * STAGES + k) * ISSUE_REC]);
-            if (s >= cta_slab[g + 1]) continue;
-            const SlabPlan &P = plans[s];
-            rec[0] = P.off16;
-            rec[1] = P.bytes;
-            rec[2] = P.mode == SLAB_STAGED ? (uint32_t)P.nseg * segbytes : 0u;
-            rec[3] = P.mode == SLAB_STAGED ? (uint32_t)P.nruns : 0u;
-            if (P.mode == SLAB_STAGED) std::memcpy(&rec[4], &run_all[P.run_off], sizeof(XRun) * P.nruns);
-        }
-    // dependency ranges: CTAs owning the x segments a CTA reads
+    if (L.head.alloc((size_t)G * STAGES * ISSUE_REC) || L.cta_slab.alloc(G + 1)) return MF_ERR_NOMEM;
+    MF_CUDA_TRY(cudaMemcpyAsync(L.cta_slab.p, cta_slab.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice, st));
+    k_heads<<<(G * STAGES + 127) / 128, 128, 0, st>>>(d_plans.p, d_runs.p, L.cta_slab.p, G, segbytes, L.head.p);
+    MF_CUDA_TRY(cudaGetLastError());
+    // dependency ranges: CTAs owning the x segments a CTA reads (each
+    // range's smallest / largest tile column comes with the plan counts)
     std::vector<int> dep(2 * G);
     for (int g = 0; g < G; ++g) {
-        int cmin = INT32_MAX, cmax = -1;
-        for (int k = tp[cta_rb[g]]; k < tp[cta_rb[g + 1]]; ++k) {
-            cmin = std::min(cmin, tc[k]);
-            cmax = std::max(cmax, tc[k]);
-        }
+        int cmin = hcnt[g].cmin, cmax = hcnt[g].cmax;
         if (cmax < 0) {
             dep[2 * g] = g;
             dep[2 * g + 1] = g - 1;  // empty range
@@ -749,53 +1115,33 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
         dep[2 * g] = owner(cmin);
         dep[2 * g + 1] = owner(cmax);
     }
-    // layout kind (oversize row blocks run in FP64 from the tile arrays and
-    // do not count)
+    // tiles per precision, algorithmic bytes and the layout kind (oversize
+    // row blocks run in FP64 from the tile arrays and do not count)
+    DevArray<unsigned long long> d_tally;
+    if (d_tally.alloc(6)) return MF_ERR_NOMEM;
+    MF_CUDA_TRY(cudaMemsetAsync(d_tally.p, 0, sizeof(unsigned long long) * 6, st));
+    if (tilem > 0)
+        k_layout_tally<<<(tilem + 255) / 256, 256, 0, st>>>(t->tile_ptr.p, t->tile_off.p, L.prec_dev.p, d_over.p,
+                                                            d_rbprom.p, tilem, mixed ? 1 : 0, d_tally.p);
+    MF_CUDA_TRY(cudaGetLastError());
+    unsigned long long tally[6];
+    MF_CUDA_TRY(cudaMemcpyAsync(tally, d_tally.p, sizeof tally, cudaMemcpyDeviceToHost, st));
+    MF_CUDA_TRY(cudaStreamSynchronize(st));
     int kind = LAYOUT_FP64;
     if (mixed) {
-        bool any64 = false;
-        for (const auto &P : plans)
-            if (P.mode != SLAB_OVERSIZE)
-                for (int k = tp[P.rb0]; k < tp[P.rb0 + P.nrb] && !any64; ++k) any64 = prec[k] == MF_PREC_FP64;
-        kind = any64 ? LAYOUT_ANY : LAYOUT_LOW;
+        kind = tally[5] ? LAYOUT_ANY : LAYOUT_LOW;
         // the LOW row path reads FP32 x: a layout planned with FP64 x (after
         // an oversize row block) takes the general path, which rounds x per
         // entry to the same FP32 value
         if (kind == LAYOUT_LOW && !x32) kind = LAYOUT_ANY;
     }
-    // algorithmic bytes and precision fractions
-    double alg = 16.0 * (double)t->rowA;
-    double cnt[4] = {0, 0, 0, 0};
-    for (int k = 0; k < tilenum; ++k) {
-        alg += tile_alg_bytes(prec[k], tn[k]);
-        cnt[prec[k]] += 1;
-    }
-    // diagonal entries of FP16 / FP8 tiles are stored in FP32 (oversize row
-    // blocks hold FP64 tiles only)
-    if (mixed)
-        for (const auto &P : plans)
-            if (P.mode != SLAB_OVERSIZE)
-                for (int rb = P.rb0; rb < P.rb0 + P.nrb; ++rb) alg += (double)rbprom[rb];
-    // upload and fill
-    DevArray<SlabPlan> d_plans;
-    DevArray<int> d_slab_cta, d_segs;
-    DevArray<XRun> d_runs;
-    if (L.slabs.alloc(off + 16) || L.head.alloc(head.size()) || L.cta_slab.alloc(G + 1) ||
-        L.cta_rb.alloc(G + 1) || L.cta_dep.alloc(2 * G) || d_plans.alloc(ns) || d_slab_cta.alloc(ns) ||
-        d_segs.alloc(seg_all.size()) || d_runs.alloc(run_all.size()))
-        return MF_ERR_NOMEM;
-    MF_CUDA_TRY(cudaMemcpyAsync(L.head.p, head.data(), head.size(), cudaMemcpyHostToDevice, st));
-    MF_CUDA_TRY(cudaMemcpyAsync(L.cta_slab.p, cta_slab.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice, st));
+    const double alg = 16.0 * (double)t->rowA + (double)tally[4];
+    double cnt[4];
+    for (int q = 0; q < 4; ++q) cnt[q] = (double)tally[q];
+    // fill
+    if (L.slabs.alloc(off + 16) || L.cta_rb.alloc(G + 1) || L.cta_dep.alloc(2 * G)) return MF_ERR_NOMEM;
     MF_CUDA_TRY(cudaMemcpyAsync(L.cta_rb.p, cta_rb.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice, st));
     MF_CUDA_TRY(cudaMemcpyAsync(L.cta_dep.p, dep.data(), sizeof(int) * 2 * G, cudaMemcpyHostToDevice, st));
-    if (ns > 0) {
-        MF_CUDA_TRY(cudaMemcpyAsync(d_plans.p, plans.data(), sizeof(SlabPlan) * ns, cudaMemcpyHostToDevice, st));
-        MF_CUDA_TRY(cudaMemcpyAsync(d_slab_cta.p, slab_cta.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, st));
-    }
-    if (!seg_all.empty())
-        MF_CUDA_TRY(cudaMemcpyAsync(d_segs.p, seg_all.data(), sizeof(int) * seg_all.size(), cudaMemcpyHostToDevice, st));
-    if (!run_all.empty())
-        MF_CUDA_TRY(cudaMemcpyAsync(d_runs.p, run_all.data(), sizeof(XRun) * run_all.size(), cudaMemcpyHostToDevice, st));
     if (ns > 0)
         k_fill_slabs<<<ns, FILL_THREADS, 0, st>>>(d_plans.p, d_slab_cta.p, L.cta_slab.p, d_segs.p, d_runs.p, A,
                                                  d_rbW.p, d_rbvb.p, d_rbaff.p, mixed, segbytes,
@@ -821,3 +1167,14 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
 }
 
 }  // namespace mf
+
+extern "C" int mf_check_planner(int on, long long *checked, long long *mismatches) {
+    const int prev = mf::g_planner_check ? 1 : 0;
+    if (on >= 0) {
+        mf::g_planner_check = on != 0;
+        mf::g_planner_checked = mf::g_planner_mismatch = 0;
+    }
+    if (checked) *checked = mf::g_planner_checked;
+    if (mismatches) *mismatches = mf::g_planner_mismatch;
+    return prev;
+}

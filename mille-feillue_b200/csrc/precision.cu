@@ -112,17 +112,26 @@ int matrix_features(const mf_tiles *t, float *lognnz, float *logrange, cudaStrea
     return MF_OK;
 }
 
-int tile_features(mf_tiles *t, std::vector<float> &feat, cudaStream_t s) {
+// Features f0..f5 of every tile, on the device (f5 = 0).
+int tile_features_dev(mf_tiles *t, DevArray<float> &d, cudaStream_t s) {
     const int tn = t->tilenum;
-    feat.assign((size_t)tn * 6, 0.0f);
+    if (d.alloc((size_t)(tn > 0 ? tn : 1) * 6)) return MF_ERR_NOMEM;
     if (tn == 0) return MF_OK;
-    DevArray<float> d;
-    if (d.alloc((size_t)tn * 6)) return MF_ERR_NOMEM;
     TileFeatArgs A = tile_feat_args(t);
     int rc = matrix_features(t, &A.lognnz, &A.logrange, s);
     if (rc) return rc;
     k_tile_features<<<(tn + 7) / 8, 256, 0, s>>>(A, d.p);
     MF_CUDA_TRY(cudaGetLastError());
+    return MF_OK;
+}
+
+int tile_features(mf_tiles *t, std::vector<float> &feat, cudaStream_t s) {
+    const int tn = t->tilenum;
+    feat.assign((size_t)tn * 6, 0.0f);
+    if (tn == 0) return MF_OK;
+    DevArray<float> d;
+    int rc = tile_features_dev(t, d, s);
+    if (rc) return rc;
     MF_CUDA_TRY(cudaMemcpyAsync(feat.data(), d.p, sizeof(float) * feat.size(), cudaMemcpyDeviceToHost, s));
     MF_CUDA_TRY(cudaStreamSynchronize(s));
     return MF_OK;
@@ -173,16 +182,12 @@ __global__ void k_rb_zrows(TileFeatArgs A, uint8_t *zflag) {
 }
 }  // namespace
 
-// Per row block: all rows diagonally dominant Z-rows (host copy).
-int rb_zrows(const mf_tiles *t, std::vector<uint8_t> &z, cudaStream_t s) {
-    z.assign(t->tilem, 0);
+// Per row block: all rows diagonally dominant Z-rows (device flags).
+int rb_zrows_dev(const mf_tiles *t, DevArray<uint8_t> &d, cudaStream_t s) {
+    if (d.alloc(t->tilem > 0 ? t->tilem : 1)) return MF_ERR_NOMEM;
     if (t->tilem == 0) return MF_OK;
-    DevArray<uint8_t> d;
-    if (d.alloc(t->tilem)) return MF_ERR_NOMEM;
     k_rb_zrows<<<(t->tilem + 7) / 8, 256, 0, s>>>(tile_feat_args(t), d.p);
     MF_CUDA_TRY(cudaGetLastError());
-    MF_CUDA_TRY(cudaMemcpyAsync(z.data(), d.p, t->tilem, cudaMemcpyDeviceToHost, s));
-    MF_CUDA_TRY(cudaStreamSynchronize(s));
     return MF_OK;
 }
 
@@ -234,7 +239,7 @@ RuleThresholds rule_thresholds(double tau) {
     return r;
 }
 
-uint8_t rule_precision_fast(const float *f, const RuleThresholds &r) {
+__host__ __device__ uint8_t rule_precision_fast(const float *f, const RuleThresholds &r) {
     const float f0 = f[0], f1 = f[1];
     const bool diag = f[3] > 0.5f;
     if (!diag && f0 <= r.mag[MF_PREC_FP8] && f1 <= r.range8) return MF_PREC_FP8;
@@ -243,6 +248,29 @@ uint8_t rule_precision_fast(const float *f, const RuleThresholds &r) {
     return MF_PREC_FP64;
 }
 
+
+// The rule for every tile at one level (one thread per row block):
+// compensated row blocks (zrb) take the lowest precision allowed by
+// kCompTau within its range (comp8 / comp16 / comp32 say which are), the
+// others the magnitude rule with thresholds thr.
+__global__ void k_rule(const int *tile_ptr, const float *feat, const uint8_t *zrb, RuleThresholds thr,
+                       RuleThresholds any, int comp8, int comp16, int comp32, int tilem, uint8_t *prec) {
+    const int rb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (rb >= tilem) return;
+    for (int k = tile_ptr[rb]; k < tile_ptr[rb + 1]; ++k) {
+        const float *f = feat + (size_t)k * 6;
+        uint8_t p;
+        if (zrb[rb]) {
+            const float f1 = f[1];
+            p = (comp8 && f1 <= any.range8) ? MF_PREC_FP8
+                : (comp16 && f1 <= any.range16) ? MF_PREC_FP16
+                : comp32 ? MF_PREC_FP32 : rule_precision_fast(f, thr);
+        } else {
+            p = rule_precision_fast(f, thr);
+        }
+        prec[k] = p;
+    }
+}
 
 // Level tolerances of the magnitude rule and the relative true residual
 // below which the solver moves to the next level. The tolerance bounds the
@@ -299,11 +327,12 @@ int build_mixed_levels(mf_tiles *t, cudaStream_t s) {
         set_last_error("precision mode not available");
         return MF_ERR_UNSUPPORTED;
     }
-    std::vector<float> feat;
-    int rc = tile_features(t, feat, s);
+    DevArray<float> feat;
+    int rc = tile_features_dev(t, feat, s);
     if (rc) return rc;
-    std::vector<uint8_t> zrb;
-    if ((rc = rb_zrows(t, zrb, s))) return rc;
+    DevArray<uint8_t> zrb, dprec;
+    if ((rc = rb_zrows_dev(t, zrb, s))) return rc;
+    if (dprec.alloc(t->tilenum > 0 ? t->tilenum : 1)) return MF_ERR_NOMEM;
     const double scale = t->opt.mixed_tau > 0 ? t->opt.mixed_tau : 1.0;
     // compensated row blocks: the lowest precision with u_p <= kCompTau
     // (scaled like the level tolerances) whose range holds the tile
@@ -315,18 +344,13 @@ int build_mixed_levels(mf_tiles *t, cudaStream_t s) {
     for (int l = 0; l < MF_NLEVELS; ++l) {
         std::vector<uint8_t> p(t->tilenum);
         const RuleThresholds thr = rule_thresholds(kLevelTau[l] * scale);
-        for (int rb = 0; rb < t->tilem; ++rb)
-            for (int k = t->h_tile_ptr[rb]; k < t->h_tile_ptr[rb + 1]; ++k) {
-                const float *f = &feat[(size_t)k * 6];
-                if (zrb[rb]) {
-                    const float f1 = f[1];
-                    p[k] = (comp8 && f1 <= any.range8) ? MF_PREC_FP8
-                           : (comp16 && f1 <= any.range16) ? MF_PREC_FP16
-                           : comp32 ? MF_PREC_FP32 : rule_precision_fast(f, thr);
-                } else {
-                    p[k] = rule_precision_fast(f, thr);
-                }
-            }
+        if (t->tilem > 0)
+            k_rule<<<(t->tilem + 255) / 256, 256, 0, s>>>(t->tile_ptr.p, feat.p, zrb.p, thr, any, comp8 ? 1 : 0,
+                                                          comp16 ? 1 : 0, comp32 ? 1 : 0, t->tilem, dprec.p);
+        MF_CUDA_TRY(cudaGetLastError());
+        if (t->tilenum > 0)
+            MF_CUDA_TRY(cudaMemcpyAsync(p.data(), dprec.p, t->tilenum, cudaMemcpyDeviceToHost, s));
+        MF_CUDA_TRY(cudaStreamSynchronize(s));
         if (l > 0 && p == prev) break;  // identical to the previous level
         rc = build_layout(t, t->Lmix[l], p, s);
         if (rc) return rc;
