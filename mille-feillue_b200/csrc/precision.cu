@@ -8,8 +8,9 @@
 // the true residual falls (the solver switches at replacement points).
 //
 // Row blocks whose rows are all diagonally dominant Z-rows (one diagonal
-// entry a_ii > 0, every other entry <= 0) are stored with row-sum-preserving
-// compensation (layout.cu): there the rounding of an entry moves only an
+// entry a_ii > 0, every other entry <= 0, row sum >= 0 up to rounding) are
+// stored with row-sum-preserving compensation (layout.cu): there the
+// rounding of an entry moves only an
 // edge weight of the operator, by at most u_p relative, so its tiles take
 // the lowest precision with u_p <= kCompTau whatever their magnitude (FP16
 // within its range; the diagonal entries themselves stay FP32).
@@ -149,8 +150,11 @@ static const double kCompTau = 1e-3;
 
 namespace {
 // 1 for a row block whose rows are all diagonally dominant Z-rows: exactly
-// one diagonal entry, positive, and every other entry <= 0 (one warp per row
-// block, a lane per row).
+// one diagonal entry, positive, every other entry <= 0, and a row sum of at
+// least -1e-12 a_ii (zero up to the rounding of the sum: the compensated
+// operator keeps the row sums, and its perturbation is bounded relative to
+// the matrix only where they are non-negative). One warp per row block, a
+// lane per row.
 __global__ void k_rb_zrows(TileFeatArgs A, uint8_t *zflag) {
     const int lane = threadIdx.x & 31;
     const int rb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -161,21 +165,24 @@ __global__ void k_rb_zrows(TileFeatArgs A, uint8_t *zflag) {
         const int row = rb * 16 + lane;
         int nd = 0;
         bool z = true, pos = false;
+        double diag = 0.0, sum = 0.0;
         for (int t = A.tile_ptr[rb]; t < A.tile_ptr[rb + 1]; ++t) {
             const int vo = A.tile_off[t], nk = A.tile_off[t + 1] - vo;
             const int cc = A.csrptr_off[t];
             const int q0 = A.bptr[cc + lane], q1 = lane + 1 < rl ? (int)A.bptr[cc + lane + 1] : nk;
             for (int q = q0; q < q1; ++q) {
                 const double a = A.val[vo + q];
+                sum += a;
                 if (A.tile_col[t] * 16 + (int)A.col[vo + q] == row) {
                     ++nd;
                     pos = a > 0.0;
+                    diag = a;
                 } else if (!(a <= 0.0)) {
                     z = false;
                 }
             }
         }
-        ok = nd == 1 && z && pos;
+        ok = nd == 1 && z && pos && sum >= -1e-12 * diag;
     }
     ok = __all_sync(0xffffffffu, ok);
     if (lane == 0) zflag[rb] = ok ? 1 : 0;

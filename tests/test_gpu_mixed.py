@@ -131,3 +131,23 @@ def test_c3_mixed_layout_is_fp16_and_keeps_fp64_iterations(mf):
     assert np.linalg.norm(xm - x64) / np.linalg.norm(x64) < 1e-6
     # the layout moves fewer bytes than an all-FP32 one would (FP16 values)
     assert rm["spmv_bytes_level"][0] < 0.8 * 113.5e6
+
+
+def test_negative_row_sums_do_not_take_compensated_fp16(mf):
+    """Row-sum compensation bounds the FP16 perturbation relative to the
+    matrix only where the row sums are non-negative. A Z-matrix with negative
+    row sums (the 2D Laplacian shifted by -0.5 lambda_min, still SPD) keeps
+    the magnitude rule: no FP16 tiles. The unshifted Laplacian takes them."""
+    N = 64
+    A0 = mf.Matrix.poisson2d(N)
+    rp, ci, v = A0.csr()
+    rp, ci, v = np.asarray(rp), np.asarray(ci), np.asarray(v, dtype=np.float64).copy()
+    lam_min = 4.0 - 4.0 * np.cos(np.pi / (N + 1))  # smallest eigenvalue of the 5-point Laplacian
+    rows = np.repeat(np.arange(A0.n), np.diff(rp))
+    v[ci == rows] -= 0.5 * lam_min
+    A = mf.Matrix.from_csr(A0.n, A0.n, rp, ci, v)
+    for M, want16 in ((A0, True), (A, False)):
+        t = mf.Tiles(M, mf.options(precision_mode=mf.MODE_MIXED_RULE))
+        _, r = t.solve_cg(np.ones(M.n), tol=1e-10, maxiter=20000)
+        assert r["status"] == 0 and r["rel_residual_true"] <= 1e-10, r
+        assert (r["tile_frac"][2] > 0.5) == want16, (want16, r["tile_frac"])
