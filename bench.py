@@ -501,12 +501,14 @@ def cusparse_arm(args, rank, local):
             "cases": rows}
 
 
-def multi_rhs_arm(args, rank, local):
+def multi_rhs_arm(args, rank, local, fp64_panel=False):
     """CG on 16 right-hand sides at once (one shared panel product per
-    iteration) against 16 single-right-hand-side solves of the same columns
-    (the tensor-memory CG kernel), on the 128^3 variable-coefficient Poisson
-    matrix with 16 seeded U[-1, 1] right-hand sides; device time of each
-    solve to 1e-10."""
+    iteration; FP32 search directions and products, FP64 x, r, dots and
+    scalars, one persistent launch) against 16 single-right-hand-side FP64
+    solves of the same columns (the tensor-memory CG kernel), on the 128^3
+    variable-coefficient Poisson matrix with 16 seeded U[-1, 1] right-hand
+    sides; device time of each solve to a 1e-10 relative residual (the true
+    one for the panel solve). fp64_panel adds the exact FP64-panel path."""
     if rank != 0:
         return None
     import torch
@@ -522,20 +524,28 @@ def multi_rhs_arm(args, rank, local):
     x = torch.zeros(n, dtype=torch.float64, device=f"cuda:{local}")
     b0 = torch.tensor(np.ascontiguousarray(B[:, 0]), device=f"cuda:{local}")
     t.solve_cg_dev(b0.data_ptr(), x.data_ptr(), TOL, 50)  # warm
-    single_ms, single_it = 0.0, []
+    single_ms, single_it, xdiff = 0.0, [], 0.0
     for j in range(16):
         b = torch.tensor(np.ascontiguousarray(B[:, j]), device=f"cuda:{local}")
         x.zero_()
         r = t.solve_cg_dev(b.data_ptr(), x.data_ptr(), TOL, MAXITER)
         single_ms += r["time_ms"]
         single_it.append(int(r["iterations"]))
-    return {"metric": "16-RHS CG time to 1e-10 (shared panel product) vs 16 single-RHS solves",
-            "value": multi_ms, "unit": "ms", "n_gpus": 1, "higher_is_better": False, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": "varpoisson3d 128^3, 16 RHS U[-1,1] seed 7, x0 = 0, CG to 1e-10 per column"},
-            "iterations_min_max": [int(it.min()), int(it.max())], "max_rel_residual": float(rel.max()),
-            "single_rhs_total_ms": single_ms, "single_iterations_min_max": [min(single_it), max(single_it)],
-            "speedup_vs_single_rhs": single_ms / multi_ms}
+        xs = x.cpu().numpy()
+        xdiff = max(xdiff, float(np.linalg.norm(X[:, j] - xs) / np.linalg.norm(xs)))
+    out = {"metric": "16-RHS CG time to 1e-10 (shared panel product) vs 16 single-RHS solves",
+           "value": multi_ms, "unit": "ms", "n_gpus": 1, "higher_is_better": False,
+           "dtype": "FP32 search directions and panel products; FP64 x, r, dots, scalars",
+           "data": "synthetic",
+           "config": {"workload": "varpoisson3d 128^3, 16 RHS U[-1,1] seed 7, x0 = 0, CG to 1e-10 per column"},
+           "iterations_min_max": [int(it.min()), int(it.max())], "max_rel_residual": float(rel.max()),
+           "single_rhs_total_ms": single_ms, "single_iterations_min_max": [min(single_it), max(single_it)],
+           "max_x_diff_vs_single": xdiff, "speedup_vs_single_rhs": single_ms / multi_ms}
+    if fp64_panel:
+        _, it64, rel64, ms64 = mf.solve_cg_multi(A, B, tol=TOL, maxiter=MAXITER, panel=mf.PANEL_FP64)
+        out["fp64_panel"] = {"ms": ms64, "iterations_min_max": [int(it64.min()), int(it64.max())],
+                             "max_rel_residual": float(rel64.max()), "speedup_vs_single_rhs": single_ms / ms64}
+    return out
 
 
 def batch_arm(args, world, rank, local, dist, steps=None, warmup=None):
@@ -625,8 +635,9 @@ def _extra_legs(args, world, rank, local, dist, out):
     if rank == 0 and world == 1 and out is not None:
         try:
             m = multi_rhs_arm(args, rank, local)
-            out["multi16"] = {k: m[k] for k in ("value", "unit", "config", "iterations_min_max", "max_rel_residual",
-                                                "single_rhs_total_ms", "single_iterations_min_max",
+            out["multi16"] = {k: m[k] for k in ("value", "unit", "dtype", "config", "iterations_min_max",
+                                                "max_rel_residual", "single_rhs_total_ms",
+                                                "single_iterations_min_max", "max_x_diff_vs_single",
                                                 "speedup_vs_single_rhs")}
         except Exception as e:
             out["multi16"] = {"unavailable": f"{type(e).__name__}: {e}"}
@@ -643,7 +654,9 @@ def profile_case(args):
                 phase times of the first N CG iterations
       bicgstab  the same on the convection-diffusion matrix
       multi     CG on 16 right-hand sides (U[-1, 1], seed 0), `--iters`
-                iterations (panel product, scalar and update kernels)
+                iterations: the persistent FP32-panel kernel, or with
+                `--prec fp64` the FP64 panel's product, scalar and update
+                kernels
 
     Matrix: the 3D variable-coefficient Poisson (cg, pcg, spmv, multi) or
     convection-diffusion (bicgstab) of `--grid`. `--prec` picks the storage:
@@ -655,9 +668,10 @@ def profile_case(args):
     A = mf.Matrix.convdiff3d(args.grid) if args.kernel == "bicgstab" else mf.Matrix.varpoisson3d(args.grid)
     if args.kernel == "multi":
         B = np.random.default_rng(0).uniform(-1, 1, (A.n, 16))
-        X, it, rel, ms = mf.solve_cg_multi(A, B, tol=1e-30, maxiter=args.iters)
-        print("multi 16 rhs: %d iterations %.2f ms -> %.1f us/iteration"
-              % (int(it.max()), ms, ms * 1e3 / max(1, int(it.max()))))
+        panel = mf.PANEL_FP64 if args.prec == "fp64" else mf.PANEL_FP32
+        X, it, rel, ms = mf.solve_cg_multi(A, B, tol=1e-30, maxiter=args.iters, panel=panel)
+        print("multi 16 rhs (%s panel): %d iterations %.2f ms -> %.1f us/iteration"
+              % ("fp64" if panel == mf.PANEL_FP64 else "fp32", int(it.max()), ms, ms * 1e3 / max(1, int(it.max()))))
         return
     prec = args.prec or args.mode
     kw, level = {}, -1
@@ -758,7 +772,8 @@ def main():
             print(json.dumps(out))
         return
     if args.workload in ("vs_cusparse", "multi16"):
-        out = (cusparse_arm if args.workload == "vs_cusparse" else multi_rhs_arm)(args, rank, local)
+        out = (cusparse_arm(args, rank, local) if args.workload == "vs_cusparse"
+               else multi_rhs_arm(args, rank, local, fp64_panel=True))
         if out is not None:
             print(json.dumps(out))
         return

@@ -293,11 +293,11 @@ int mf_true_residual(mf_tiles *t, const double *b_dev, const double *x_dev,
  * test, the reference's CG) sharing every matrix-panel product, so the
  * matrix streams once per iteration for all of them. B, X: n x k column-major
  * (column j = right-hand side j; X holds x0 on entry). The SpMM keeps
- * blockspmv_cpu's order per column (FP64); the CSR columns must ascend within
- * each row. The _dev variant checks the CSR on the GPU before use (row_ptr[0]
+ * blockspmv_cpu's order per column; the CSR columns must ascend within each
+ * row. The _dev variant checks the CSR on the GPU before use (row_ptr[0]
  * == 0, row_ptr non-decreasing, columns in [0, n) and ascending) and returns
  * MF_ERR_ARG otherwise; it reads row_ptr[n] entries of col_idx_dev/val_dev.
- * Per right-hand side: iterations and recursive relative residual;
+ * Per right-hand side: iterations and final relative residual;
  * *time_ms = device time of the whole call. MF_ERR_NOT_CONVERGED if any
  * column missed tol within maxiter.                                          */
 int mf_solve_cg_multi(const mf_csr *A, int k, const double *B_host,
@@ -308,6 +308,25 @@ int mf_solve_cg_multi_dev(int n, const int *row_ptr_dev, const int *col_idx_dev,
                           double *X_dev, double tol, int maxiter,
                           int *iterations, double *rel_residual,
                           double *time_ms);
+/* Panel precision of the multi-right-hand-side CG. MF_PANEL_FP32 (what the
+ * two calls above use): search directions P and products Q = A P stored in
+ * FP32 (the product summed in FP64, then rounded), x, r, dots and scalars
+ * FP64, r replaced by b - A x every 50 iterations and whenever a column's
+ * recursive residual reaches tol; a column converges on that true residual
+ * (rel_residual is then the true one). One persistent launch per solve.
+ * MF_PANEL_FP64: every panel FP64; each column is exactly the single
+ * right-hand-side FP64 CG (recursive residual), five launches an iteration. */
+#define MF_PANEL_FP64 0
+#define MF_PANEL_FP32 1
+int mf_solve_cg_multi_ex(int panel, const mf_csr *A, int k,
+                         const double *B_host, double *X_host, double tol,
+                         int maxiter, int *iterations, double *rel_residual,
+                         double *time_ms);
+int mf_solve_cg_multi_dev_ex(int panel, int n, const int *row_ptr_dev,
+                             const int *col_idx_dev, const double *val_dev,
+                             int k, const double *B_dev, double *X_dev,
+                             double tol, int maxiter, int *iterations,
+                             double *rel_residual, double *time_ms);
 
 /* ---- autotuner (no reference counterpart) ------------------------------- */
 /* The tile shape is the reference's 16x16 (the bit-exact contract); what is

@@ -32,6 +32,8 @@ MF_ERR_IO = -6
 MF_ERR_NOMEM = -7
 MF_ERR_RESIDENCY = -8
 MF_ERR_UNSUPPORTED = -9
+PANEL_FP64 = 0  # multi-right-hand-side CG: every panel FP64 (each column the FP64 CG)
+PANEL_FP32 = 1  # FP32 search directions and products, one persistent launch (default)
 
 PREC_FP64, PREC_FP32, PREC_FP16, PREC_FP8 = 0, 1, 2, 3
 MODE_FP64, MODE_MIXED_RULE, MODE_MIXED_MLP, MODE_FIXED = 0, 1, 2, 3
@@ -125,7 +127,7 @@ EXPORTED = [
     "mf_solve_cg_dev_noalloc", "mf_mlp_set_weights", "mf_mlp_get_weights", "mf_tiles_features",
     "mf_tiles_select_mlp", "mf_mlp_forward_dev", "mf_mlp_grad_dev", "mf_mlp_train_dev", "mf_solve_pcg",
     "mf_solve_pcg_dev", "mf_memory_report", "mf_tiles_autotune", "mf_solve_cg_multi", "mf_solve_cg_multi_dev",
-    "mf_check_planner",
+    "mf_solve_cg_multi_ex", "mf_solve_cg_multi_dev_ex", "mf_check_planner",
 ]
 MLP_WEIGHTS = 4868
 MLP_WEIGHTS_PATH = os.path.join(_HERE, "mlp_weights.bin")
@@ -187,6 +189,8 @@ def lib():
     L.mf_tiles_autotune.argtypes = [_p, _i, C.POINTER(MfTuneResult)]
     L.mf_solve_cg_multi.argtypes = [C.POINTER(MfCsr), _i, _p, _p, _d, _i, _p, _p, C.POINTER(_d)]
     L.mf_solve_cg_multi_dev.argtypes = [_i, _p, _p, _p, _i, _p, _p, _d, _i, _p, _p, C.POINTER(_d)]
+    L.mf_solve_cg_multi_ex.argtypes = [_i, C.POINTER(MfCsr), _i, _p, _p, _d, _i, _p, _p, C.POINTER(_d)]
+    L.mf_solve_cg_multi_dev_ex.argtypes = [_i, _i, _p, _p, _p, _i, _p, _p, _d, _i, _p, _p, C.POINTER(_d)]
     L.mf_mlp_set_weights.argtypes = [_p]
     L.mf_mlp_get_weights.argtypes = [_p]
     L.mf_tiles_features.argtypes = [_p, _p]
@@ -225,17 +229,18 @@ def _ptr(a):
     return a.ctypes.data_as(_p)
 
 
-def solve_cg_multi(matrix, B, X0=None, tol=1e-10, maxiter=10000):
-    """CG on the k <= 16 columns of B (n x k) at once, sharing each SpMM.
-    Returns (X, iterations[k], rel_residual[k], device ms)."""
+def solve_cg_multi(matrix, B, X0=None, tol=1e-10, maxiter=10000, panel=PANEL_FP32):
+    """CG on the k <= 16 columns of B (n x k) at once, sharing each SpMM
+    (panel: PANEL_FP32 or PANEL_FP64). Returns (X, iterations[k],
+    rel_residual[k], device ms)."""
     B = np.asfortranarray(B, dtype=np.float64)
     n, k = B.shape
     X = np.asfortranarray(np.zeros((n, k)) if X0 is None else X0, dtype=np.float64)
     it = np.zeros(k, np.int32)
     rel = np.zeros(k)
     ms = _d()
-    rc = lib().mf_solve_cg_multi(C.byref(matrix.csr_struct()), k, _ptr(B), _ptr(X), tol, maxiter, _ptr(it),
-                                 _ptr(rel), C.byref(ms))
+    rc = lib().mf_solve_cg_multi_ex(panel, C.byref(matrix.csr_struct()), k, _ptr(B), _ptr(X), tol, maxiter,
+                                    _ptr(it), _ptr(rel), C.byref(ms))
     if rc not in (MF_OK, MF_ERR_NOT_CONVERGED):
         _check(rc, "mf_solve_cg_multi")
     return X, it, rel, ms.value

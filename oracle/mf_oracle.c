@@ -412,6 +412,56 @@ int mfo_cg(const mfo_tiles *t, const double *b, double *x, double tol, int maxit
     return it;
 }
 
+/* One column of the 16-right-hand-side CG with FP32 search directions
+ * (csrc/multi.cu, panel FP32): the reference recurrence
+ * (Mille-feuille_CG_NVIDIA.cu:722-804) with d stored in FP32 (d = fl32(r +
+ * beta d)) and q = fl32(A d) (the tiled SpMV in the reference's order on the
+ * FP32 values); x, r, the dots and the scalars stay FP64. After the r update,
+ * r is replaced by the true residual b - A x (FP64) every `replace`
+ * iterations and whenever the recursive residual reaches tol; convergence is
+ * decided on that true residual only. */
+int mfo_cg_dir32(const mfo_tiles *t, const double *b, double *x, double tol, int maxiter, int replace,
+                 double *rel_res) {
+    const int n = t->rowA;
+    double *r = (double *)malloc(sizeof(double) * (size_t)n);
+    double *d = (double *)malloc(sizeof(double) * (size_t)n);
+    double *q = (double *)malloc(sizeof(double) * (size_t)n);
+    mfo_blockspmv(t, x, q, NULL, NULL, NULL);
+    for (int i = 0; i < n; ++i) { r[i] = b[i] - q[i]; d[i] = (double)(float)r[i]; }
+    const double bb = mfo_dot(n, b, b);
+    double rr = mfo_dot(n, r, r);
+    double rel = bb > 0 ? sqrt(rr / bb) : sqrt(rr);
+    int it = 0;
+    while (it < maxiter && rel > tol) {
+        ++it;
+        mfo_blockspmv(t, d, q, NULL, NULL, NULL);
+        for (int i = 0; i < n; ++i) q[i] = (double)(float)q[i];
+        const double dq = mfo_dot(n, d, q);
+        if (!(dq > 0.0) || !isfinite(dq)) break; /* breakdown: not converged */
+        const double alpha = rr / dq;
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < n; ++i) { x[i] += alpha * d[i]; r[i] -= alpha * q[i]; }
+        double rrn = mfo_dot(n, r, r);
+        double relr = bb > 0 ? sqrt(rrn / bb) : sqrt(rrn);
+        if ((replace > 0 && it % replace == 0) || !(relr > tol)) {
+            mfo_blockspmv(t, x, q, NULL, NULL, NULL);
+            for (int i = 0; i < n; ++i) r[i] = b[i] - q[i];
+            rrn = mfo_dot(n, r, r);
+            relr = bb > 0 ? sqrt(rrn / bb) : sqrt(rrn);
+            rel = relr;
+            if (!(relr > tol)) { rr = rrn; break; }
+        }
+        rel = relr;
+        const double beta = rrn / rr;
+        rr = rrn;
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < n; ++i) d[i] = (double)(float)(r[i] + beta * d[i]);
+    }
+    if (rel_res) *rel_res = rel;
+    free(r); free(d); free(q);
+    return it;
+}
+
 /* Jacobi-preconditioned CG: KSPCG with PCJACOBI as in the "jpcg" runs of the
  * reference's PETSc comparison (PC/PETSc/src/ksp/ksp/impls/cg/cg.c:112-380,
  * unpreconditioned-norm stop test as test_a100.sh asks): z = r / a_ii,

@@ -66,6 +66,13 @@ double mfo_dot(int n, const double *a, const double *b);
 int mfo_cg(const mfo_tiles *t, const double *b, double *x, double tol, int maxiter,
            double *rel_res);
 
+/* One column of the FP32-direction multi-right-hand-side CG: d and q = A d
+ * rounded to FP32, x, r, dots and scalars FP64, r replaced by b - A x every
+ * `replace` iterations and when the recursive residual reaches tol (the stop
+ * test uses that true residual). */
+int mfo_cg_dir32(const mfo_tiles *t, const double *b, double *x, double tol, int maxiter, int replace,
+                 double *rel_res);
+
 /* Jacobi-preconditioned CG (KSPCG + PCJACOBI, PETSc/src/ksp/ksp/impls/cg/cg.c:112-380);
  * diag[i] = a_ii. Stops on the unpreconditioned ||r|| / ||b|| <= tol. */
 int mfo_pcg_jacobi(const mfo_tiles *t, const double *diag, const double *b, double *x, double tol,

@@ -57,6 +57,8 @@ def lib():
         L.mfo_dot.restype = C.c_double
         L.mfo_cg.argtypes = [C.POINTER(MfoTiles), _p, _p, C.c_double, _i, C.POINTER(C.c_double)]
         L.mfo_cg.restype = _i
+        L.mfo_cg_dir32.argtypes = [C.POINTER(MfoTiles), _p, _p, C.c_double, _i, _i, C.POINTER(C.c_double)]
+        L.mfo_cg_dir32.restype = _i
         L.mfo_pcg_jacobi.argtypes = [C.POINTER(MfoTiles), _p, _p, _p, C.c_double, _i, C.POINTER(C.c_double)]
         L.mfo_pcg_jacobi.restype = _i
         L.mfo_bicgstab.argtypes = [C.POINTER(MfoTiles), _p, _p, C.c_double, _i, C.POINTER(C.c_double)]
@@ -302,6 +304,14 @@ class OracleTiles:
         x = np.zeros(self.sizes["rowA"]) if x0 is None else np.array(x0, np.float64)
         rel = C.c_double()
         it = lib().mfo_cg(C.byref(self.t), _ptr(b), _ptr(x), tol, maxiter, C.byref(rel))
+        return it, x, rel.value
+
+    def cg_dir32(self, b, tol, maxiter, replace=50, x0=None):
+        """One column of the FP32-direction multi-right-hand-side CG."""
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(self.sizes["rowA"]) if x0 is None else np.array(x0, np.float64)
+        rel = C.c_double()
+        it = lib().mfo_cg_dir32(C.byref(self.t), _ptr(b), _ptr(x), tol, maxiter, replace, C.byref(rel))
         return it, x, rel.value
 
     def pcg_jacobi(self, diag, b, tol, maxiter, x0=None):

@@ -6,7 +6,8 @@ import pytest
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("k", [16, 5])
-def test_multi_rhs_columns_match_single_solves(mf, O, k):
+def test_multi_rhs_fp64_panel_columns_match_single_solves(mf, O, k):
+    """MF_PANEL_FP64: every column is the single-right-hand-side FP64 CG."""
     import scipy.sparse as sp
 
     A = mf.Matrix.varpoisson3d(16)
@@ -15,7 +16,7 @@ def test_multi_rhs_columns_match_single_solves(mf, O, k):
     rng = np.random.default_rng(20 + k)
     B = rng.uniform(-1, 1, (n, k))
     B[:, 0] = A.b()
-    X, it, rel, ms = mf.solve_cg_multi(A, B, tol=1e-10, maxiter=20000)
+    X, it, rel, ms = mf.solve_cg_multi(A, B, tol=1e-10, maxiter=20000, panel=mf.PANEL_FP64)
     assert ms > 0
     M = sp.csr_matrix((v, ci, rp), shape=(n, n))
     t = mf.Tiles(A)
@@ -30,6 +31,61 @@ def test_multi_rhs_columns_match_single_solves(mf, O, k):
         if j < 2:
             it_o, _, _ = o.cg(b, 1e-10, 20000)
             assert abs(int(it[j]) - it_o) <= max(2, 0.02 * it_o)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k", [16, 3])
+def test_multi_rhs_fp32_panel_columns_match_oracle(mf, O, k):
+    """MF_PANEL_FP32 (the persistent kernel): each column against the
+    oracle's FP32-direction CG (mfo_cg_dir32, the same recurrence summed in
+    another order): iterations within 2 %, the FP64 true residual at tol,
+    and x against the oracle's and the FP64 CG's solutions."""
+    import scipy.sparse as sp
+
+    A = mf.Matrix.varpoisson3d(16)
+    n = A.n
+    rp, ci, v = A.csr()
+    rng = np.random.default_rng(40 + k)
+    B = rng.uniform(-1, 1, (n, k))
+    B[:, 0] = A.b()
+    X0 = np.zeros((n, k))
+    X0[:, -1] = rng.uniform(-1, 1, n)  # one column starts from a non-zero x0
+    X, it, rel, ms = mf.solve_cg_multi(A, B, X0=X0, tol=1e-10, maxiter=20000)
+    assert ms > 0
+    M = sp.csr_matrix((v, ci, rp), shape=(n, n))
+    o = O.OracleTiles(n, n, rp, ci, v)
+    for j in range(k):
+        b = B[:, j]
+        true_rel = np.linalg.norm(b - M @ X[:, j]) / np.linalg.norm(b)
+        assert rel[j] <= 1e-10 and true_rel <= 1.01e-10, (j, rel[j], true_rel)
+        it_o, x_o, rel_o = o.cg_dir32(b, 1e-10, 20000, replace=50, x0=X0[:, j])
+        assert rel_o <= 1e-10
+        assert abs(int(it[j]) - it_o) <= max(2, 0.02 * it_o), (j, it[j], it_o)
+        assert np.linalg.norm(X[:, j] - x_o) / np.linalg.norm(x_o) < 1e-7
+        it64, x64, _ = o.cg(b, 1e-10, 20000, x0=X0[:, j])
+        assert np.linalg.norm(X[:, j] - x64) / np.linalg.norm(x64) < 1e-7
+        assert it[j] <= 1.06 * it64, (j, it[j], it64)
+
+
+@pytest.mark.gpu
+def test_multi_rhs_fp32_panel_at_64_cubed_keeps_fp64_iterations(mf):
+    """k = 16 on the 64^3 variable-coefficient Poisson: the FP32 panels
+    reach the 1e-10 true residual in every column within 3 % of the FP64
+    panel's iterations (speed is measured by the benchmark at 128^3)."""
+    import scipy.sparse as sp
+
+    A = mf.Matrix.varpoisson3d(64)
+    n = A.n
+    rp, ci, v = A.csr()
+    B = np.random.default_rng(3).uniform(-1, 1, (n, 16))
+    X32, it32, rel32, ms32 = mf.solve_cg_multi(A, B, tol=1e-10, maxiter=40000)
+    X64, it64, rel64, ms64 = mf.solve_cg_multi(A, B, tol=1e-10, maxiter=40000, panel=mf.PANEL_FP64)
+    M = sp.csr_matrix((v, ci, rp), shape=(n, n))
+    for j in range(16):
+        assert rel32[j] <= 1e-10 and rel64[j] <= 1e-10
+        assert np.linalg.norm(B[:, j] - M @ X32[:, j]) / np.linalg.norm(B[:, j]) <= 1.01e-10
+        assert it32[j] <= 1.03 * it64[j], (j, it32[j], it64[j])
+        assert np.linalg.norm(X32[:, j] - X64[:, j]) / np.linalg.norm(X64[:, j]) < 1e-6
 
 
 def test_multi_rhs_argument_checks(mf):
