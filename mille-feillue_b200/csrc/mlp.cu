@@ -254,9 +254,10 @@ __global__ void __launch_bounds__(256) k_mlp_forward(const float *w, const float
 
 // Features + network for every tile, one warp per tile: precision class of
 // tile t at level l -> prec[l * tilenum + t], with f5 = logres[l]. Hard limits
-// on the network's choice: diagonal tiles stay at FP32 or above, FP8 needs a
-// tile dynamic range <= 2^12 and FP16 <= 1e8, and a tile whose scaled
-// magnitude is not finite stays FP64.
+// on the network's choice: FP8 needs a tile dynamic range <= 2^12 and FP16
+// <= 1e8, and a tile whose scaled magnitude is not finite stays FP64. (The
+// diagonal entries of an FP16 / FP8 tile are stored in FP32 by the layout
+// whatever the class, so diagonal tiles need no limit of their own.)
 __global__ void __launch_bounds__(256) k_tile_select_mlp(TileFeatArgs A, const float *w, int nlev,
                                                           const float *logres, uint8_t *prec) {
     __shared__ __align__(16) float sw[FW_FLOATS];
@@ -274,8 +275,6 @@ __global__ void __launch_bounds__(256) k_tile_select_mlp(TileFeatArgs A, const f
 #pragma unroll
         for (int o = 1; o < 4; ++o)
             if (F.o[o] > F.o[c]) c = o;
-        const bool diag = xs[3] > 0.5f;
-        if (diag && c > MF_PREC_FP32) c = MF_PREC_FP32;
         if (c == MF_PREC_FP8 && xs[1] > 3.6124f) c = MF_PREC_FP16;  // log10(4096)
         if (c == MF_PREC_FP16 && xs[1] > 8.0f) c = MF_PREC_FP32;
         if (!isfinite(xs[0]) || xs[0] > 300.f) c = MF_PREC_FP64;

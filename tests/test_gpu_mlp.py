@@ -162,3 +162,43 @@ def test_packaged_selector_solves(mf):
         assert res["status"] == 0 and res["rel_residual_true"] <= 1e-10, res
     finally:
         mf.set_mlp_weights(None)
+
+
+@pytest.mark.gpu
+def test_packaged_selector_gain_over_rule(mf):
+    """What the trained selector gains over the precision rule, judged by the
+    FP64 solve, on held-out matrices of the training family (grids and seeds
+    outside the training set, contrasts over the training range): iterations,
+    SpMV bytes and solve time of the selector's mixed solve against the
+    rule's. Both must reach the 1e-10 FP64 true residual and stay within
+    1e-6 of the FP64 solution; the selector must not fall back, must not
+    lose more than 10 % of the rule's iterations nor add SpMV bytes. The
+    measured ratios are printed (on this family the rule already stores
+    every tile at the lowest precision that converges, FP16 with FP32
+    diagonals, and the selector reproduces it: ratios 1.0)."""
+    import os
+
+    if not os.path.exists(mf.MLP_WEIGHTS_PATH):
+        pytest.skip("no trained selector weights packaged")
+    gains = []
+    for grid, lg, seed in ((44, 1.5, 7001), (52, 4.0, 7002), (60, 7.0, 7003)):
+        A = mf.Matrix.varpoisson3d(grid, 10 ** (-lg / 2), 10 ** (lg / 2), seed)
+        b = A.b()
+        x64, r64 = mf.Tiles(A).solve_cg(b, tol=1e-10, maxiter=40000)
+        tr = mf.Tiles(A, mf.options(precision_mode=mf.MODE_MIXED_RULE))
+        xr, rr = tr.solve_cg(b, tol=1e-10, maxiter=40000)
+        o = mf.options(precision_mode=mf.MODE_MIXED_MLP)
+        o.reserved[6] = rr["iterations"]
+        tm = mf.Tiles(A, o)
+        xm, rm = tm.solve_cg(b, tol=1e-10, maxiter=40000, opts=o)
+        for x, r in ((xr, rr), (xm, rm)):
+            assert r["status"] == 0 and r["rel_residual_true"] <= 1e-10, r
+            assert np.linalg.norm(x - x64) / np.linalg.norm(x64) < 1e-6
+        assert rm["selector_fallback"] == 0, rm
+        assert rm["iterations"] <= 1.1 * rr["iterations"], (rm["iterations"], rr["iterations"])
+        assert rm["spmv_bytes_level"][0] <= rr["spmv_bytes_level"][0] * (1 + 1e-9)
+        gains.append({"grid": grid, "log10_contrast": lg, "fp64_iters": r64["iterations"],
+                      "iters_rule_over_mlp": rr["iterations"] / rm["iterations"],
+                      "bytes_rule_over_mlp": rr["spmv_bytes_level"][0] / rm["spmv_bytes_level"][0],
+                      "time_rule_over_mlp": rr["time_ms"] / rm["time_ms"]})
+    print("selector gain over the rule:", gains)
