@@ -84,8 +84,8 @@ def test_training_learns_a_rule(mf):
 
 
 def _select_numpy(logits, f):
+    """The selector's class with its hard limits (k_tile_select_mlp)."""
     c = logits.argmax(1)
-    c = np.where((f[:, 3] > 0.5) & (c > 1), 1, c)
     c = np.where((c == 3) & (f[:, 1] > 3.6124), 2, c)
     c = np.where((c == 2) & (f[:, 1] > 8.0), 1, c)
     c = np.where(~np.isfinite(f[:, 0]) | (f[:, 0] > 300), 0, c)
