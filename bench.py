@@ -310,7 +310,7 @@ def gpu_arm(args, world, rank, local, dist):
     errpc = float(np.linalg.norm(xd.cpu().numpy() - xstar) / np.linalg.norm(xstar))
     # the same FP64 CG built from cuSPARSE + cuBLAS calls (baseline/cusparse)
     vs_cusp = None
-    Lc = _cusp_lib() if rank == 0 else None
+    Lc = _cusp_lib() if rank == 0 and not args.no_cusparse else None
     if Lc is not None:
         _cusp_solve(Lc, "cg", A, b, 0.0, 5)
         cu = _cusp_solve(Lc, "cg", A, b, TOL, MAXITER)
@@ -744,6 +744,7 @@ def main():
                          "smaller only for quick checks)")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cusparse", action="store_true", help="skip the cuSPARSE + cuBLAS comparison leg")
     ap.add_argument("--no-extra", action="store_true", help="skip the batch512 / multi16 legs of the default run")
     ap.add_argument("--workload", default="poisson128",
                     choices=["poisson128", "batch", "vs_cusparse", "multi16", "profile"])
