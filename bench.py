@@ -368,11 +368,12 @@ def gpu_arm(args, world, rank, local, dist):
         return gbs
 
     gbs = roof(res, kms)
-    # DRAM bytes per CG iteration (read + write) measured with ncu on a
-    # 20-iteration launch of the same matrix (dram__bytes_read + write),
+    # DRAM bytes per CG iteration (read + write) measured with ncu as the
+    # difference of a 40- and a 20-iteration launch of the same matrix
+    # (dram__bytes_read + write; profiles/k_cg_tm_k_cgcg_tm_varpoisson128.md),
     # scaled by the iterations of the timed solve (plus the initial and the
     # replacement FP64 SpMVs at their algorithmic bytes)
-    dram_per_iter = {"mixed": 98.8e6, "fp64": 151.7e6}[headline]
+    dram_per_iter = {"mixed": 44.2e6, "fp64": 150.4e6}[headline]
     traffic = res["iterations"] * dram_per_iter + (1 + res["replacements"]) * spmv_bytes
     kname = ("k_cgcg_tm (mixed single-reduction CG, x and r in tensor memory)" if headline == "mixed"
              else "k_cg_tm (FP64 CG, x and r in tensor memory)")
