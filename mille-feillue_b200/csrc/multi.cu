@@ -569,6 +569,11 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+// The same with an L2 eviction policy (the streamed FP64 panels X and R).
+__device__ __forceinline__ void st_d4_pol(double *p, const double (&v)[4], uint64_t pol) {
+    st2_hint(p, make_double2(v[0], v[1]), pol);
+    st2_hint(p + 2, make_double2(v[2], v[3]), pol);
+}
 __device__ __forceinline__ void st_d4(double *p, const double (&v)[4]) {
     reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
     reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
@@ -730,12 +735,16 @@ __device__ void mrf_residual(const MrfParams &P, const MrfShared &S, int r0, int
 // rows of a CTA are contiguous, so each array of a chunk is one copy) up to
 // MRF_STAGES chunks ahead, and the whole CTA computes from shared memory and
 // stores its results to global memory. `par` holds the parity of each
-// stage's next wait (uniform across the CTA).
+// stage's next wait (uniform across the CTA). L2 policies: the streamed
+// arrays (matrix, X, R, B, Q) evict first; the search directions P, which
+// the product pass reads again through the windows of several blocks, evict
+// last.
 struct MrfRing {
     uint8_t *buf;
     int sb;  // bytes a stage
     uint32_t par;
-    uint64_t pol;
+    uint64_t pol;  // evict first
+    uint64_t pl;   // evict last (P)
 };
 
 __device__ __forceinline__ void mrf_wait_full(const MrfParams &P, MrfShared &S, MrfRing &R, int k) {
@@ -910,7 +919,7 @@ __device__ __forceinline__ void mrf_spmm_win(const MrfParams &P, MrfShared &S, M
             for (int j = 0; j < pl.nruns; ++j) {
                 const MrfRun ru = pl.run[j];
                 bulk_g2s(st + MRF_WOFF_WIN + (size_t)ru.slot0 * 1024, P.P + (size_t)ru.seg0 * 16 * KW,
-                         (uint32_t)ru.nseg * 1024, &S.full[k], R.pol);
+                         (uint32_t)ru.nseg * 1024, &S.full[k], R.pl);
             }
         } else {
             bulk_g2s(st + MRF_WOFF_EC, P.ecT + blk * 8 * MRF_BLK, MRF_BLK * 8 * 4, &S.full[k], R.pol);
@@ -992,6 +1001,7 @@ __global__ void __launch_bounds__(MRF_THREADS, 1) k_mr_fused(MrfParams P) {
     ring.sb = P.stage_bytes;
     ring.par = 0;
     ring.pol = policy_evict_first();
+    ring.pl = policy_evict_last();
     if (tid == 0) {
         S.abort = 0, S.any_rep = 0;
         for (int k = 0; k < MRF_STAGES; ++k) mbar_init(&S.full[k], 1);
@@ -1124,7 +1134,7 @@ __global__ void __launch_bounds__(MRF_THREADS, 1) k_mr_fused(MrfParams P) {
                 r[3] = __dsub_rn(r23.y, dmul(al[3], (double)q.w));
 #pragma unroll
                 for (int m = 0; m < 4; ++m) rr[m] += r[m] * r[m];
-                st_d4(P.R + (size_t)row * KW + 4 * cg, r);
+                st_d4_pol(P.R + (size_t)row * KW + 4 * cg, r, ring.pol);
             };
             mrf_pass(P, S, ring, r0, r1, MRF_ROWS, issue, body);
             if (!mrf_gsum(P, S, rr, phase)) return;
@@ -1149,7 +1159,7 @@ __global__ void __launch_bounds__(MRF_THREADS, 1) k_mr_fused(MrfParams P) {
                 uint8_t *st = ring.buf + (size_t)k * ring.sb;
                 mbar_arrive_expect_tx(&S.full[k], (uint32_t)rn * 192);
                 bulk_g2s(st, P.X + (size_t)rb * KW, (uint32_t)rn * 128, &S.full[k], ring.pol);
-                bulk_g2s(st + MRF_ROWS * 128, P.P + (size_t)rb * KW, (uint32_t)rn * 64, &S.full[k], ring.pol);
+                bulk_g2s(st + MRF_ROWS * 128, P.P + (size_t)rb * KW, (uint32_t)rn * 64, &S.full[k], ring.pl);
             };
             auto body = [&](int rb, int rn, const uint8_t *st) {
                 if (rs >= rn) return;
@@ -1162,7 +1172,7 @@ __global__ void __launch_bounds__(MRF_THREADS, 1) k_mr_fused(MrfParams P) {
                 x[1] = dadd(x01.y, dmul(al[1], (double)p.y));
                 x[2] = dadd(x23.x, dmul(al[2], (double)p.z));
                 x[3] = dadd(x23.y, dmul(al[3], (double)p.w));
-                st_d4(P.X + (size_t)row * KW + 4 * cg, x);
+                st_d4_pol(P.X + (size_t)row * KW + 4 * cg, x, ring.pol);
             };
             mrf_pass(P, S, ring, r0, r1, MRF_ROWS, issue, body);
             mrf_publish(P, ++ep);
@@ -1207,7 +1217,7 @@ __global__ void __launch_bounds__(MRF_THREADS, 1) k_mr_fused(MrfParams P) {
             auto issue = [&](int rb, int rn, int k) {
                 uint8_t *st = ring.buf + (size_t)k * ring.sb;
                 mbar_arrive_expect_tx(&S.full[k], (uint32_t)rn * (replaced ? 192 : 320));
-                bulk_g2s(st, P.P + (size_t)rb * KW, (uint32_t)rn * 64, &S.full[k], ring.pol);
+                bulk_g2s(st, P.P + (size_t)rb * KW, (uint32_t)rn * 64, &S.full[k], ring.pl);
                 bulk_g2s(st + C2 * 64, P.R + (size_t)rb * KW, (uint32_t)rn * 128, &S.full[k], ring.pol);
                 if (!replaced)
                     bulk_g2s(st + C2 * 192, P.X + (size_t)rb * KW, (uint32_t)rn * 128, &S.full[k], ring.pol);
@@ -1227,14 +1237,14 @@ __global__ void __launch_bounds__(MRF_THREADS, 1) k_mr_fused(MrfParams P) {
                     x[1] = dadd(x01.y, dmul(al[1], (double)p.y));
                     x[2] = dadd(x23.x, dmul(al[2], (double)p.z));
                     x[3] = dadd(x23.y, dmul(al[3], (double)p.w));
-                    st_d4(P.X + (size_t)row * KW + 4 * cg, x);
+                    st_d4_pol(P.X + (size_t)row * KW + 4 * cg, x, ring.pol);
                 }
                 float4 np;
                 np.x = live[0] ? __double2float_rn(dadd(r01.x, dmul(bt[0], (double)p.x))) : 0.f;
                 np.y = live[1] ? __double2float_rn(dadd(r01.y, dmul(bt[1], (double)p.y))) : 0.f;
                 np.z = live[2] ? __double2float_rn(dadd(r23.x, dmul(bt[2], (double)p.z))) : 0.f;
                 np.w = live[3] ? __double2float_rn(dadd(r23.y, dmul(bt[3], (double)p.w))) : 0.f;
-                *reinterpret_cast<float4 *>(P.P + (size_t)row * KW + 4 * cg) = np;
+                stf4_hint(P.P + (size_t)row * KW + 4 * cg, np, ring.pl);
             };
             mrf_pass(P, S, ring, r0, r1, C2, issue, body);
         }
