@@ -313,7 +313,8 @@ int mf_solve_cg_multi_dev(int n, const int *row_ptr_dev, const int *col_idx_dev,
  * FP32 (the product summed in FP64, then rounded), x, r, dots and scalars
  * FP64, r replaced by b - A x every 50 iterations and whenever a column's
  * recursive residual reaches tol; a column converges on that true residual
- * (rel_residual is then the true one). One persistent launch per solve.
+ * (rel_residual is then the true one), and a replacement whose true residual
+ * norm exceeds twice the recursive one restarts that column (p = r). One persistent launch per solve.
  * MF_PANEL_FP64: every panel FP64; each column is exactly the single
  * right-hand-side FP64 CG (recursive residual), five launches an iteration. */
 #define MF_PANEL_FP64 0

@@ -470,7 +470,15 @@ static int solve_dev_once(mf_tiles *t, int kind, const double *b_dev, double *x_
         P.trace_iters = ti;
         t->trace_iters = ti;
     }
-    const bool mixed = (kind == 0 || kind == 1) && opt.precision_mode != MF_MODE_FP64 && t->mixed_ready;
+    // A mixed solve whose levels hold no tile below FP64 (every row block
+    // oversize, for example) gains nothing from the low-precision kernels
+    // and runs the FP64 solver: the single-reduction CG keeps its search
+    // directions in FP32, which only pays with a low-precision operator.
+    bool any_low = false;
+    for (int l = 0; l < MF_NLEVELS; ++l)
+        if (t->Lmix[l].built && t->Lmix[l].kind != LAYOUT_FP64) any_low = true;
+    const bool mixed =
+        (kind == 0 || kind == 1) && opt.precision_mode != MF_MODE_FP64 && t->mixed_ready && any_low;
     const Layout *lv[MF_NLEVELS] = {nullptr, nullptr, nullptr};  // the mixed levels this solve runs
     if (mixed) {
         int nl = 1;

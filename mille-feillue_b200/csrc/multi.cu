@@ -344,8 +344,10 @@ __global__ void k_mr_unpack(int n, int k, const double *panel, double *cm) {
 // in blockspmv_cpu's order. FP32 directions need the true residual: after
 // the r update, r = b - A x replaces it every MRF_REPLACE iterations and
 // whenever a column's recursive residual reaches tol; a column converges only
-// on that true residual. Each column then runs the recurrence of
-// mfo_cg_dir32 (oracle), independently of the others.
+// on that true residual, and a replacement whose true residual norm exceeds
+// twice the recursive one restarts that column's recurrence (beta = 0). Each
+// column then runs the recurrence of mfo_cg_dir32 (oracle), independently of
+// the others.
 //
 // One cooperative launch runs the whole solve. Every CTA owns a contiguous
 // range of rows; per iteration
@@ -430,7 +432,7 @@ struct MrfShared {
     double chunk[32][KW];
     double bres[KW];
     double rr[KW], bb[KW], alpha[KW], beta[KW];
-    int live[KW], rep[KW], iters[KW], conv[KW];
+    int live[KW], rep[KW], iters[KW], conv[KW], restart[KW];
     int any_rep, n_live, abort;
     uint64_t full[MRF_STAGES];
 };
@@ -1011,6 +1013,7 @@ __global__ void __launch_bounds__(MRF_THREADS, 1) k_mr_fused(MrfParams P) {
         S.rep[tid] = 1;
         S.iters[tid] = 0;
         S.conv[tid] = 0;
+        S.restart[tid] = 0;
     }
     // window mode: this CTA's block plans, after the ring (they never change)
     MrfPlan *plans = reinterpret_cast<MrfPlan *>(mrf_dyn + (size_t)MRF_STAGES * P.stage_bytes);
@@ -1144,6 +1147,7 @@ __global__ void __launch_bounds__(MRF_THREADS, 1) k_mr_fused(MrfParams P) {
             const double rel = b2 > 0 ? sqrt(rrn / b2) : sqrt(rrn);
             S.rep[tid] = S.live[tid] && ((P.replace_every > 0 && it % P.replace_every == 0) || !(rel > P.tol));
             S.beta[tid] = rrn;  // r.r of the recursive residual, until replaced
+            S.restart[tid] = 0;
         }
         __syncthreads();
         if (tid == 0) {
@@ -1184,6 +1188,11 @@ __global__ void __launch_bounds__(MRF_THREADS, 1) k_mr_fused(MrfParams P) {
             if (tid < KW) {
                 const double rrn = S.bres[tid], b2 = S.bb[tid];
                 if (S.rep[tid]) {
+                    // a true residual norm more than twice the recursive one:
+                    // the FP32 products let the recursive residual drift below
+                    // it, and beta from the two would break the directions'
+                    // conjugacy; restart from the true residual (p = r)
+                    S.restart[tid] = rrn > 4.0 * S.beta[tid];
                     S.beta[tid] = rrn;
                     const double rel = b2 > 0 ? sqrt(rrn / b2) : sqrt(rrn);
                     if (!(rel > P.tol)) {  // converged on the true residual
@@ -1198,7 +1207,7 @@ __global__ void __launch_bounds__(MRF_THREADS, 1) k_mr_fused(MrfParams P) {
         if (tid < KW) {
             const double rrn = S.beta[tid];
             if (S.live[tid]) {
-                S.beta[tid] = rrn / S.rr[tid];
+                S.beta[tid] = S.restart[tid] ? 0.0 : rrn / S.rr[tid];
                 S.rr[tid] = rrn;
                 S.iters[tid] = it;
                 if (!isfinite(rrn)) S.live[tid] = 0;

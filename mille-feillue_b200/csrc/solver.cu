@@ -976,12 +976,32 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cg(KParams P) {
             if (!cta_spmv<false>(P, lay64, x, S, dyn, pp, e2)) return;
             double v1[1] = {e2.rr}, o1[1];
             if (!grid_sum<1>(P, S, v1, o1, phase)) return;
+            const double rr_rec = rr;
             rr = o1[0];
             ++repl;
             if (pending) {
                 pending = false;
                 rel = bnorm > 0 ? sqrt(rr) / bnorm : 0.0;
                 if (rel <= tol) break;
+            }
+            // a true residual norm more than twice the recursive one (a
+            // low-precision operator's iterate drifted from A's): restart
+            // the directions from the true residual, d = r
+            if (rr > 4.0 * rr_rec) {
+                MF_PAIRS(4, vlo, vhi, {
+                    double2 rv[_vb];
+#pragma unroll
+                    MF_FOR_VB if (MF_LIVE(u, vhi)) rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+#pragma unroll
+                    MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                        st2_hint(d + 2 * MF_PI(u), rv[u], vpol);
+                        if (MIXED)
+                            stf2_hint(d32 + 2 * MF_PI(u),
+                                      make_float2(__double2float_rn(rv[u].x), __double2float_rn(rv[u].y)), vpol);
+                    }
+                })
+                ++ep;
+                publish(P, ep);
             }
             // a low-precision operator that lets the true residual grow
             // 100x above the best seen falls back to the FP64 layout
@@ -1365,6 +1385,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_cgcg(KParams P) {
                 rel = relt;
                 if (rel <= tol) break;
             }
+            // a true residual norm more than twice the recursive one (the
+            // low-precision operator's iterate has drifted from A's):
+            // beta = gamma_true / gamma_old would break the directions'
+            // conjugacy, so the next step restarts from the true residual
+            // (beta = 0: p = r, s = w)
+            if (c1[0] > 4.0 * gam) first = true;
             if (lay != lay64) {
                 if (c1[0] < rr_best) rr_best = c1[0];
                 if (!(c1[0] <= 1e4 * rr_best)) {
@@ -1778,6 +1804,12 @@ __device__ __forceinline__ void cgcg_tm_body(const KParams &P, Smem &S, uint8_t 
                 rel = relt;
                 if (rel <= tol) break;
             }
+            // a true residual norm more than twice the recursive one (the
+            // low-precision operator's iterate has drifted from A's):
+            // beta = gamma_true / gamma_old would break the directions'
+            // conjugacy, so the next step restarts from the true residual
+            // (beta = 0: p = r, s = w)
+            if (c1[0] > 4.0 * gam) first = true;
             if (lay != lay64) {
                 if (c1[0] < rr_best) rr_best = c1[0];
                 if (!(c1[0] <= 1e4 * rr_best)) {
@@ -1847,8 +1879,12 @@ __device__ __forceinline__ void cgcg_tm_body(const KParams &P, Smem &S, uint8_t 
         }
         const float *sp = reinterpret_cast<const float *>(dyn);
         double rsn, psn;
+        // the next SpMV reads r from global memory unless its layout stages
+        // x in FP32 (then it reads r32): the FP64 layout, and mixed layouts
+        // with FP64 tiles, need r written back from tensor memory
+        const bool r_global = lay == lay64 || !P.lay[lay].x32;
         s_gpart[tid] = tm_update_smem(tm_rows(P, s_tmem), alpha, beta, sp, sp + (vhi - vlo), sp + 2 * (vhi - vlo),
-                                      pv32, sv32, r32, lay == lay64 ? r : nullptr, vpol, rsn, psn);
+                                      pv32, sv32, r32, r_global ? r : nullptr, vpol, rsn, psn);
         for (int o = 16; o > 0; o >>= 1) {
             rsn += __shfl_xor_sync(0xffffffffu, rsn, o);
             psn += __shfl_xor_sync(0xffffffffu, psn, o);

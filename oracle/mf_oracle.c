@@ -443,16 +443,21 @@ int mfo_cg_dir32(const mfo_tiles *t, const double *b, double *x, double tol, int
         for (int i = 0; i < n; ++i) { x[i] += alpha * d[i]; r[i] -= alpha * q[i]; }
         double rrn = mfo_dot(n, r, r);
         double relr = bb > 0 ? sqrt(rrn / bb) : sqrt(rrn);
+        int restart = 0;
         if ((replace > 0 && it % replace == 0) || !(relr > tol)) {
+            const double rec = rrn;
             mfo_blockspmv(t, x, q, NULL, NULL, NULL);
             for (int i = 0; i < n; ++i) r[i] = b[i] - q[i];
             rrn = mfo_dot(n, r, r);
             relr = bb > 0 ? sqrt(rrn / bb) : sqrt(rrn);
             rel = relr;
             if (!(relr > tol)) { rr = rrn; break; }
+            /* a true residual norm more than twice the recursive one: the
+             * directions no longer match r; restart from it (d = r) */
+            restart = rrn > 4.0 * rec;
         }
         rel = relr;
-        const double beta = rrn / rr;
+        const double beta = restart ? 0.0 : rrn / rr;
         rr = rrn;
 #pragma omp parallel for schedule(static)
         for (int i = 0; i < n; ++i) d[i] = (double)(float)(r[i] + beta * d[i]);

@@ -69,7 +69,8 @@ int mfo_cg(const mfo_tiles *t, const double *b, double *x, double tol, int maxit
 /* One column of the FP32-direction multi-right-hand-side CG: d and q = A d
  * rounded to FP32, x, r, dots and scalars FP64, r replaced by b - A x every
  * `replace` iterations and when the recursive residual reaches tol (the stop
- * test uses that true residual). */
+ * test uses that true residual); a replacement whose true residual norm is
+ * more than twice the recursive one restarts the recurrence (d = r). */
 int mfo_cg_dir32(const mfo_tiles *t, const double *b, double *x, double tol, int maxiter, int replace,
                  double *rel_res);
 

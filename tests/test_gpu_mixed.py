@@ -151,3 +151,37 @@ def test_negative_row_sums_do_not_take_compensated_fp16(mf):
         _, r = t.solve_cg(np.ones(M.n), tol=1e-10, maxiter=20000)
         assert r["status"] == 0 and r["rel_residual_true"] <= 1e-10, r
         assert (r["tile_frac"][2] > 0.5) == want16, (want16, r["tile_frac"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["spd_random", "scattered"])
+@pytest.mark.parametrize("tmem", [True, False])
+def test_mixed_cg_fast_converging_systems(mf, case, tmem):
+    """Diagonally dominant Z-matrices that CG solves in ~50-80 iterations
+    (the batch workload's random SPD systems; a matrix of scattered columns,
+    at most 4 entries a row) get compensated FP16 tiles. With so few
+    iterations, the recursive residual reaches 1e-10 while the true residual
+    still carries the FP16 operator's offset: the solve must restart its
+    directions from the true residual at such a replacement instead of
+    stagnating or diverging, and reach the FP64 true residual."""
+    import sys
+    import os
+
+    sys.path.insert(0, os.path.dirname(__file__))
+    from test_gpu_multi import _matching_spd
+
+    if case == "spd_random":
+        A = mf.Matrix.spd_random(30000, 5)
+    else:
+        M = _matching_spd(40000, 3, 9)
+        A = mf.Matrix.from_csr(M.shape[0], M.shape[0], M.indptr, M.indices, M.data)
+    b = np.random.default_rng(11).uniform(-1, 1, A.n)
+    x64, r64 = mf.Tiles(A).solve_cg(b, tol=1e-10, maxiter=5000)
+    t = mf.Tiles(A, mf.options(precision_mode=mf.MODE_MIXED_RULE))
+    o = mf.options(precision_mode=mf.MODE_MIXED_RULE)
+    if not tmem:
+        o.reserved[5] = 1  # vectors in global memory (k_cgcg)
+    x, r = t.solve_cg(b, tol=1e-10, maxiter=5000, opts=o)
+    assert r["status"] == 0 and r["rel_residual_true"] <= 1e-10, r
+    assert r["iterations"] <= 3 * r64["iterations"], (r["iterations"], r64["iterations"])
+    assert np.linalg.norm(x - x64) / np.linalg.norm(x64) < 1e-7

@@ -171,3 +171,63 @@ def test_multi_rhs_dev_rejects_invalid_csr(mf):
     # the valid matrix still solves through the same entry point
     rc, X, _, rel = _dev_multi(mf, n, rp, ci, v, B)
     assert rc == 0 and rel.max() <= 1e-10
+
+
+def _matching_spd(n, k, seed):
+    """Symmetric, strictly diagonally dominant matrix whose off-diagonal
+    pattern is the union of k random perfect matchings: at most k + 1
+    entries a row, columns scattered over the whole matrix."""
+    import scipy.sparse as sp
+
+    rng = np.random.default_rng(seed)
+    rows, cols, vals = [], [], []
+    for _ in range(k):
+        perm = rng.permutation(n)
+        a, b = perm[0::2], perm[1::2]
+        w = -rng.uniform(0.1, 1.0, len(a))
+        rows += [a, b]
+        cols += [b, a]
+        vals += [w, w]
+    M = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n))
+    M = M + sp.diags(np.asarray(abs(M).sum(1)).ravel() + 0.05)
+    M = sp.csr_matrix(M)
+    M.sort_indices()
+    return M
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["scattered_8", "random_spd_pad32"])
+def test_multi_rhs_fp32_panel_other_product_modes(mf, O, case):
+    """The persistent panel kernel's other product modes against the oracle:
+    a matrix of at most 8 entries a row whose 128-row blocks reach too many
+    panel segments to stage (window mode, unstaged blocks: panel rows loaded
+    from global memory), and the random SPD systems of the batch workload
+    (~17 entries a row, padded to 32: the padded-gather mode with per-thread
+    asynchronous copies). Every column: iterations within 2 % (or 2) of the
+    oracle's FP32-direction CG, the FP64 true residual at tol, x within 1e-7
+    of the oracle's."""
+    import scipy.sparse as sp
+
+    if case == "scattered_8":
+        M = _matching_spd(40000, 3, 9)
+        assert np.diff(M.indptr).max() <= 8
+        A = mf.Matrix.from_csr(M.shape[0], M.shape[0], M.indptr, M.indices, M.data)
+    else:
+        A = mf.Matrix.spd_random(30000, 5)
+        rp, ci, v = A.csr()
+        M = sp.csr_matrix((v, ci, rp), shape=(A.n, A.n))
+        assert 8 < np.diff(rp).max() <= 64
+    n = A.n
+    rp, ci, v = A.csr()
+    B = np.random.default_rng(11).uniform(-1, 1, (n, 16))
+    X, it, rel, _ = mf.solve_cg_multi(A, B, tol=1e-10, maxiter=5000)
+    o = O.OracleTiles(n, n, rp, ci, v)
+    for j in range(16):
+        b = B[:, j]
+        assert rel[j] <= 1e-10
+        assert np.linalg.norm(b - M @ X[:, j]) / np.linalg.norm(b) <= 1.01e-10
+        if j % 5 == 0:
+            it_o, x_o, rel_o = o.cg_dir32(b, 1e-10, 5000)
+            assert rel_o <= 1e-10
+            assert abs(int(it[j]) - it_o) <= max(2, 0.02 * it_o), (j, it[j], it_o)
+            assert np.linalg.norm(X[:, j] - x_o) / np.linalg.norm(x_o) < 1e-7
