@@ -411,15 +411,28 @@ __device__ __forceinline__ bool pair_mixed(const uint8_t *st, int j1, int j2, in
     if (c1 != c2 || (c1 & 0xffu) != 0u || ((f1 ^ f2) & RBF_UNSCALED) || !(f1 & f2 & RBF_FAST)) return false;
     const int n32 = (c1 >> 8) & 0xffu, n16 = (c1 >> 16) & 0xffu, n8 = c1 >> 24;
     float s1 = 0.0f, s2 = 0.0f;
-    if (n8 == 0 && n32 == 1 && (n16 == 6 || n16 == 4)) {
-        // the 3D 7-point / 2D 5-point stencil shapes, fully unrolled
+    if (n8 == 0 && n32 == 1 && n16 >= 3 && n16 <= 6) {
+        // the 3D 7-point / 2D 5-point stencil shapes and their boundary
+        // faces (a plane of the domain lacks one neighbour: the first and
+        // last planes of the 3D stencil have 5), fully unrolled
         const bool u = (f1 & RBF_UNSCALED) != 0;
-        if (n16 == 6) {
-            if (u) rows2_fixed<6, true>(b1, b2, f1, f2, r, xs, s1, s2);
-            else rows2_fixed<6, false>(b1, b2, f1, f2, r, xs, s1, s2);
-        } else {
-            if (u) rows2_fixed<4, true>(b1, b2, f1, f2, r, xs, s1, s2);
-            else rows2_fixed<4, false>(b1, b2, f1, f2, r, xs, s1, s2);
+        switch (n16) {
+            case 6:
+                if (u) rows2_fixed<6, true>(b1, b2, f1, f2, r, xs, s1, s2);
+                else rows2_fixed<6, false>(b1, b2, f1, f2, r, xs, s1, s2);
+                break;
+            case 5:
+                if (u) rows2_fixed<5, true>(b1, b2, f1, f2, r, xs, s1, s2);
+                else rows2_fixed<5, false>(b1, b2, f1, f2, r, xs, s1, s2);
+                break;
+            case 4:
+                if (u) rows2_fixed<4, true>(b1, b2, f1, f2, r, xs, s1, s2);
+                else rows2_fixed<4, false>(b1, b2, f1, f2, r, xs, s1, s2);
+                break;
+            default:
+                if (u) rows2_fixed<3, true>(b1, b2, f1, f2, r, xs, s1, s2);
+                else rows2_fixed<3, false>(b1, b2, f1, f2, r, xs, s1, s2);
+                break;
         }
         a1 = (double)s1;
         a2 = (double)s2;
