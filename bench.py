@@ -402,7 +402,9 @@ def gpu_arm(args, world, rank, local, dist):
             "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
                          "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": kname + "; one launch = one solve; algorithmic bytes = every SpMV's "
-                                   "algorithmic bytes + 56 n per iteration"},
+                                   "algorithmic bytes + the vector bytes the kernel moves per iteration "
+                                   "(28 n mixed, 32 n FP64: x and r stay in tensor memory)",
+                         "dram_bytes_per_iteration_measured": dram_per_iter},
             "spmv": {"fp64": {"ms": spmv_ms, "alg_bytes": spmv_bytes, "gbs": spmv_bytes / spmv_ms / 1e6,
                               "frac": spmv_bytes / spmv_ms / 1e6 / peak, "gflops": 2.0 * len(v) / spmv_ms / 1e6},
                      "mixed_level0": {"ms": spmv_mx_ms, "alg_bytes": spmv_mx_bytes,

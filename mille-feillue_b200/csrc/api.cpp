@@ -596,9 +596,20 @@ static int solve_dev_once(mf_tiles *t, int kind, const double *b_dev, double *x_
         R.spmv_bytes_level[l] = (mixed && lv[l]) ? lv[l]->alg_bytes : 0.0;
     }
     {
-        // per iteration: CG one SpMV + 56 n, PCG + 16 n for 1/a_ii, BiCGSTAB
-        // two SpMVs + 88 n
-        const double vec = (kind == 1 ? 88.0 : kind == 2 ? 72.0 : 56.0) * (double)n;
+        // per iteration: the SpMVs' algorithmic bytes + the vector bytes the
+        // launched kernel moves per row: BiCGSTAB (two SpMVs) 88; CG with
+        // vectors in global memory 56 (x, r, d, q; single-reduction CG
+        // likewise), Jacobi PCG 72 (+ 1/a_ii); with x and r in tensor memory:
+        // single-reduction CG 28 (p, s, w in; p, s and the FP32 copy of r
+        // out; w from the SpMV), FP64 CG 32 (q, d in; q, d out), Jacobi PCG
+        // 40 (q, d and the FP32 1/a_ii twice in; q, d out)
+        const double vpr = kind == 1 ? 88.0
+                           : launch_kind == 3 ? 28.0
+                           : launch_kind == 5 ? 32.0
+                           : launch_kind == 6 ? 40.0
+                           : launch_kind == 4 ? 72.0
+                                              : 56.0;
+        const double vec = vpr * (double)n;
         const double nsp = kind == 1 ? 2.0 : 1.0;
         double tb = (double)(1 + dr.replacements) * (t->L64.alg_bytes + 16.0 * n);  // initial + replacements
         tb += (double)dr.it_layout[0] * (nsp * t->L64.alg_bytes + vec);
