@@ -43,9 +43,14 @@ const char *mf_last_error(void);
 
 /* ---- precision ------------------------------------------------------- */
 enum { MF_PREC_FP64 = 0, MF_PREC_FP32 = 1, MF_PREC_FP16 = 2, MF_PREC_FP8 = 3 };
+/* Mixed modes apply to mf_solve_cg* and mf_solve_bicgstab*. A mixed layout
+ * whose levels hold no tile below FP64 (every row block oversize, for
+ * example) is solved by the FP64 kernels.                                   */
 enum {
     MF_MODE_FP64 = 0,        /* every tile FP64, exact blockspmv order          */
-    MF_MODE_MIXED_RULE = 1,  /* per-tile precision from the magnitude rule      */
+    MF_MODE_MIXED_RULE = 1,  /* per-tile precision from the precision rule:     */
+                             /* FP16 with row-sum compensation on diagonally    */
+                             /* dominant Z-row blocks, the magnitude rule else  */
     MF_MODE_MIXED_MLP = 2,   /* per-tile precision from the learned selector    */
     MF_MODE_FIXED = 3        /* every tile at options.fixed_precision           */
 };
