@@ -118,8 +118,11 @@ typedef struct {
     int iters_level[3];      /* iterations per mixed-precision level           */
     double spmv_bytes_level[3]; /* algorithmic bytes of one SpMV per level     */
     double total_bytes;      /* algorithmic bytes of the whole solve: every
-                                SpMV (replacements included) + 56 n per
-                                iteration of vector traffic                   */
+                                SpMV (replacements included) + the vector
+                                bytes the launched kernel moves per row and
+                                iteration (56 with vectors in global memory;
+                                28 mixed and 32 FP64 CG, 40 Jacobi PCG with
+                                x and r in tensor memory; 88 BiCGSTAB)        */
     int fell_back_fp64;      /* 1 if a low-precision level let the true
                                 residual grow and the solve finished on the
                                 FP64 layout                                   */
