@@ -130,9 +130,10 @@ constexpr int XSEG_MAX = 112;      // staged x segments per slab (14 KB of FP64 
 constexpr uint32_t XZERO_OFF = XSEG_MAX * 128;
 // Layouts staging FP32 x (every tile below FP64) move XEXTRA32 bytes of each
 // stage from the slab area to the x window, when the slab area is large
-// enough: their slabs are small (FP16 values), and the slab count, not its
-// bytes, sets the ring's pace, so a wider x window (more row blocks per
-// slab) is what they need. The window then ends at the same zero slot.
+// enough: their slabs are small (FP16 values), and the wider window lets a
+// slab hold twice the row blocks of an FP64-x layout. The window then ends
+// at the same zero slot. (Measured on the 128^3 Poisson: 6 KB with 60 row
+// blocks a slab is faster than 12 KB / 90 or 16 KB / 120.)
 constexpr int XEXTRA32 = 6144;
 __host__ __device__ inline int x32_extra(int slab_area) { return slab_area >= 4 * XEXTRA32 ? XEXTRA32 : 0; }
 // Start of the x window in a stage, and the x-window position of the zero
