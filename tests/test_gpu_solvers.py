@@ -148,3 +148,77 @@ def test_jacobi_pcg_iterations_match_oracle(mf, O, maker):
     assert abs(res["iterations"] - it_o) <= max(2, 0.02 * it_o), (res["iterations"], it_o)
     M = _csr_mat(rp, ci, v, n)
     assert np.linalg.norm(b - M @ x) / np.linalg.norm(b) <= 2e-10
+
+
+def _tridiag(n, lo=-1.0, d=2.5, hi=-1.0):
+    rp, ci, v = [0], [], []
+    for i in range(n):
+        for j, a in ((i - 1, lo), (i, d), (i + 1, hi)):
+            if 0 <= j < n:
+                ci.append(j)
+                v.append(a)
+        rp.append(len(ci))
+    return np.array(rp, np.int32), np.array(ci, np.int32), np.array(v)
+
+
+@pytest.mark.parametrize("n", [1, 5, 16, 17, 33, 2047])
+def test_tiny_and_ragged_systems_against_oracle(mf, O, n):
+    """Systems of fewer row blocks than CTAs (most CTAs own no rows) and of
+    a ragged last row block: SpMV bit-exact, CG and BiCGSTAB iterations
+    within +-2 of the oracle's, Jacobi PCG to the true residual.
+
+    With n = 1 (mod 16) the last row block holds one row, for which the
+    reference's Tile_create copies no values (exclusive_scan_char skips a
+    length-1 scan: Performance-Comparison/utils.h:52-53, csr2block.h:236-250):
+    the reference and the oracle return 0 for that row, the device tiles keep
+    it. There every other row is compared bit for bit, the last with the
+    exact product, and the solves with the true residual only."""
+    rng = np.random.default_rng(n)
+    b = rng.uniform(-1, 1, n)
+    rp, ci, v = _tridiag(n)
+    A = mf.Matrix.from_csr(n, n, rp, ci, v)
+    t = mf.Tiles(A)
+    o = O.OracleTiles(n, n, rp, ci, v)
+    M = _csr_mat(rp, ci, v, n)
+    tail1 = n % 16 == 1
+    xr = rng.standard_normal(n)
+    y, yo = t.spmv(xr), o.spmv(xr)
+    if tail1:
+        assert np.array_equal(y[:-1], yo[:-1]) and yo[-1] == 0.0
+        assert np.isclose(y[-1], (M @ xr)[-1], rtol=1e-13, atol=1e-13)
+    else:
+        assert np.array_equal(y, yo)
+    x, r = t.solve_cg(b, tol=1e-10, maxiter=1000)
+    assert r["status"] == 0, r
+    if not tail1:
+        it_o, _, _ = o.cg(b, 1e-10, 1000)
+        assert abs(r["iterations"] - it_o) <= 2, (r, it_o)
+    assert np.linalg.norm(b - M @ x) / np.linalg.norm(b) <= 2e-10
+    x, r = t.solve_pcg(b, tol=1e-10, maxiter=1000)
+    assert r["status"] == 0 and np.linalg.norm(b - M @ x) / np.linalg.norm(b) <= 2e-10, r
+    rp2, ci2, v2 = _tridiag(n, lo=-1.3, hi=-0.7)  # nonsymmetric
+    A2 = mf.Matrix.from_csr(n, n, rp2, ci2, v2)
+    t2 = mf.Tiles(A2)
+    o2 = O.OracleTiles(n, n, rp2, ci2, v2)
+    x, r = t2.solve_bicgstab(b, tol=1e-10, maxiter=1000)
+    assert r["status"] == 0, r
+    if not tail1:
+        it_o, _, _ = o2.bicgstab(b, 1e-10, 1000)
+        assert abs(r["iterations"] - it_o) <= 2, (r, it_o)
+    M2 = _csr_mat(rp2, ci2, v2, n)
+    assert np.linalg.norm(b - M2 @ x) / np.linalg.norm(b) <= 2e-10
+
+
+def test_zero_rhs_and_zero_maxiter(mf):
+    """b = 0 is solved by x0 = 0 without an iteration; maxiter = 0 returns
+    MF_ERR_NOT_CONVERGED with x0 untouched."""
+    A = mf.Matrix.poisson2d(32)
+    t = mf.Tiles(A)
+    z = np.zeros(A.n)
+    for solve in (t.solve_cg, t.solve_bicgstab, t.solve_pcg):
+        x, r = solve(z, tol=1e-10, maxiter=100)
+        assert r["status"] == 0 and r["iterations"] == 0 and not x.any(), (solve.__name__, r)
+        x0 = np.full(A.n, 0.5)
+        x, r = solve(A.b(), x0=x0, tol=1e-10, maxiter=0)
+        assert r["status"] == mf.MF_ERR_NOT_CONVERGED and r["iterations"] == 0, (solve.__name__, r)
+        assert np.array_equal(x, x0)
