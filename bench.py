@@ -620,7 +620,7 @@ def batch_arm(args, world, rank, local, dist, steps=None, warmup=None):
 
 
 def _extra_legs(args, world, rank, local, dist, out):
-    """The north star's two other workloads, measured in the default run
+    """The two other workloads of the solver, measured in the default run
     beside the headline: the batched 512-system launch against one launch
     per system (systems split over the ranks), and CG on 16 right-hand sides
     against 16 single solves (rank 0 of a one-GPU run)."""

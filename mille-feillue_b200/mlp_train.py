@@ -128,7 +128,7 @@ def train(x, y, steps, batch, lr, seed):
 
 def evaluate(cases, weights):
     """Per held-out matrix: the FP64 solve, the rule's and the network's
-    mixed solves (the network's with its rule fallback), each judged by the
+    mixed solves (the network's with its rule fallback), each checked by the
     FP64 true residual and by ||x - x_FP64|| / ||x_FP64||."""
     mf.set_mlp_weights(weights)
     rows = []

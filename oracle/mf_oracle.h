@@ -1,7 +1,7 @@
 /*
  * mf_oracle.h -- CPU oracle of the tiled CG / BiCGSTAB path.
  *
- * TEST INFRASTRUCTURE ONLY. This library is the checker: only tests/,
+ * TEST INFRASTRUCTURE ONLY. This library checks the CUDA path: only tests/,
  * __graft_entry__.smoke() and the cpu_baseline / reference legs of bench.py
  * may load it. The product path (libmf.so) never links or calls it.
  *

@@ -166,8 +166,8 @@ def test_packaged_selector_solves(mf):
 
 @pytest.mark.gpu
 def test_packaged_selector_gain_over_rule(mf):
-    """What the trained selector gains over the precision rule, judged by the
-    FP64 solve, on held-out matrices of the training family (grids and seeds
+    """What the trained selector gains over the precision rule, measured
+    against the FP64 solve, on held-out matrices of the training family (grids and seeds
     outside the training set, contrasts over the training range): iterations,
     SpMV bytes and solve time of the selector's mixed solve against the
     rule's. Both must reach the 1e-10 FP64 true residual and stay within

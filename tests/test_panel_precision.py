@@ -1,7 +1,7 @@
 """Numerics of the multi-right-hand-side panel product's precision (CPU).
 
-The block-CG workload's north star names a BF16 tile x panel product on
-tensor cores. These tests restate that product on the CPU for one column
+The block-CG workload's specification names a BF16 tile x panel product
+on tensor cores. These tests restate that product on the CPU for one column
 (q = fl32(bf16(A) bf16(p)): BF16 off-diagonal entries and directions, the
 diagonal in FP32 as in the mixed layouts, exact products, FP32 result),
 inside the CG the panel kernel runs (FP64 x, r, dots and scalars, r replaced
