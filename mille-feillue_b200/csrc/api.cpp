@@ -64,7 +64,11 @@ void mf_options_default(mf_options *o) {
     o->device = 0;
 }
 
-static int fetch_host_tiles(mf_tiles *t) {
+}  // extern "C"
+
+namespace mf {
+int ensure_host_tiles(const mf_tiles *t) {
+    if (t->host_tiles) return MF_OK;
     t->h_tile_ptr.resize(t->tilem + 1);
     t->h_tile_col.resize(t->tilenum);
     std::vector<int> off(t->tilenum + 1);
@@ -74,12 +78,10 @@ static int fetch_host_tiles(mf_tiles *t) {
     MF_CUDA_TRY(cudaMemcpy(off.data(), t->tile_off.p, sizeof(int) * (t->tilenum + 1), cudaMemcpyDeviceToHost));
     t->h_tile_nnz.resize(t->tilenum);
     for (int k = 0; k < t->tilenum; ++k) t->h_tile_nnz[k] = off[k + 1] - off[k];
+    t->host_tiles = true;
     return MF_OK;
 }
 
-}  // extern "C"
-
-namespace mf {
 // Encodes a device CSR; G > 0 forces the number of CTA ranges of the layout
 // (1 for the batched solver, whose CTAs each own a whole system).
 int encode_dev_impl(int n, int ncols, int nnz, const int *rp, const int *ci, const double *val,
@@ -96,7 +98,6 @@ int encode_dev_impl(int n, int ncols, int nnz, const int *rp, const int *ci, con
     if (G_force > 0) t->G = G_force;
     cudaStream_t s = 0;
     if ((rc = encode_device(t, n, ncols, nnz, rp, ci, val, s)) != MF_OK) { delete t; return rc; }
-    if ((rc = fetch_host_tiles(t)) != MF_OK) { delete t; return rc; }
     std::vector<uint8_t> prec(t->tilenum, MF_PREC_FP64);
     if ((rc = build_layout(t, t->L64, prec, s)) != MF_OK) { delete t; return rc; }
     if (t->opt.precision_mode != MF_MODE_FP64) {
@@ -174,6 +175,7 @@ double layout_dev_bytes(const Layout &L) {
 int mf_memory_report(const mf_tiles *t, mf_memory_cost *r) {
     if (!t || !r) return MF_ERR_ARG;
     std::memset(r, 0, sizeof *r);
+    if (int rc = mf::ensure_host_tiles(t)) return rc;
     const double tn = t->tilenum, tm = t->tilem;
     r->csr_bytes = (double)(t->rowA + 1) * 4 + (double)t->csrsize * (4 + 8);
     r->tile_index_bytes = (tm + 1) * 4 + tn * 4 + (tn + 1) * 1 + (tn + 1) * 4 + (tn + 1) * 4 + (tn + 3) * 4 +

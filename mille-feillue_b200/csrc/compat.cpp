@@ -81,6 +81,7 @@ int bicgstab(int *RowPtr, int *ColIdx, double *Val, double *rhs, double *x, int 
 int mf_balance_twopointer(const mf_tiles *t, int block_nnz, int block_per_warp, int *index, int *bptr,
                           int *idx_new, int *row_new, int *non_new) {
     if (!t || !index || block_nnz <= 0 || block_per_warp <= 0) return MF_ERR_ARG;
+    if (int rc = mf::ensure_host_tiles(t)) return rc;
     const int tilenum = t->tilenum;
     std::vector<int> non(tilenum + 1, 0), row(tilenum + 1, 0);
     for (int rb = 0; rb < t->tilem; ++rb)

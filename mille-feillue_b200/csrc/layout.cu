@@ -806,6 +806,7 @@ int check_plans(mf_tiles *t, int G, const std::vector<int> &cta_rb, const std::v
                 int xseg_max, int slab_lim, int rbps, int maxw, const std::vector<int> &cta_slab_gpu, int ns,
                 int nsegs, int nruns, const DevArray<SlabPlan> &d_plans, const DevArray<int> &d_slab_cta,
                 const DevArray<int> &d_segs, const DevArray<XRun> &d_runs, cudaStream_t st) {
+    if (int rc = ensure_host_tiles(t)) return rc;
     const auto &tp = t->h_tile_ptr;
     const auto &tc = t->h_tile_col;
     auto rb_bytes = [&](int rb, bool gather) {
@@ -1076,6 +1077,7 @@ int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec_in, cu
     // oversize row blocks are computed in FP64 from the tile arrays
     std::vector<uint8_t> over(tilem, 0);
     if (n_over > 0) {
+        if (int rc = ensure_host_tiles(t)) return rc;
         MF_CUDA_TRY(cudaMemcpyAsync(over.data(), d_over.p, tilem, cudaMemcpyDeviceToHost, st));
         MF_CUDA_TRY(cudaStreamSynchronize(st));
         for (int rb = 0; rb < tilem; ++rb)

@@ -281,9 +281,13 @@ struct mf_tiles {
     int nlevels = 0;                        // mixed levels built
     double level_switch[MF_NLEVELS] = {0};  // relative residual to leave level l
     double encode_ms = 0, layout_ms = 0;
-    // host copies used by the layout planner; h_cta_rb is the CTA row-block
-    // partition shared by every layout of this matrix
-    std::vector<int> h_tile_ptr, h_tile_col, h_tile_nnz, h_cta_rb;
+    // host copies of tile_ptr, tile_col and the per-tile nnz, fetched on
+    // first use (mf::ensure_host_tiles: oversize row blocks, the planner
+    // check, the memory report, the two-pointer export), not per encode
+    mutable std::vector<int> h_tile_ptr, h_tile_col, h_tile_nnz;
+    mutable bool host_tiles = false;
+    // the CTA row-block partition shared by every layout of this matrix
+    std::vector<int> h_cta_rb;
     // solver workspace
     mf::DevArray<double> ws;
     mf::DevArray<uint32_t> sync;
@@ -298,5 +302,6 @@ namespace mf {
 int encode_device(mf_tiles *t, int n, int ncols, int nnz, const int *rp, const int *ci,
                   const double *val, cudaStream_t s);
 int build_layout(mf_tiles *t, Layout &L, const std::vector<uint8_t> &prec, cudaStream_t s);
+int ensure_host_tiles(const mf_tiles *t);  // fills h_tile_ptr, h_tile_col, h_tile_nnz once
 int exclusive_scan_int(int *d, long long n, cudaStream_t s);  // in place, n elements
 }  // namespace mf

@@ -239,3 +239,18 @@ def test_encode_rejects_invalid_csr(mf, defect):
     rc = L.mf_encode_dev(A.n, A.n, len(v), C.c_void_p(drp.data_ptr()), C.c_void_p(dci.data_ptr()),
                          C.c_void_p(dv.data_ptr()), C.byref(opts), C.byref(h2))
     assert rc == mf.MF_ERR_ARG
+
+
+@pytest.mark.parametrize("block_nnz", [64, 256, 2048])
+def test_two_pointer_export_matches_oracle(mf, O, cases, block_nnz):
+    """mf_balance_twopointer (the reference driver's warp work split, a
+    compatibility export computed on the host from the handle's tile arrays)
+    equals the oracle's restatement, unit for unit."""
+    for name in ("poisson2d_256", "spd_random_20000", "dense_rows_4000"):
+        n, rp, ci, v = cases[name]
+        t = mf.Tiles(csr=(n, n, rp, ci, v))
+        got = t.balance_twopointer(block_nnz, 180)
+        want = O.OracleTiles(n, n, rp, ci, v).balance(block_nnz, 180)
+        assert got[0] == want[0], (name, got[0], want[0])
+        for g, w in zip(got[1:], want[1:]):
+            assert np.array_equal(g, w), name
