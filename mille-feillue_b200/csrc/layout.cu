@@ -565,9 +565,11 @@ __global__ void __launch_bounds__(32) k_plan(PlanArgs A, PlanCounts *cnt, PlanSc
             const int key = has ? TC(k) : -1;
             const bool isnew = has && !find(key);
             const bool left_s = isnew && find(key - 1), right_s = isnew && find(key + 1);
+            // tile columns ascend within a row block (Tile_create's order), so
+            // among the batch's new keys only the previous lane's can be key - 1
             const int nk = isnew ? key : -2;
-            bool left_n = false;
-            for (int j = 0; j < 32; ++j) left_n |= __shfl_sync(full, nk, j) == key - 1 && isnew;
+            const int nk_prev = __shfl_up_sync(full, nk, 1);
+            const bool left_n = isnew && lane > 0 && nk_prev == key - 1;
             const int d = isnew ? 1 - ((left_s || left_n) ? 1 : 0) - (right_s ? 1 : 0) : 0;
             const unsigned bal = __ballot_sync(full, isnew);
             if (isnew) {
