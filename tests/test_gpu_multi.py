@@ -231,3 +231,48 @@ def test_multi_rhs_fp32_panel_other_product_modes(mf, O, case):
             assert rel_o <= 1e-10
             assert abs(int(it[j]) - it_o) <= max(2, 0.02 * it_o), (j, it[j], it_o)
             assert np.linalg.norm(X[:, j] - x_o) / np.linalg.norm(x_o) < 1e-7
+
+
+def _band_spd(n, half):
+    """SPD band matrix: -1 on the `half` diagonals each side, diagonal
+    2 * half + 1 (strictly diagonally dominant)."""
+    rp, ci, v = [0], [], []
+    for i in range(n):
+        for j in range(max(0, i - half), min(n, i + half + 1)):
+            ci.append(j)
+            v.append(2.0 * half + 1.0 if j == i else -1.0)
+        rp.append(len(ci))
+    return np.array(rp, np.int32), np.array(ci, np.int32), np.array(v)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["band_17_csr", "varpoisson3d_3_win", "poisson2d_10_win", "band_50_pad"])
+@pytest.mark.parametrize("panel", ["fp32", "fp64"])
+def test_multi_rhs_tiny_systems(mf, case, panel):
+    """Systems smaller than one 128-row block (most CTAs own no rows; the
+    panels are padded to a whole block) in each product mode: CSR rows
+    (W = 3), 128-row windows (W = 8), padded rows (W = 16). Every column
+    reaches the FP64 true residual and agrees with the single solver."""
+    import scipy.sparse as sp
+
+    if case.startswith("band"):
+        n = int(case.split("_")[1])
+        rp, ci, v = _band_spd(n, 1 if n == 17 else 5)
+        A = mf.Matrix.from_csr(n, n, rp, ci, v)
+    elif case.startswith("varpoisson3d"):
+        A = mf.Matrix.varpoisson3d(3)
+    else:
+        A = mf.Matrix.poisson2d(10)
+    n = A.n
+    rp, ci, v = A.csr()
+    M = sp.csr_matrix((v, ci, rp), shape=(n, n))
+    B = np.random.default_rng(n).uniform(-1, 1, (n, 4))
+    X, it, rel, ms = mf.solve_cg_multi(A, B, tol=1e-10, maxiter=2000,
+                                       panel=mf.PANEL_FP64 if panel == "fp64" else mf.PANEL_FP32)
+    t = mf.Tiles(A)
+    for j in range(B.shape[1]):
+        b = B[:, j]
+        true_rel = np.linalg.norm(b - M @ X[:, j]) / np.linalg.norm(b)
+        assert rel[j] <= 1e-10 and true_rel <= 1.01e-10, (case, j, it[j], rel[j], true_rel)
+        xs, rs = t.solve_cg(b, tol=1e-10, maxiter=2000)
+        assert np.linalg.norm(X[:, j] - xs) / np.linalg.norm(xs) < 1e-8, (case, j)
