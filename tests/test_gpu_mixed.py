@@ -185,3 +185,32 @@ def test_mixed_cg_fast_converging_systems(mf, case, tmem):
     assert r["status"] == 0 and r["rel_residual_true"] <= 1e-10, r
     assert r["iterations"] <= 3 * r64["iterations"], (r["iterations"], r64["iterations"])
     assert np.linalg.norm(x - x64) / np.linalg.norm(x64) < 1e-7
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [5, 17, 33, 2047])
+def test_mixed_solvers_on_tiny_systems(mf, n):
+    """Mixed CG and BiCGSTAB on systems of fewer row blocks than CTAs (most
+    CTAs own no rows) and ragged tails: the FP64 true residual at 1e-10 and
+    the FP64 solver's solution."""
+    import scipy.sparse as sp
+
+    b = np.random.default_rng(n).uniform(-1, 1, n)
+    for lo, hi in ((-1.0, -1.0), (-1.3, -0.7)):  # SPD for CG, nonsymmetric for BiCGSTAB
+        rp, ci, v = [0], [], []
+        for i in range(n):
+            for j, a in ((i - 1, lo), (i, 2.5), (i + 1, hi)):
+                if 0 <= j < n:
+                    ci.append(j)
+                    v.append(a)
+            rp.append(len(ci))
+        rp, ci, v = np.array(rp, np.int32), np.array(ci, np.int32), np.array(v)
+        A = mf.Matrix.from_csr(n, n, rp, ci, v)
+        M = sp.csr_matrix((v, ci, rp), shape=(n, n))
+        t = mf.Tiles(A, mf.options(precision_mode=mf.MODE_MIXED_RULE))
+        solve = t.solve_cg if lo == hi else t.solve_bicgstab
+        x64, r64 = solve(b, tol=1e-10, maxiter=2000, opts=mf.options())
+        xm, rm = solve(b, tol=1e-10, maxiter=2000)
+        assert r64["status"] == 0 and rm["status"] == 0, (n, r64, rm)
+        assert np.linalg.norm(b - M @ xm) / np.linalg.norm(b) <= 1.01e-10, (n, rm)
+        assert np.linalg.norm(xm - x64) / np.linalg.norm(x64) < 1e-8, n
