@@ -68,6 +68,7 @@ void mf_options_default(mf_options *o) {
 
 namespace mf {
 int ensure_host_tiles(const mf_tiles *t) {
+    std::lock_guard<std::mutex> lock(t->host_tiles_mu);
     if (t->host_tiles) return MF_OK;
     t->h_tile_ptr.resize(t->tilem + 1);
     t->h_tile_col.resize(t->tilenum);

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -286,6 +287,7 @@ struct mf_tiles {
     // check, the memory report, the two-pointer export), not per encode
     mutable std::vector<int> h_tile_ptr, h_tile_col, h_tile_nnz;
     mutable bool host_tiles = false;
+    mutable std::mutex host_tiles_mu;  // const entry points may fetch them concurrently
     // the CTA row-block partition shared by every layout of this matrix
     std::vector<int> h_cta_rb;
     // solver workspace
