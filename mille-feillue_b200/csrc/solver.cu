@@ -2450,6 +2450,22 @@ struct EpiDot2 {  // t = A s, ts += t*s, tt += t*t
         tt += acc * acc;
     }
 };
+struct EpiDot4 {  // t = A s; ts += t*s, tt += t*t, hs += r^*s, ht += r^*t
+    static constexpr bool kUsesX = true;  // s is the SpMV input
+    const double *s, *rh;
+    double *t;
+    double ts, tt, hs, ht;
+    uint64_t pol;
+    __device__ double pre(int row) const { return ld_hint(s + row, pol); }
+    __device__ void operator()(int row, double acc, double sv) {
+        st_hint(t + row, acc, pol);
+        const double hv = ld_hint(rh + row, pol);
+        ts += acc * sv;
+        tt += acc * acc;
+        hs += hv * sv;
+        ht += hv * acc;
+    }
+};
 
 // MIXED: both SpMVs run on the low-precision layouts (FP32 copies of p and
 // s are their input on FP32-x layouts); x, r, p, s, t, v, the dots and the
@@ -2510,6 +2526,107 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_bicgstab(KParams P) {
     bool pending = false;
     const bool fixed = P.fixed_iterations > 0;
     const int maxit = fixed ? P.fixed_iterations : P.maxiter;
+    if constexpr (!MIXED) {
+        // FP64: two grid reductions and two vector passes an iteration.
+        // rho' = r^.r_new = r^.s - omega r^.t joins the t.s, t.t reduction;
+        // the x, r and p updates share one pass; that pass's r.r is reduced
+        // with the next iteration's r^.v, so the stop test sees it after the
+        // next SpMV, with x already final (that SpMV's v goes unused).
+        double rrp = 0.0;
+        bool carry = false;  // rrp holds the r.r of an update not yet reduced
+        while (carry || (it < maxit && (fixed || rel > tol))) {
+            if (!wait_deps(P, S, lay64, ep)) return;
+            EpiDot ev{rh, v, 0.0, vpol};
+            if (!cta_spmv<false>(P, lay64, p, S, dyn, pp, ev)) return;
+            double a1[2] = {ev.dot, rrp}, b1[2];
+            if (!grid_sum<2>(P, S, a1, b1, phase)) return;
+            if (carry) {
+                carry = false;
+                rr = b1[1];
+                rel = bnorm > 0 ? sqrt(rr) / bnorm : 0.0;
+                if (!isfinite(rr)) {
+                    status = MF_ERR_BREAKDOWN;
+                    break;
+                }
+                if (it >= maxit || (!fixed && rel <= tol)) break;
+            }
+            if (!(b1[0] != 0.0) || !isfinite(b1[0])) {
+                status = MF_ERR_BREAKDOWN;
+                break;
+            }
+            const double alpha = rho / b1[0];
+            MF_PAIRS(4, vlo, vhi, {
+                double2 rv[_vb], vv[_vb];
+#pragma unroll
+                MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                    rv[u] = ld2_hint(r + 2 * MF_PI(u), vpol);
+                    vv[u] = ld2_hint(v + 2 * MF_PI(u), vpol);
+                }
+#pragma unroll
+                MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                    double2 o;
+                    o.x = rv[u].x - alpha * vv[u].x;
+                    o.y = rv[u].y - alpha * vv[u].y;
+                    st2_hint(s + 2 * MF_PI(u), o, vpol);
+                }
+            })
+            ++ep;
+            publish(P, ep);
+            if (!wait_deps(P, S, lay64, ep)) return;
+            EpiDot4 et{s, rh, t, 0.0, 0.0, 0.0, 0.0, vpol};
+            if (!cta_spmv<false>(P, lay64, s, S, dyn, pp, et)) return;
+            double a2[4] = {et.ts, et.tt, et.hs, et.ht}, b2[4];
+            if (!grid_sum<4>(P, S, a2, b2, phase)) return;
+            if (!(b2[1] != 0.0) || !isfinite(b2[1])) {
+                status = MF_ERR_BREAKDOWN;
+                break;
+            }
+            const double omega = b2[0] / b2[1];
+            const double rho1 = b2[2] - omega * b2[3];
+            const double beta = omega != 0.0 ? (rho1 * alpha) / (rho * omega) : 0.0;
+            rrp = 0.0;
+            MF_PAIRS(2, vlo, vhi, {
+                double2 sv[_vb], xv[_vb], pv[_vb], tv[_vb], vv[_vb];
+#pragma unroll
+                MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                    sv[u] = ld2_hint(s + 2 * MF_PI(u), vpol);
+                    xv[u] = ld2_hint(x + 2 * MF_PI(u), vpol);
+                    pv[u] = ld2_hint(p + 2 * MF_PI(u), vpol);
+                    tv[u] = ld2_hint(t + 2 * MF_PI(u), vpol);
+                    vv[u] = ld2_hint(v + 2 * MF_PI(u), vpol);
+                }
+#pragma unroll
+                MF_FOR_VB if (MF_LIVE(u, vhi)) {
+                    double2 xo, ro, po;
+                    xo.x = xv[u].x + alpha * pv[u].x + omega * sv[u].x;
+                    xo.y = xv[u].y + alpha * pv[u].y + omega * sv[u].y;
+                    st2_hint(x + 2 * MF_PI(u), xo, vpol);
+                    ro.x = sv[u].x - omega * tv[u].x;
+                    ro.y = sv[u].y - omega * tv[u].y;
+                    st2_hint(r + 2 * MF_PI(u), ro, vpol);
+                    po.x = ro.x + beta * (pv[u].x - omega * vv[u].x);
+                    po.y = ro.y + beta * (pv[u].y - omega * vv[u].y);
+                    st2_hint(p + 2 * MF_PI(u), po, vpol);
+                    rrp += ro.x * ro.x + ro.y * ro.y;
+                }
+            })
+            rho = rho1;
+            ++it;
+            carry = true;
+            ++ep;
+            publish(P, ep);
+            if (omega == 0.0) {
+                status = MF_ERR_BREAKDOWN;
+                break;
+            }
+        }
+        if (carry) {  // a breakdown left the last update's r.r unreduced
+            double a1[1] = {rrp}, b1[1];
+            if (!grid_sum<1>(P, S, a1, b1, phase)) return;
+            rr = b1[0];
+            rel = bnorm > 0 ? sqrt(rr) / bnorm : 0.0;
+        }
+    } else {
     while (it < maxit && (fixed || rel > tol || pending)) {
         if (MIXED && (pending || (P.replace_every > 0 && it > 0 && it % P.replace_every == 0))) {
             // r = b - A x on the FP64 layout, rho = r^.r from it
@@ -2654,6 +2771,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_bicgstab(KParams P) {
         rho = rho1;
         ++ep;
         publish(P, ep);
+    }
     }
     if (g == 0 && tid == 0) {
         if (status == MF_OK && !fixed && rel > tol) status = MF_ERR_NOT_CONVERGED;
