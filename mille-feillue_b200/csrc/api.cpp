@@ -600,13 +600,17 @@ static int solve_dev_once(mf_tiles *t, int kind, const double *b_dev, double *x_
     }
     {
         // per iteration: the SpMVs' algorithmic bytes + the vector bytes the
-        // launched kernel moves per row: BiCGSTAB (two SpMVs) 88; CG with
+        // launched kernel moves per row (the SpMVs count their own x and y):
+        // BiCGSTAB (two SpMVs) FP64 112 (r^ in both SpMV epilogues and s in
+        // the second; s pass: r, v in, s out; x, r, p pass: s, x, p, t, v
+        // in, x, r, p out), mixed 136 (s from global memory, three vector
+        // passes, FP32 copies of s and p out); CG with
         // vectors in global memory 56 (x, r, d, q; single-reduction CG
         // likewise), Jacobi PCG 72 (+ 1/a_ii); with x and r in tensor memory:
         // single-reduction CG 28 (p, s, w in; p, s and the FP32 copy of r
         // out; w from the SpMV), FP64 CG 32 (q, d in; q, d out), Jacobi PCG
         // 40 (q, d and the FP32 1/a_ii twice in; q, d out)
-        const double vpr = kind == 1 ? 88.0
+        const double vpr = kind == 1 ? (P.nlay > 1 ? 136.0 : 112.0)
                            : launch_kind == 3 ? 28.0
                            : launch_kind == 5 ? 32.0
                            : launch_kind == 6 ? 40.0
