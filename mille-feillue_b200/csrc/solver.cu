@@ -21,7 +21,10 @@
 //
 // The recurrences follow Mille-feuille_CG_NVIDIA.cu:722-804 (CG) and
 // Mille-feuille_BiCGSTAB_NVIDIA.cu:787-1061 (BiCGSTAB), run to a tolerance
-// instead of a fixed iteration count.
+// instead of a fixed iteration count. The FP64 BiCGSTAB computes the same
+// iterates with two grid reductions an iteration instead of three
+// (r^.r_new = r^.s - omega r^.t): equal in exact arithmetic, rounded
+// differently.
 #include <cuda_fp16.h>
 #include <cuda_fp8.h>
 #include <cuda_runtime.h>
